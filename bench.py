@@ -1,0 +1,416 @@
+#!/usr/bin/env python
+"""Throughput of the B200 electrostatic PIC step (particle-steps/s incl. the
+Poisson multigrid solve), on the 2-D bounded two-species plasma:
+
+  1024 x 1024 cells, dx = 1 (Debye length), grounded Dirichlet walls and
+  absorbing particle boundaries; 256 particles/cell/species (536,870,912
+  particles); electrons vth = 1, ions m = 1836 at equal temperature; uniform
+  positions, Maxwellian velocities; leapfrog push, dt = 0.1/omega_p; FP32
+  push with int32 cell + FP32 offset; FP32 V(2,2) multigrid inside FP64
+  refinement to 1e-8 relative residual.
+
+One step = rho from the exact charge accumulators -> multigrid solve -> fused
+gather/push/boundary/deposit -> stable re-sort by cell (every
+--sort-interval steps).  Inputs are larger than L2, so no flush is needed.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs independent replicas (one per GPU, different seeds): the path has
+no data-path exchange between GPUs.  `--impl reference` times the CPU
+restatement of PSuM's algorithm (oracle/, FP64, OpenMP on all host cores) on
+a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CELLS = 1024
+PPC = 256
+DT = 0.1
+MASS_RATIO = 1836.0
+SEED = 20261203 + 2
+MG_OPTIONS = (f"I {CELLS + 1} J {CELLS + 1} K 1 depth 6 pre_relax 2 post_relax 2 max_cycles 16 "
+              f"correction_interval 4 tol 1e-8")
+BYTES_PER_PARTICLE = 24          # int32 cell + 2 FP32 offsets + 3 FP32 velocities (2D3V mixed)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ppc", type=int, default=PPC, help="particles per cell per species")
+    ap.add_argument("--cells", type=int, default=CELLS)
+    ap.add_argument("--sort-interval", type=int, default=1)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=1 << 21, help="particles in the CPU baseline sample")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- helpers --
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=self.file,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.file is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def make_species_device(torch, gen, n, cells, vth, device):
+    pos = torch.rand((2, n), generator=gen, device=device, dtype=torch.float64) * cells
+    vel = torch.randn((3, n), generator=gen, device=device, dtype=torch.float64) * vth
+    return pos, vel
+
+
+def build_problem(torch, P, cells, ppc, seed, device, sort_interval):
+    """Context + solver for the bounded two-species plasma; particles are
+    returned (device FP64 SoA) but not loaded."""
+    n = cells * cells * ppc
+    w = 1.0 / ppc
+    ctx = P.ParticleContext((cells, cells), (0.0, 0.0), (float(cells), float(cells)), (0, 0), P.MIXED)
+    ctx.set_options(f"sort_interval {sort_interval}")
+    e = ctx.add_species(-1.0, 1.0, w, n)
+    i = ctx.add_species(1.0, MASS_RATIO, w, n)
+    grid = P.simple_grid((0.0, 0.0), (float(cells), float(cells)), (cells, cells))
+    ps = P.Poisson_solver_2d()
+    opts = MG_OPTIONS.replace(f"I {CELLS + 1} J {CELLS + 1}", f"I {cells + 1} J {cells + 1}")
+    ps.set_options(opts)
+    ps.init("cuda_multigrid32f_gpu", grid, P.Poisson_solver_2d.Cartesian,
+            [P.Dirichlet_line(grid, d, 0.0) for d in "NSEW"], 1.0)
+    ps.make_righthand_item()
+    return ctx, (e, i), ps, n, w
+
+
+def roofline_block(push_ms_per_step, n_total, peak, peak_kind, traffic):
+    algo = n_total * 2 * BYTES_PER_PARTICLE
+    achieved = algo / (push_ms_per_step * 1e-3) / 1e9
+    return {"bound": "hbm", "kernel": "k_push_mixed (gather+push+boundary+deposit, both species)",
+            "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "peak_kind": peak_kind, "algorithmic_bytes_per_step": algo, "traffic": traffic}
+
+
+# ------------------------------------------------------------ CPU baseline --
+def cpu_baseline(cells, ppc, sample):
+    """Times the FP64 CPU restatement (oracle/) on `sample` particles of each
+    species over the full grid: deposit + multigrid solve + push.  The
+    particle part scales linearly with the particle count, so the full-step
+    time is t_solve + t_particles * (N_full / sample)."""
+    import numpy as np
+    from oracle import oracle as O
+    from psum_b200.field_solver import Dirichlet_line, simple_grid
+    rng = np.random.default_rng(SEED)
+    g = O.make_grid((cells, cells), (0.0, 0.0), (float(cells), float(cells)), (0, 0))
+    grid = simple_grid((0.0, 0.0), (float(cells), float(cells)), (cells, cells))
+    fixed = np.unique(np.concatenate([Dirichlet_line(grid, d, 0.0)[0] for d in "NSEW"]))
+    r, c, v = O.poisson_assemble((cells, cells), (0, 0), (cells, cells), 1.0, fixed)
+    nn = (cells + 1) ** 2
+    mg = O.Multigrid(r, c, v, nn, cells + 1, cells + 1, 1, 6)
+    w = 1.0 / ppc
+    species = []
+    for q, m, vth in ((-1.0, 1.0, 1.0), (1.0, MASS_RATIO, 1.0 / np.sqrt(MASS_RATIO))):
+        pos = rng.uniform(0.0, cells, size=(2, sample))
+        vel = rng.normal(0.0, vth, size=(3, sample))
+        species.append((q, m, pos, vel))
+    t0 = time.perf_counter()
+    rho = np.ones(nn) * 0.0
+    for q, m, pos, vel in species:
+        rho += O.deposit(g, pos, q * w, nn)
+    t_dep = time.perf_counter() - t0
+    b = rho.copy()
+    b[fixed.astype(np.int64)] = 0.0
+    t0 = time.perf_counter()
+    phi, hist = mg.solve_mixed(b, np.zeros(nn), 16, 4, 2, 2)
+    t_solve = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for q, m, pos, vel in species:
+        O.push(g, pos, vel, phi, q / m, DT)
+    t_push = time.perf_counter() - t0
+    n_full = 2 * cells * cells * ppc
+    t_full = t_solve + (t_dep + t_push) * (n_full / (2 * sample))
+    return {"value": n_full / t_full, "unit": "particle-steps/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": (f"{2 * sample} particles (2 species) on the full {cells}x{cells} grid: deposit "
+                       f"{t_dep:.3f}s + mixed-precision MG solve {t_solve:.3f}s + push {t_push:.3f}s; "
+                       f"particle part scaled to {n_full} particles"),
+            "t_step_full_s": t_full}
+
+
+# --------------------------------------------------------------- main arm --
+def run_ours(args, rank, world, dist):
+    import numpy as np
+    import torch
+
+    import psum_b200 as P
+    torch.cuda.set_device(rank % torch.cuda.device_count())
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.Stream()
+    cells, ppc = args.cells, args.ppc
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(SEED + 1000 * rank)
+
+    ctx, (e, i), ps, n, w = build_problem(torch, P, cells, ppc, SEED + rank, dev, args.sort_interval)
+    ctx.set_stream(stream)
+    nn = (cells + 1) ** 2
+    rho = torch.zeros(nn, dtype=torch.float64, device=dev)
+    phi = torch.zeros(nn, dtype=torch.float64, device=dev)
+    vth_i = 1.0 / np.sqrt(MASS_RATIO)
+    for sp, vth in ((e, 1.0), (i, vth_i)):
+        pos, vel = make_species_device(torch, gen, n, cells, vth, dev)
+        ctx.load(sp, pos, vel)
+        del pos, vel
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    ctx.sort()
+    ctx.deposit()
+
+    def step():
+        ctx.step(ps.backend, 0.0, rho, phi, DT)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ctx.get_timing(reset=True)
+    ctx.set_timing(True)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = P.lib().psum_kernel_launches()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        with torch.cuda.stream(stream):
+            start.record(stream)
+            for _ in range(args.steps):
+                step()
+            stop.record(stream)
+        torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    launches = P.lib().psum_kernel_launches() - launches0
+    ms = start.elapsed_time(stop)
+    phases = ctx.get_timing(reset=True)
+    ctx.set_timing(False)
+    stats = ps.backend.last_stats()
+    n_valid = sum(ctx.count(sp)[1] for sp in (e, i))
+    diag = ctx.diagnostics(phi, 1.0)
+    clocks = clk.summary()
+
+    ms_max = ms
+    if dist is not None:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, torch, P, dev, rank, dist)
+
+    if rank != 0:
+        return None
+    n_total = 2 * n
+    value = n_total * world * args.steps / (ms_max * 1e-3)
+    peak, peak_kind = measured_peaks()
+    push_ms = phases["push"][0] / max(phases["push"][1], 1)
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "push_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get("bytes_per_step")
+    line = {
+        "metric": "particle-steps/s incl. Poisson MG, mixed-prec vs FP64 on GPU at stated error",
+        "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 push / f32-in-f64 MG", "data": "synthetic",
+        "config": {"workload": "2D bounded two-species plasma, mixed precision",
+                   "grid_cells": [cells, cells], "particles": n_total, "ppc_per_species": ppc,
+                   "mass_ratio": MASS_RATIO, "dt": DT, "mg": MG_OPTIONS, "sort_interval": args.sort_interval,
+                   "parallelism": "replicas" if world > 1 else "single GPU",
+                   "l2_policy": "inputs larger than L2 (state 12.9 GB)"},
+        "roofline": roofline_block(push_ms, n_total, peak, peak_kind, traffic),
+        "phase_ms_per_step": {k: round(v[0] / max(v[1], 1), 4) for k, v in phases.items()},
+        "step_roofline_frac": round((n_total * 2 * BYTES_PER_PARTICLE) / (ms_max / args.steps * 1e-3) / 1e9 / peak, 4),
+        "mg_last_solve": stats, "valid_particles_end": n_valid, "charge_end": diag["charge"],
+        "gpu_launches": int(launches), "clocks": clocks,
+    }
+    if e2e is not None:
+        line["e2e"] = e2e
+    if not args.no_cpu_baseline:
+        cb = cpu_baseline(cells, ppc, args.cpu_sample)
+        cb.pop("t_step_full_s", None)
+        line["cpu_baseline"] = cb
+    return line
+
+
+def run_e2e(args, torch, P, dev, rank, dist):
+    """The same job end to end through the C ABI from pinned host buffers:
+    H2D of the initial particle state (FP64 SoA, as PSuM's particles are
+    FP64), then K steps, each followed by a D2H read of the loss counters,
+    then a D2H read of phi."""
+    import numpy as np
+    cells, ppc = args.cells, args.ppc
+    n = cells * cells * ppc
+    need = 2 * n * 5 * 8
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+    except Exception:
+        avail = 0
+    if avail and avail < 1.5 * need:
+        return {"value": None, "unit": "particle-steps/s",
+                "skipped": f"host RAM {avail / 1e9:.0f} GB < 1.5 x {need / 1e9:.0f} GB pinned input"}
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(SEED + 7 + 1000 * rank)
+    host = []
+    for vth in (1.0, 1.0 / np.sqrt(MASS_RATIO)):
+        pos, vel = make_species_device(torch, gen, n, cells, vth, dev)
+        hp = torch.empty(pos.shape, dtype=torch.float64, pin_memory=True)
+        hv = torch.empty(vel.shape, dtype=torch.float64, pin_memory=True)
+        hp.copy_(pos)
+        hv.copy_(vel)
+        del pos, vel
+        host.append((hp, hv))
+    torch.cuda.synchronize()
+    ctx, (e, i), ps, n, w = build_problem(torch, P, cells, ppc, SEED + rank, dev, args.sort_interval)
+    nn = (cells + 1) ** 2
+    rho = torch.zeros(nn, dtype=torch.float64, device=dev)
+    phi = torch.zeros(nn, dtype=torch.float64, device=dev)
+    phi_host = torch.empty(nn, dtype=torch.float64, pin_memory=True)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for sp, (hp, hv) in zip((e, i), host):
+        P.check(P.lib().psum_pic_load(ctx.handle, sp, n, hp.data_ptr(), hv.data_ptr()))
+    ctx.sort()
+    ctx.deposit()
+    losses_total = 0
+    for _ in range(args.steps):
+        ctx.step(ps.backend, 0.0, rho, phi, DT)
+        losses_total += int(ctx.losses(reset=True).sum())
+    phi_host.copy_(phi)
+    torch.cuda.synchronize()
+    sec = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([sec], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        sec = float(t.item())
+    world = dist.get_world_size() if dist is not None else 1
+    h2d = 2 * n * 5 * 8
+    d2h = args.steps * 2 * 2 * 2 * 8 + nn * 8
+    del ctx, ps, host
+    return {"value": 2 * n * world * args.steps / sec, "unit": "particle-steps/s",
+            "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps,
+            "wall_s": sec, "definition": "whole job: H2D of the FP64 particle state, then K steps with a D2H "
+                                         "of the loss counters after each, then D2H of phi"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return None
+    steps = max(args.steps, 1)
+    vals = []
+    cb = None
+    for _ in range(min(steps, 3)):
+        cb = cpu_baseline(args.cells, args.ppc, args.cpu_sample)
+        vals.append(cb["value"])
+    value = statistics.median(vals)
+    return {"impl": "reference",
+            "metric": "particle-steps/s incl. Poisson MG, mixed-prec vs FP64 on GPU at stated error",
+            "value": value, "unit": "particle-steps/s", "n_gpus": 1, "steps": len(vals), "warmup": 0,
+            "ms_per_step": 1e3 * (2 * args.cells * args.cells * args.ppc) / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "2D bounded two-species plasma, mixed precision",
+                       "grid_cells": [args.cells, args.cells], "particles": 2 * args.cells * args.cells * args.ppc},
+            "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cb["cores"], "kind": "port",
+                             "sample": cb["sample"]},
+            "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "PSuM cannot be built here (needs AdaptiveCpp and Eigen 3.4); this is the FP64 CPU "
+                    "restatement of its algorithm (oracle/) on all host cores"}
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+        if args.impl == "ours":
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", rank)))
+            tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            dist = tdist
+    if args.impl == "reference":
+        line = run_reference(args, rank)
+    else:
+        line = run_ours(args, rank, world, dist)
+    if line is not None:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

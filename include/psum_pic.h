@@ -1,0 +1,155 @@
+/*
+ * psum_pic.h -- C-ABI particle-kernel set of the B200 electrostatic PIC step.
+ *
+ * PSuM has no C ABI on the particle side: its step is header code,
+ * `particle_group<P,Validator>::for_each` plus user lambdas
+ * (src/particle_container/particle_group.hpp:169-221) over AoS
+ * `tagged_struct{position, velocity}` particles, with CIC gather
+ * (`interp_diff`, src/field/device_field.hpp:275-284), CIC deposit
+ * (`add_back`, device_field.hpp:300-310) and cell binning
+ * (src/particle_collision/grid_mapped_device_vector.hpp:47-87).  The
+ * functions below are the plain-pointer entry points a PSuM `particle_group`
+ * / `device_field` adapter binds to run the same step on one B200.
+ *
+ * Semantics kept from the reference:
+ *   - grid: `simple_grid<D>` (src/field/simple_grid.hpp:16-307): node index
+ *     last-dimension-fastest, node count cells+1 per axis, CIC base node
+ *     `cN = floor((p-lo)*dr)`, reference cell key `c2i(nC(p))` with
+ *     `nC = int((p-lo)*dr)` (truncation) for in-grid points only;
+ *   - a periodic axis is PSuM's wrapping-node idiom (application/benchmark/TSI/main.cpp:94):
+ *     `cells` cells between lower and upper, the node lattice wraps at
+ *     cells+1 nodes, so the period is (cells+1)*dx;
+ *   - an invalid (absorbed) particle exports with x = NaN
+ *     (src/particle_container/validator.hpp:19-26);
+ *   - E = -grad of the multilinear interpolant of phi (simple_interpolation.hpp:58-98).
+ *
+ * Layout choices of this implementation (not visible through the ABI):
+ *   - SoA storage, sorted by cell with an int32 key;
+ *   - PSUM_PIC_MIXED: int32 cell index + FP32 in-cell offset per axis,
+ *     FP32 velocity (24 B per 2D3V particle, 28 B per 3D3V particle);
+ *   - PSUM_PIC_FP64: FP64 absolute position and velocity (40 / 48 B);
+ *   - deposition is exact integer (fixed-point) accumulation of per-particle
+ *     CIC weights, so rho does not depend on particle order or thread timing.
+ *
+ * Bulk arguments named *_dev are device pointers; *_host are host pointers.
+ * Every function returns a psum_status (include/psum_field_solver.h).
+ */
+#ifndef PSUM_B200_PIC_H
+#define PSUM_B200_PIC_H
+
+#include "psum_field_solver.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct psum_pic_grid_desc {
+    int dim;            /* 2 or 3 */
+    int cells[3];       /* simple_grid<D>::cell_num */
+    double lower[3];    /* simple_grid<D>::lower_bounds */
+    double upper[3];    /* simple_grid<D>::upper_bounds */
+    int periodic[3];    /* 1: periodic axis (wrapping node lattice); 0: absorbing walls at lower/upper */
+} psum_pic_grid_desc;
+
+typedef struct psum_pic_species_desc {
+    double charge;      /* q */
+    double mass;        /* m */
+    double weight;      /* macro-particle weight; deposit adds weight/cell_volume per particle */
+} psum_pic_species_desc;
+
+enum { PSUM_PIC_MIXED = 0, PSUM_PIC_FP64 = 1 };
+enum { PSUM_PIC_LEAPFROG = 0, PSUM_PIC_BORIS = 1 };
+
+typedef struct psum_pic_ctx psum_pic_ctx;
+
+EXPORT int psum_pic_create(const psum_pic_grid_desc* grid, int precision, psum_pic_ctx** out);
+EXPORT int psum_pic_destroy(psum_pic_ctx* ctx);
+/* Run all later work of this context on `stream` (a cudaStream_t; NULL = own stream). */
+EXPORT int psum_pic_set_stream(psum_pic_ctx* ctx, void* stream);
+/* Options as whitespace `key value` pairs (the solver option grammar):
+ *   sort_interval N   re-sort by cell every N steps (default 1; 0 = never) */
+EXPORT int psum_pic_set_options(psum_pic_ctx* ctx, const char* options);
+
+/* Adds a species able to hold `capacity` particles; *id receives its index. */
+EXPORT int psum_pic_add_species(psum_pic_ctx* ctx, const psum_pic_species_desc* sp,
+                                unsigned long long capacity, int* id);
+/* Replaces the species' particles by `n` particles given as FP64 SoA host
+ * arrays pos_host[d*n+i] (d < dim) and vel_host[c*n+i] (c < 3), in the given
+ * order (no sort).  Particles with non-finite x[0] are loaded as invalid.
+ * Periodic coordinates are wrapped into the period; particles outside an
+ * absorbing axis are loaded as invalid. */
+EXPORT int psum_pic_load(psum_pic_ctx* ctx, int species, unsigned long long n,
+                         const double* pos_host, const double* vel_host);
+/* Same, from FP64 SoA device arrays (no host staging). */
+EXPORT int psum_pic_load_device(psum_pic_ctx* ctx, int species, unsigned long long n,
+                                const double* pos_dev, const double* vel_dev);
+/* Current array length (valid + not yet compacted invalid) and valid count. */
+EXPORT int psum_pic_count(psum_pic_ctx* ctx, int species, unsigned long long* n_stored,
+                          unsigned long long* n_valid);
+/* Copies the species state, in storage order, into FP64 SoA host arrays of
+ * n_stored entries; invalid particles have pos[0] = NaN. */
+EXPORT int psum_pic_get_state(psum_pic_ctx* ctx, int species, double* pos_host, double* vel_host);
+/* Internal cell key per stored particle (row-major over the internal cell
+ * lattice; invalid = -1) into an int32 device array of n_stored entries. */
+EXPORT int psum_pic_get_keys(psum_pic_ctx* ctx, int species, int* keys_dev);
+
+/* Stable counting sort of every species by internal cell key (invalid
+ * particles are dropped: this is also `compress`). */
+EXPORT int psum_pic_sort(psum_pic_ctx* ctx);
+
+/* Reference binning (grid_mapped_device_vector::update, :47-87) of one species:
+ * keys_dev[i] = c2i(nC(p_i)) for in-grid particles, -1 otherwise (int64, n_stored);
+ * counts_dev[c] (uint64, prod(cells)) particles per reference cell;
+ * offsets_dev[c] (uint64, prod(cells)) exclusive prefix of counts;
+ * perm_dev[s] (uint64, n_in_grid) = stored index of the particle in output slot s,
+ * stable: ascending stored index within a cell.  *n_in_grid is returned. */
+EXPORT int psum_pic_bin(psum_pic_ctx* ctx, int species, long long* keys_dev, unsigned long long* counts_dev,
+                        unsigned long long* offsets_dev, unsigned long long* perm_dev,
+                        unsigned long long* n_in_grid);
+
+/* Recomputes the charge accumulators from the current positions (CIC). */
+EXPORT int psum_pic_deposit(psum_pic_ctx* ctx);
+/* rho_dev (FP64 node field) = background + sum_s charge_s*weight_s/cell_volume * n_s. */
+EXPORT int psum_pic_rho(psum_pic_ctx* ctx, double background, double* rho_dev);
+/* Per-species deposited particle count density n_s (no charge/background). */
+EXPORT int psum_pic_density(psum_pic_ctx* ctx, int species, double* n_dev);
+
+/* Gather E = -grad(phi) at every particle, push (leapfrog, or Boris with the
+ * uniform field B[3]), apply the particle boundary, then deposit the new
+ * positions into the charge accumulators.  phi_dev is an FP64 node field.
+ * Absorbed particles become invalid and are counted per species, axis and
+ * side into the context's loss counters (read with psum_pic_get_losses). */
+EXPORT int psum_pic_push(psum_pic_ctx* ctx, const double* phi_dev, double dt, int pusher, const double* B);
+/* losses_host[(s*dim + axis)*2 + side] since the last reset (side 0 = lower wall). */
+EXPORT int psum_pic_get_losses(psum_pic_ctx* ctx, unsigned long long* losses_host, int reset);
+
+/* One full electrostatic step through a solver handle obtained from this
+ * library's func_table (cuda_multigrid32f_gpu / cuda_multigrid64_gpu):
+ *   rho = background + deposited charge  ->  solve A phi = rho  ->  push + deposit
+ *   -> re-sort when due.  phi_dev is the initial guess and the output field;
+ * rho_dev is scratch that receives the right-hand side.  Asynchronous. */
+EXPORT int psum_pic_step(psum_pic_ctx* ctx, psum_field_solver_handle solver, double background,
+                         double* rho_dev, double* phi_dev, double dt, int pusher, const double* B);
+
+/* Per-phase CUDA-event timing of psum_pic_step on the context's stream.
+ * Phases: 0 rho, 1 Poisson solve, 2 gather+push+deposit, 3 sort.
+ * get_timing returns accumulated milliseconds and phase executions since the
+ * last reset (synchronises the stream). */
+EXPORT int psum_pic_set_timing(psum_pic_ctx* ctx, int enable);
+EXPORT int psum_pic_get_timing(psum_pic_ctx* ctx, double* ms_host, int* count_host, int reset);
+
+/* FP64 diagnostics (fixed-order reductions): out_host[s] = kinetic energy of
+ * species s (sum 0.5*m*w*|v|^2); out_host[ns] = field energy
+ * 0.5*eps*sum over edges (dphi/dx)^2 * cell_volume; out_host[ns+1] = total
+ * deposited charge sum_s q_s w_s N_s (exact from the integer accumulators). */
+EXPORT int psum_pic_diagnostics(psum_pic_ctx* ctx, const double* phi_dev, double epsilon, double* out_host);
+
+/* Error word of the device-side checks since the last call (bit set per
+ * psum_status code: non-finite state, overflow, key out of range); resets it. */
+EXPORT int psum_pic_device_errors(psum_pic_ctx* ctx, unsigned int* flags);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PSUM_B200_PIC_H */

@@ -1,0 +1,15 @@
+"""psum_b200 -- B200 (sm_100a) electrostatic PIC step behind PSuM's plugin ABI.
+
+Native library: ``libpsum_b200.so`` (built in-tree by ``psum_b200.build``),
+exporting the solver plugin ABI of include/psum_field_solver.h and the
+particle-kernel set of include/psum_pic.h.  The Python modules are thin
+ctypes mirrors of the reference interfaces; there is no CPU fallback.
+"""
+from ._lib import LIB_PATH, PROTOTYPES, PsumError, check, lib
+from .field_solver import (Dirichlet_line, Dirichlet_nodes, Dirichlet_plane, Poisson_solver_2d, Poisson_solver_3d,
+                           assemble_poisson, registered_table, simple_grid, solver_backend)
+from .pic import BORIS, FP64, LEAPFROG, MIXED, ParticleContext
+
+__all__ = ["LIB_PATH", "PROTOTYPES", "PsumError", "check", "lib", "Dirichlet_line", "Dirichlet_nodes",
+           "Dirichlet_plane", "Poisson_solver_2d", "Poisson_solver_3d", "assemble_poisson", "registered_table",
+           "simple_grid", "solver_backend", "ParticleContext", "MIXED", "FP64", "LEAPFROG", "BORIS"]

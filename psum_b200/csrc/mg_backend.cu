@@ -1,0 +1,566 @@
+// mg_backend.cu -- the B200 multigrid solver backends behind PSuM's func_table.
+//
+//   cuda_multigrid32f_gpu : FP32 V-cycles inside FP64 iterative refinement,
+//                           restating sycl_multigrid32f_gpu::solve
+//                           (src/field_solver/implements/sycl_multigrid32f_gpu.cpp:106-160)
+//   cuda_multigrid64_gpu  : FP64 V-cycles with the caller's x as initial guess,
+//                           restating cuda_multigrid_gpu::solve
+//                           (src/field_solver/implements/cuda_multigrid_gpu.cu:140-180)
+//
+// Both accept PSuM's option grammar (sycl_multigrid32f_gpu.cpp:162-196) and
+// add `tol` (stop once ||b - A x||_2 <= tol ||b||_2, checked on the device
+// every correction_interval cycles; 0 = run exactly max_cycles like PSuM),
+// `max_coarse`, and `periodic_I/J/K 1` (wrap-around transfers on that axis
+// for operators whose node lattice wraps, where PSuM's open-interval
+// transfers make the V-cycle diverge).  The whole solve is enqueued on one stream without host
+// synchronisation; func_table.solve synchronises at the end, like PSuM.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "common.hpp"
+#include "mg_backend.hpp"
+#include "mg_host.hpp"
+#include "mg_kernels.cuh"
+
+namespace psum_b200 {
+
+namespace mgdetail {
+
+inline unsigned grid_for(long long n, int threads = kThreads) {
+    return (unsigned)std::max<long long>(1, (n + threads - 1) / threads);
+}
+
+constexpr int kNormBlocks = 296;   // 2 x 148 SMs: fixed grid -> fixed reduction order
+
+template <class T>
+struct DevStencil {
+    StencilDev<T> view{};
+    DevBuf<uint32_t> mask, mask_prefix;
+    DevBuf<int> exc_ptr, exc_col;
+    DevBuf<T> exc_val;
+    long long exceptions = 0;
+
+    void upload(const StencilOp& op, cudaStream_t s) {
+        mask.upload(op.mask.data(), op.mask.size(), s);
+        mask_prefix.upload(op.mask_prefix.data(), op.mask_prefix.size(), s);
+        exc_ptr.upload(op.exc_ptr.data(), op.exc_ptr.size(), s);
+        exc_col.upload(op.exc_col.data(), op.exc_col.size(), s);
+        std::vector<T> v(op.exc_val.begin(), op.exc_val.end());
+        exc_val.upload(v.data(), v.size(), s);
+        cuda_check(cudaStreamSynchronize(s), "upload stencil");
+        exceptions = (long long)op.exc_rows.size();
+        view.n0 = op.dims[0];
+        view.n1 = op.dims[1];
+        view.n2 = op.dims[2];
+        view.n = op.n;
+        view.ns = op.ns;
+        for (int t = 0; t < op.ns && t < kMaxTaps; ++t) {
+            view.di[t] = (signed char)op.delta[t][0];
+            view.dj[t] = (signed char)op.delta[t][1];
+            view.dk[t] = (signed char)op.delta[t][2];
+            view.c[t] = T(op.coef[t]);
+        }
+        view.mask = mask.p;
+        view.mask_prefix = mask_prefix.p;
+        view.exc_ptr = exc_ptr.p;
+        view.exc_col = exc_col.p;
+        view.exc_val = exc_val.p;
+    }
+};
+
+template <class T>
+struct DevAxis {
+    DevBuf<int> p_c0, p_c1, r_f;
+    DevBuf<T> p_w0, p_w1, r_w;
+    void upload(const Axis1D& a, cudaStream_t s, AxisDev<T>& view) {
+        std::vector<T> w0(a.p_w0.begin(), a.p_w0.end()), w1(a.p_w1.begin(), a.p_w1.end()),
+            rw(a.r_w.begin(), a.r_w.end());
+        p_c0.upload(a.p_c0.data(), a.p_c0.size(), s);
+        p_c1.upload(a.p_c1.data(), a.p_c1.size(), s);
+        r_f.upload(a.r_f.data(), a.r_f.size(), s);
+        p_w0.upload(w0.data(), w0.size(), s);
+        p_w1.upload(w1.data(), w1.size(), s);
+        r_w.upload(rw.data(), rw.size(), s);
+        cuda_check(cudaStreamSynchronize(s), "upload transfer");
+        view.nf = a.nf;
+        view.nc = a.nc;
+        view.p_c0 = p_c0.p;
+        view.p_c1 = p_c1.p;
+        view.p_w0 = p_w0.p;
+        view.p_w1 = p_w1.p;
+        view.r_f = r_f.p;
+        view.r_w = r_w.p;
+    }
+};
+
+template <class T>
+struct Level {
+    long long n = 0;
+    DevStencil<T> op;
+    DevBuf<T> dinv;
+    DevBuf<T> bufA, bufB, b;   // x ping-pong pair and right-hand side
+    XferDev<T> xfer{};         // to the next coarser level
+    DevAxis<T> axes[3];
+};
+
+}  // namespace mgdetail
+
+using namespace mgdetail;
+
+// ------------------------------------------------------------------------
+struct SolverBase {
+    uint32_t magic = kSolverMagic;
+    int precision = 32;   // 32: mixed refinement, 64: FP64 V-cycles
+    // options (defaults of sycl_multigrid32f_gpu.cpp:28-38)
+    int I = 0, J = 0, K = 0;
+    int depth = 3, pre_relax = 2, post_relax = 1, max_cycles = 10, correction_interval = 4;
+    int max_coarse = 8192;
+    std::array<int, 3> periodic{0, 0, 0};   // wrap-around transfers per axis (option periodic_I/J/K)
+    double tol = 0.0;
+    unsigned long long n_row = 0;
+    bool ready = false;
+    cudaStream_t own_stream = nullptr;
+    // sources (host copies kept, device copies uploaded at set time)
+    std::vector<unsigned long long> rep_idx, add_idx;
+    std::vector<double> rep_val, add_val;
+    DevBuf<unsigned long long> d_rep_idx, d_add_idx;
+    DevBuf<double> d_rep_val, d_add_val;
+    // FP64 fine operator for the residual
+    DevStencil<double> a0;
+    DevBuf<double> dinv0;
+    DevBuf<double> partials;
+    DevBuf<MGState> state;
+    Hierarchy host;   // kept for introspection
+    int levels = 0;
+    unsigned long long coarse_rows = 0;
+
+    virtual ~SolverBase() {
+        if (own_stream) cudaStreamDestroy(own_stream);
+    }
+    virtual void build_device(cudaStream_t s) = 0;
+    virtual void enqueue_solve(double* b, double* x, cudaStream_t s) = 0;
+};
+
+namespace {
+
+template <class T>
+struct Solver : SolverBase {
+    std::vector<std::unique_ptr<Level<T>>> lv;
+    DevBuf<T> coarse_inv;
+    DevBuf<double> x64;   // FP64 level-0 iterate for the FP64 backend
+
+    void build_device(cudaStream_t s) override {
+        a0.upload(host.a0, s);
+        dinv0.upload(host.dinv[0].data(), host.dinv[0].size(), s);
+        partials.alloc(kNormBlocks);
+        state.alloc(1);
+        lv.clear();
+        for (int l = 0; l <= host.L; ++l) {
+            auto L = std::make_unique<Level<T>>();
+            L->n = (long long)host.dims[l][0] * host.dims[l][1] * host.dims[l][2];
+            if (l < host.L) L->op.upload(host.ahat[l], s);
+            std::vector<T> d(host.dinv[l].begin(), host.dinv[l].end());
+            L->dinv.upload(d.data(), d.size(), s);
+            L->bufA.alloc(L->n);
+            L->bufB.alloc(L->n);
+            L->b.alloc(L->n);
+            if (l < host.L)
+                for (int a = 0; a < 3; ++a) L->axes[a].upload(host.xfer[l][a], s, L->xfer.ax[a]);
+            lv.push_back(std::move(L));
+        }
+        std::vector<T> ci(host.coarse_inv.begin(), host.coarse_inv.end());
+        coarse_inv.upload(ci.data(), ci.size(), s);
+        if (precision == 64) x64.alloc(n_row);
+        cuda_check(cudaStreamSynchronize(s), "build_device");
+        levels = host.L + 1;
+        coarse_rows = (unsigned long long)lv.back()->n;
+    }
+
+    // Enqueue `cycles` V(pre,post) cycles on level-0 (x0 in/out, b0 = scaled rhs).
+    // `x_is_zero`: the level-0 iterate starts at zero (first sweep simplified).
+    // Returns the buffer holding the final level-0 iterate.
+    T* enqueue_vcycles(T* x0, T* other0, T* b0, int cycles, bool x_is_zero, cudaStream_t s) {
+        const MGState* st = state.p;
+        const T omega = T(2.0 / 3);
+        const int L = host.L;
+        std::vector<T*> xcur(L + 1), xoth(L + 1), bl(L + 1);
+        xcur[0] = x0;
+        xoth[0] = other0;
+        bl[0] = b0;
+        for (int l = 1; l <= L; ++l) {
+            xcur[l] = lv[l]->bufA.p;
+            xoth[l] = lv[l]->bufB.p;
+            bl[l] = lv[l]->b.p;
+        }
+        std::vector<bool> zero(L + 1, false);
+        zero[0] = x_is_zero;
+        auto smooth = [&](int l) {
+            Level<T>& V = *lv[l];
+            const unsigned g = grid_for(V.n);
+            if (zero[l]) {
+                { k_level_op<T, kSmoothFromZero><<<g, kThreads, 0, s>>>(V.op.view, xcur[l], bl[l], xoth[l], omega, st); count_launch(); }
+                zero[l] = false;
+            } else {
+                { k_level_op<T, kSmooth><<<g, kThreads, 0, s>>>(V.op.view, xcur[l], bl[l], xoth[l], omega, st); count_launch(); }
+            }
+            std::swap(xcur[l], xoth[l]);
+        };
+        for (int c = 0; c < cycles; ++c) {
+            for (int l = 0; l < L; ++l) {
+                for (int k = 0; k < pre_relax; ++k) smooth(l);
+                Level<T>& V = *lv[l];
+                if (zero[l]) {
+                    // x is zero: residual = b; restrict b directly
+                    { k_restrict<T><<<grid_for(lv[l + 1]->n), kThreads, 0, s>>>(V.xfer, bl[l], bl[l + 1], xcur[l + 1],
+                                                                             lv[l + 1]->dinv.p, st); count_launch(); }
+                } else {
+                    { k_level_op<T, kResidual><<<grid_for(V.n), kThreads, 0, s>>>(V.op.view, xcur[l], bl[l], xoth[l],
+                                                                                omega, st); count_launch(); }
+                    { k_restrict<T><<<grid_for(lv[l + 1]->n), kThreads, 0, s>>>(V.xfer, xoth[l], bl[l + 1],
+                                                                             xcur[l + 1], lv[l + 1]->dinv.p, st); count_launch(); }
+                }
+                zero[l + 1] = true;
+            }
+            {
+                const int n = (int)lv[L]->n;
+                { k_dense_mv<T><<<grid_for((long long)n * 32), kThreads, 0, s>>>(coarse_inv.p, bl[L], xcur[L], n, st); count_launch(); }
+                zero[L] = false;
+            }
+            for (int l = L - 1; l >= 0; --l) {
+                if (zero[l]) {
+                    // only possible with pre_relax == 0 on a level that started at zero:
+                    // x_l was never written; the restriction kernel did not zero it.
+                    cuda_check(cudaMemsetAsync(xcur[l], 0, sizeof(T) * lv[l]->n, s), "memset");
+                    zero[l] = false;
+                }
+                { k_prolong_add<T><<<grid_for(lv[l]->n), kThreads, 0, s>>>(lv[l]->xfer, xcur[l + 1], xcur[l], st); count_launch(); }
+                for (int k = 0; k < post_relax; ++k) smooth(l);
+            }
+        }
+        cuda_check(cudaGetLastError(), "multigrid kernel launch");
+        return xcur[0];
+    }
+
+    void enqueue_sources(double* b, cudaStream_t s) {
+        const long long na = (long long)add_idx.size(), nr = (long long)rep_idx.size();
+        if (na > 0) { k_addback<<<grid_for(na), kThreads, 0, s>>>(b, d_add_idx.p, d_add_val.p, na); count_launch(); }
+        if (nr > 0) { k_replace<<<grid_for(nr), kThreads, 0, s>>>(b, d_rep_idx.p, d_rep_val.p, nr); count_launch(); }
+    }
+
+    void enqueue_solve(double* b, double* x, cudaStream_t s) override {
+        const long long n = (long long)n_row;
+        MGState* st = state.p;
+        enqueue_sources(b, s);
+        { k_norm2<<<kNormBlocks, kThreads, 0, s>>>(b, n, partials.p); count_launch(); }
+        { k_check<<<1, 32, 0, s>>>(partials.p, kNormBlocks, st, 0, tol, 0, 0); count_launch(); }
+        Level<T>& F = *lv[0];
+        int cycles_done = 0, refinements = 0;
+        if (precision == 32) {
+            // FP64 refinement around FP32 V-cycles (sycl_multigrid32f_gpu.cpp:137-157)
+            while (cycles_done < max_cycles) {
+                const int batch = std::min(correction_interval, max_cycles - cycles_done);
+                { k_residual64<T><<<kNormBlocks, kThreads, 0, s>>>(a0.view, x, b, dinv0.p, F.b.p, partials.p, st, 1); count_launch(); }
+                { k_check<<<1, 32, 0, s>>>(partials.p, kNormBlocks, st, 1, tol, cycles_done, refinements); count_launch(); }
+                T* e = enqueue_vcycles(F.bufA.p, F.bufB.p, F.b.p, batch, /*x_is_zero=*/true, s);
+                { k_correct<T><<<grid_for(n), kThreads, 0, s>>>(x, e, n, st); count_launch(); }
+                cycles_done += batch;
+                ++refinements;
+            }
+        } else {
+            cuda_check(cudaMemcpyAsync(x64.p, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, s), "copy x");
+            { k_scale<T><<<grid_for(n), kThreads, 0, s>>>(b, dinv0.p, F.b.p, n); count_launch(); }
+            double* xc = x64.p;
+            double* xo = reinterpret_cast<double*>(F.bufB.p);
+            while (cycles_done < max_cycles) {
+                const int batch = tol > 0 ? std::min(correction_interval, max_cycles - cycles_done) : max_cycles;
+                if (tol > 0) {
+                    { k_residual64<double><<<kNormBlocks, kThreads, 0, s>>>(a0.view, xc, b, nullptr, (double*)nullptr,
+                                                                          partials.p, st, 1); count_launch(); }
+                    { k_check<<<1, 32, 0, s>>>(partials.p, kNormBlocks, st, 1, tol, cycles_done, refinements); count_launch(); }
+                }
+                T* r = enqueue_vcycles(reinterpret_cast<T*>(xc), reinterpret_cast<T*>(xo), F.b.p, batch, false, s);
+                if ((double*)r != xc) std::swap(xc, xo);
+                cycles_done += batch;
+            }
+            cuda_check(cudaMemcpyAsync(x, xc, sizeof(double) * n, cudaMemcpyDeviceToDevice, s), "copy x");
+        }
+        { k_residual64<double><<<kNormBlocks, kThreads, 0, s>>>(a0.view, x, b, nullptr, (double*)nullptr, partials.p, st, 0); count_launch(); }
+        { k_check<<<1, 32, 0, s>>>(partials.p, kNormBlocks, st, 2, tol, cycles_done, refinements); count_launch(); }
+        cuda_check(cudaGetLastError(), "solve launch");
+    }
+};
+
+int parse_int(std::istringstream& iss, const std::string& key) {
+    int v;
+    if (!(iss >> v)) throw std::invalid_argument("set_options: option '" + key + "' needs an integer value");
+    return v;
+}
+
+}  // namespace
+
+SolverBase* solver_from_handle(void* h) {
+    SolverBase* s = static_cast<SolverBase*>(h);
+    if (!s || s->magic != kSolverMagic) throw Error(PSUM_ERR_INVALID_ARGUMENT, "not a handle of this library");
+    return s;
+}
+
+cudaStream_t solver_stream(SolverBase* s) { return s->own_stream; }
+
+SolverBase* create_solver(int precision) {
+    SolverBase* s = precision == 64 ? static_cast<SolverBase*>(new Solver<double>())
+                                    : static_cast<SolverBase*>(new Solver<float>());
+    s->precision = precision;
+    return s;   // the CUDA stream is created on first device use (set_matrix)
+}
+
+static void ensure_stream(SolverBase* s) {
+    if (!s->own_stream)
+        cuda_check(cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+}
+
+void solver_set_options(SolverBase* s, const char* options) {
+    if (!options) throw std::invalid_argument("set_options: null option string");
+    std::istringstream iss(options);
+    std::string key;
+    bool k_provided = false;
+    while (iss >> key) {
+        if (key == "I") s->I = parse_int(iss, key);
+        else if (key == "J") s->J = parse_int(iss, key);
+        else if (key == "K") {
+            s->K = parse_int(iss, key);
+            k_provided = true;
+        } else if (key == "depth") s->depth = parse_int(iss, key);
+        else if (key == "pre_relax") s->pre_relax = parse_int(iss, key);
+        else if (key == "post_relax") s->post_relax = parse_int(iss, key);
+        else if (key == "max_cycles") s->max_cycles = parse_int(iss, key);
+        else if (key == "max_coarse") s->max_coarse = parse_int(iss, key);
+        else if (key == "periodic_I") s->periodic[0] = parse_int(iss, key) != 0;
+        else if (key == "periodic_J") s->periodic[1] = parse_int(iss, key) != 0;
+        else if (key == "periodic_K") s->periodic[2] = parse_int(iss, key) != 0;
+        else if (key == "correction_interval") {
+            int v = 0;
+            if (!(iss >> v) || v < 1) throw std::invalid_argument("correction_interval must be positive");
+            s->correction_interval = v;
+        } else if (key == "tol") {
+            double v;
+            if (!(iss >> v) || !(v >= 0)) throw std::invalid_argument("tol must be a non-negative number");
+            s->tol = v;
+        } else if (key.rfind("num_conv", 0) == 0 || key == "num_threads") {
+            parse_int(iss, key);   // PSuM tuning keys: accepted and ignored
+        }
+        // other unknown keys are skipped like PSuM's parser does
+    }
+    if (!k_provided) s->K = 1;
+    if (s->pre_relax < 0 || s->post_relax < 0 || s->max_cycles < 0 || s->depth < 1)
+        throw std::invalid_argument("set_options: negative relax/cycle counts or depth < 1");
+}
+
+void solver_set_matrix(SolverBase* s, unsigned long long n_row, unsigned long long n_col, unsigned long long nnz,
+                       const unsigned long long* rows, const unsigned long long* cols, const double* vals) {
+    if (n_row != n_col) throw std::invalid_argument("set_matrix: matrix must be square");
+    HostCSR A = csr_from_coo((long long)n_row, (long long)n_col, (long long)nnz, rows, cols, vals);
+    s->host = build_hierarchy(A, s->I, s->J, s->K, s->depth, s->max_coarse, s->periodic);
+    s->n_row = n_row;
+    ensure_stream(s);
+    s->build_device(s->own_stream);
+    s->ready = true;
+}
+
+static void upload_sources(SolverBase* s) {
+    ensure_stream(s);
+    s->d_rep_idx.upload(s->rep_idx.data(), s->rep_idx.size(), s->own_stream);
+    s->d_rep_val.upload(s->rep_val.data(), s->rep_val.size(), s->own_stream);
+    s->d_add_idx.upload(s->add_idx.data(), s->add_idx.size(), s->own_stream);
+    s->d_add_val.upload(s->add_val.data(), s->add_val.size(), s->own_stream);
+    cuda_check(cudaStreamSynchronize(s->own_stream), "upload sources");
+}
+
+void solver_set_source(SolverBase* s, bool replace, unsigned long long n, const unsigned long long* idx,
+                       const double* v) {
+    if (n > 0 && (!idx || !v)) throw std::invalid_argument("set_source: null array");
+    if (s->ready)
+        for (unsigned long long i = 0; i < n; ++i)
+            if (idx[i] >= s->n_row) throw std::invalid_argument("set_source: index out of range");
+    if (replace) {
+        s->rep_idx.assign(idx, idx + n);
+        s->rep_val.assign(v, v + n);
+    } else {
+        s->add_idx.assign(idx, idx + n);
+        s->add_val.assign(v, v + n);
+    }
+    upload_sources(s);
+}
+
+void solver_solve_async(SolverBase* s, double* b, double* x, cudaStream_t stream) {
+    if (!s->ready) throw Error(PSUM_ERR_NOT_READY, "solve called before set_matrix");
+    if (!b || !x) throw std::invalid_argument("solve: null device pointer");
+    for (auto i : s->rep_idx)
+        if (i >= s->n_row) throw std::invalid_argument("set_source_replace: index out of range");
+    for (auto i : s->add_idx)
+        if (i >= s->n_row) throw std::invalid_argument("set_source_addback: index out of range");
+    s->enqueue_solve(b, x, stream ? stream : s->own_stream);
+}
+
+MGState solver_read_state(SolverBase* s, cudaStream_t stream) {
+    MGState st{};
+    cuda_check(cudaMemcpyAsync(&st, s->state.p, sizeof(MGState), cudaMemcpyDeviceToHost,
+                               stream ? stream : s->own_stream),
+               "read state");
+    cuda_check(cudaStreamSynchronize(stream ? stream : s->own_stream), "read state sync");
+    return st;
+}
+
+void solver_destroy(SolverBase* s) {
+    if (s->own_stream) cudaStreamSynchronize(s->own_stream);
+    s->magic = 0;
+    delete s;
+}
+
+}  // namespace psum_b200
+
+// ===================================================================== ABI ==
+using namespace psum_b200;
+
+namespace {
+
+template <int P>
+psum_field_solver_handle ft_init() {
+    return create_solver(P);
+}
+
+void ft_set_matrix(psum_field_solver_handle h, unsigned long long n_row, unsigned long long n_col,
+                   unsigned long long nnz, unsigned long long* rows, unsigned long long* cols, double* vals) {
+    solver_set_matrix(solver_from_handle(h), n_row, n_col, nnz, rows, cols, vals);
+}
+
+void ft_solve(psum_field_solver_handle h, double* b, double* x) {
+    SolverBase* s = solver_from_handle(h);
+    solver_solve_async(s, b, x, s->own_stream);
+    cuda_check(cudaStreamSynchronize(s->own_stream), "solve sync");
+    MGState st = solver_read_state(s, s->own_stream);
+    if (st.status == PSUM_ERR_DIVERGED) throw Error(PSUM_ERR_DIVERGED, "multigrid: residual diverged");
+}
+
+void ft_set_options(psum_field_solver_handle h, const char* o) { solver_set_options(solver_from_handle(h), o); }
+
+void ft_set_source_replace(psum_field_solver_handle h, unsigned long long n, unsigned long long* idx, double* v) {
+    solver_set_source(solver_from_handle(h), true, n, idx, v);
+}
+
+void ft_set_source_addback(psum_field_solver_handle h, unsigned long long n, unsigned long long* idx, double* v) {
+    solver_set_source(solver_from_handle(h), false, n, idx, v);
+}
+
+void ft_free(psum_field_solver_handle h) {
+    if (h) solver_destroy(solver_from_handle(h));
+}
+
+// Static registration, as the reference backends do (sycl_multigrid32f_gpu.cpp:255-266).
+int register_backends() {
+    func_table t32{ft_init<32>, ft_set_matrix, ft_solve, ft_set_options, ft_set_source_replace, ft_set_source_addback,
+                   ft_free};
+    func_table t64{ft_init<64>, ft_set_matrix, ft_solve, ft_set_options, ft_set_source_replace, ft_set_source_addback,
+                   ft_free};
+    register_solver("cuda_multigrid32f_gpu", t32);
+    register_solver("cuda_multigrid64_gpu", t64);
+    return 0;
+}
+const int g_registered = register_backends();
+
+}  // namespace
+
+extern "C" {
+
+EXPORT int psum_mg_create(const char* kind, psum_field_solver_handle* out) {
+    return guarded([&] {
+        if (!out) throw std::invalid_argument("psum_mg_create: null output");
+        *out = nullptr;
+        func_table t = get_solver_funcs(kind ? kind : "");
+        if (!t.init) throw std::invalid_argument(std::string("unknown solver backend: ") + (kind ? kind : "(null)"));
+        *out = t.init();
+        if (!*out) throw Error(PSUM_ERR_INTERNAL, "failed to create solver.");
+    });
+}
+
+EXPORT int psum_mg_set_options(psum_field_solver_handle h, const char* options) {
+    return guarded([&] { solver_set_options(solver_from_handle(h), options); });
+}
+
+EXPORT int psum_mg_set_matrix(psum_field_solver_handle h, unsigned long long n_row, unsigned long long n_col,
+                              unsigned long long nnz, const unsigned long long* rows, const unsigned long long* cols,
+                              const double* vals) {
+    return guarded([&] { solver_set_matrix(solver_from_handle(h), n_row, n_col, nnz, rows, cols, vals); });
+}
+
+EXPORT int psum_mg_set_source_replace(psum_field_solver_handle h, unsigned long long n, const unsigned long long* idx,
+                                      const double* values) {
+    return guarded([&] { solver_set_source(solver_from_handle(h), true, n, idx, values); });
+}
+
+EXPORT int psum_mg_set_source_addback(psum_field_solver_handle h, unsigned long long n, const unsigned long long* idx,
+                                      const double* values) {
+    return guarded([&] { solver_set_source(solver_from_handle(h), false, n, idx, values); });
+}
+
+EXPORT int psum_mg_solve(psum_field_solver_handle h, double* b_dev, double* x_dev) {
+    int status = PSUM_OK;
+    int rc = guarded([&] {
+        SolverBase* s = solver_from_handle(h);
+        solver_solve_async(s, b_dev, x_dev, s->own_stream);
+        MGState st = solver_read_state(s, s->own_stream);
+        status = st.status;
+    });
+    if (rc != PSUM_OK) return rc;
+    if (status == PSUM_ERR_NOT_CONVERGED) set_last_error("multigrid: tol not reached within max_cycles");
+    if (status == PSUM_ERR_DIVERGED) set_last_error("multigrid: residual diverged");
+    return status;
+}
+
+EXPORT int psum_mg_solve_async(psum_field_solver_handle h, double* b_dev, double* x_dev, void* stream) {
+    return guarded([&] {
+        SolverBase* s = solver_from_handle(h);
+        solver_solve_async(s, b_dev, x_dev, static_cast<cudaStream_t>(stream));
+    });
+}
+
+EXPORT int psum_mg_last_stats(psum_field_solver_handle h, int* cycles, int* refinements, double* rel_residual,
+                              double* initial_rel_residual) {
+    return guarded([&] {
+        SolverBase* s = solver_from_handle(h);
+        if (!s->ready) throw Error(PSUM_ERR_NOT_READY, "no solve has run");
+        cuda_check(cudaDeviceSynchronize(), "stats sync");
+        MGState st = solver_read_state(s, s->own_stream);
+        const double bn = st.bnorm2 > 0 ? std::sqrt(st.bnorm2) : 1.0;
+        if (cycles) *cycles = st.cycles;
+        if (refinements) *refinements = st.refinements;
+        if (rel_residual) *rel_residual = std::sqrt(std::max(0.0, st.rnorm2_last)) / bn;
+        if (initial_rel_residual) *initial_rel_residual = std::sqrt(std::max(0.0, st.rnorm2_first)) / bn;
+    });
+}
+
+EXPORT int psum_mg_hierarchy_info(psum_field_solver_handle h, int* levels, unsigned long long* coarse_rows,
+                                  unsigned long long* exception_rows_level0) {
+    return guarded([&] {
+        SolverBase* s = solver_from_handle(h);
+        if (!s->ready) throw Error(PSUM_ERR_NOT_READY, "set_matrix has not been called");
+        if (levels) *levels = s->levels;
+        if (coarse_rows) *coarse_rows = s->coarse_rows;
+        if (exception_rows_level0) *exception_rows_level0 = s->host.ahat[0].exc_rows.size();
+    });
+}
+
+EXPORT int psum_mg_destroy(psum_field_solver_handle h) {
+    return guarded([&] {
+        if (h) solver_destroy(solver_from_handle(h));
+    });
+}
+
+}  // extern "C"

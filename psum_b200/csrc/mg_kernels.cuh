@@ -1,0 +1,330 @@
+// mg_kernels.cuh -- sm_100a multigrid kernels of the B200 solver backend.
+//
+// Every level operator is a constant stencil (<= 27 taps with periodic wrap
+// on the level's node box) plus an exception CSR for the rows that differ
+// (mg_host.hpp).  All kernels are HBM-bound streaming kernels: one row per
+// thread, coalesced along the last (fastest) dimension; neighbour rows are
+// re-read through L1/L2.  Kernels in the V-cycle return immediately once the
+// solve's device-side `done` flag is set, so a fixed launch schedule can stop
+// early without a host round trip.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/psum_field_solver.h"
+
+namespace psum_b200 {
+
+constexpr int kMaxTaps = 27;
+constexpr int kThreads = 256;
+
+struct MGState {
+    double bnorm2;          // ||b||^2 after the source fix-ups
+    double rnorm2_first;    // ||b - A x||^2 at the first check
+    double rnorm2_last;     // ||b - A x||^2 at the last check
+    int done;               // 1: converged (or diverged) -> gated kernels skip
+    int cycles;             // V-cycles run before `done` was raised / in total
+    int refinements;        // refinement steps run
+    int status;             // psum_status of the solve
+};
+
+template <class T>
+struct StencilDev {
+    int n0, n1, n2;
+    long long n;
+    int ns;
+    signed char di[kMaxTaps], dj[kMaxTaps], dk[kMaxTaps];
+    T c[kMaxTaps];
+    const uint32_t* mask;
+    const uint32_t* mask_prefix;
+    const int* exc_ptr;
+    const int* exc_col;
+    const T* exc_val;
+};
+
+template <class T>
+struct AxisDev {
+    int nf, nc;
+    const int* p_c0;
+    const int* p_c1;
+    const T* p_w0;
+    const T* p_w1;
+    const int* r_f;   // stride 3
+    const T* r_w;     // stride 3
+};
+
+template <class T>
+struct XferDev {
+    AxisDev<T> ax[3];
+};
+
+__device__ __forceinline__ int wrap_idx(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+// (A x)_r for one row of a stencil operator; Acc is the accumulation type.
+template <class T, class Acc>
+__device__ __forceinline__ Acc stencil_row(const StencilDev<T>& A, const T* __restrict__ x, long long r) {
+    const uint32_t word = __ldg(A.mask + (r >> 5));
+    const uint32_t bit = 1u << (r & 31);
+    Acc s = Acc(0);
+    if (word & bit) {
+        const int q = (int)__ldg(A.mask_prefix + (r >> 5)) + __popc(word & (bit - 1u));
+        const int b = __ldg(A.exc_ptr + q), e = __ldg(A.exc_ptr + q + 1);
+        for (int k = b; k < e; ++k) s += Acc(__ldg(A.exc_val + k)) * Acc(__ldg(x + __ldg(A.exc_col + k)));
+        return s;
+    }
+    const long long n12 = (long long)A.n1 * A.n2;
+    const int i = (int)(r / n12);
+    const long long rem = r - (long long)i * n12;
+    const int j = (int)(rem / A.n2);
+    const int k = (int)(rem - (long long)j * A.n2);
+#pragma unroll 1
+    for (int t = 0; t < A.ns; ++t) {
+        const int ii = wrap_idx(i + A.di[t], A.n0);
+        const int jj = wrap_idx(j + A.dj[t], A.n1);
+        const int kk = wrap_idx(k + A.dk[t], A.n2);
+        s += Acc(A.c[t]) * Acc(__ldg(x + ((long long)ii * A.n1 + jj) * A.n2 + kk));
+    }
+    return s;
+}
+
+enum SmoothMode { kSmooth = 0, kSmoothFromZero = 1, kResidual = 2 };
+
+// kSmooth:          out = x + w (b - A x)      (damped Jacobi on the scaled system)
+// kSmoothFromZero:  out = w b                  (first sweep from x = 0)
+// kResidual:        out = b - A x
+template <class T, int Mode>
+__global__ void __launch_bounds__(kThreads) k_level_op(StencilDev<T> A, const T* __restrict__ x,
+                                                       const T* __restrict__ b, T* __restrict__ out, T omega,
+                                                       const MGState* __restrict__ st) {
+    if (st->done) return;
+    const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= A.n) return;
+    if (Mode == kSmoothFromZero) {
+        out[r] = omega * b[r];
+        return;
+    }
+    const T ax = stencil_row<T, T>(A, x, r);
+    if (Mode == kSmooth) out[r] = x[r] + omega * (b[r] - ax);
+    else out[r] = b[r] - ax;
+}
+
+// b_c = dinv_c * (R r_f), x_c = 0
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_restrict(XferDev<T> X, const T* __restrict__ rf, T* __restrict__ bc,
+                                                       T* __restrict__ xc, const T* __restrict__ dinv_c,
+                                                       const MGState* __restrict__ st) {
+    if (st->done) return;
+    const int nc0 = X.ax[0].nc, nc1 = X.ax[1].nc, nc2 = X.ax[2].nc;
+    const int nf1 = X.ax[1].nf, nf2 = X.ax[2].nf;
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long ncount = (long long)nc0 * nc1 * nc2;
+    if (c >= ncount) return;
+    const int ci = (int)(c / ((long long)nc1 * nc2));
+    const long long rem = c - (long long)ci * nc1 * nc2;
+    const int cj = (int)(rem / nc2);
+    const int ck = (int)(rem - (long long)cj * nc2);
+    T s = T(0);
+#pragma unroll
+    for (int qa = 0; qa < 3; ++qa) {
+        const int fi = __ldg(X.ax[0].r_f + 3 * ci + qa);
+        if (fi < 0) continue;
+        const T wi = __ldg(X.ax[0].r_w + 3 * ci + qa);
+#pragma unroll
+        for (int qb = 0; qb < 3; ++qb) {
+            const int fj = __ldg(X.ax[1].r_f + 3 * cj + qb);
+            if (fj < 0) continue;
+            const T wij = wi * __ldg(X.ax[1].r_w + 3 * cj + qb);
+            const T* row = rf + ((long long)fi * nf1 + fj) * nf2;
+#pragma unroll
+            for (int qc = 0; qc < 3; ++qc) {
+                const int fk = __ldg(X.ax[2].r_f + 3 * ck + qc);
+                if (fk < 0) continue;
+                s += (wij * __ldg(X.ax[2].r_w + 3 * ck + qc)) * __ldg(row + fk);
+            }
+        }
+    }
+    bc[c] = s * dinv_c[c];
+    xc[c] = T(0);
+}
+
+// x_f += P x_c
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_prolong_add(XferDev<T> X, const T* __restrict__ xc, T* __restrict__ xf,
+                                                          const MGState* __restrict__ st) {
+    if (st->done) return;
+    const int nf0 = X.ax[0].nf, nf1 = X.ax[1].nf, nf2 = X.ax[2].nf;
+    const int nc1 = X.ax[1].nc, nc2 = X.ax[2].nc;
+    const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nfc = (long long)nf0 * nf1 * nf2;
+    if (f >= nfc) return;
+    const int fi = (int)(f / ((long long)nf1 * nf2));
+    const long long rem = f - (long long)fi * nf1 * nf2;
+    const int fj = (int)(rem / nf2);
+    const int fk = (int)(rem - (long long)fj * nf2);
+    const int ci[2] = {__ldg(X.ax[0].p_c0 + fi), __ldg(X.ax[0].p_c1 + fi)};
+    const int cj[2] = {__ldg(X.ax[1].p_c0 + fj), __ldg(X.ax[1].p_c1 + fj)};
+    const int ck[2] = {__ldg(X.ax[2].p_c0 + fk), __ldg(X.ax[2].p_c1 + fk)};
+    const T wi[2] = {__ldg(X.ax[0].p_w0 + fi), __ldg(X.ax[0].p_w1 + fi)};
+    const T wj[2] = {__ldg(X.ax[1].p_w0 + fj), __ldg(X.ax[1].p_w1 + fj)};
+    const T wk[2] = {__ldg(X.ax[2].p_w0 + fk), __ldg(X.ax[2].p_w1 + fk)};
+    T s = T(0);
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+        if (ci[a] < 0) continue;
+#pragma unroll
+        for (int b2 = 0; b2 < 2; ++b2) {
+            if (cj[b2] < 0) continue;
+#pragma unroll
+            for (int c2 = 0; c2 < 2; ++c2) {
+                if (ck[c2] < 0) continue;
+                s += (wi[a] * wj[b2] * wk[c2]) * __ldg(xc + ((long long)ci[a] * nc1 + cj[b2]) * nc2 + ck[c2]);
+            }
+        }
+    }
+    xf[f] = s + xf[f];
+}
+
+// x = Ainv b (dense, row-major), one warp per row, fixed shuffle tree.
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_dense_mv(const T* __restrict__ Ainv, const T* __restrict__ b,
+                                                       T* __restrict__ x, int n, const MGState* __restrict__ st) {
+    if (st->done) return;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const T* row = Ainv + (long long)warp * n;
+    T s = T(0);
+    for (int c = lane; c < n; c += 32) s += __ldg(row + c) * __ldg(b + c);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) x[warp] = s;
+}
+
+// Block-level FP64 sum in a fixed order (deterministic for a fixed launch).
+__device__ __forceinline__ double block_sum(double v) {
+    __shared__ double sh[kThreads / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += sh[q];
+    return t;   // valid in thread 0
+}
+
+// FP64 residual of the unscaled fine operator: r = b - A x; optional output
+// bhat = TOut(dinv * r) (the FP32 defect of the refinement); per-block
+// partial sums of r^2 (grid-stride, fixed grid -> deterministic).
+template <class TOut>
+__global__ void __launch_bounds__(kThreads) k_residual64(StencilDev<double> A, const double* __restrict__ x,
+                                                         const double* __restrict__ b, const double* __restrict__ dinv,
+                                                         TOut* __restrict__ bhat, double* __restrict__ partials,
+                                                         const MGState* __restrict__ st, int gated) {
+    if (gated && st->done) return;
+    double acc = 0.0;
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < A.n;
+         r += (long long)gridDim.x * blockDim.x) {
+        const double ax = stencil_row<double, double>(A, x, r);
+        const double res = b[r] - ax;
+        acc += res * res;
+        if (bhat) bhat[r] = TOut(dinv[r] * res);
+    }
+    const double t = block_sum(acc);
+    if (threadIdx.x == 0) partials[blockIdx.x] = t;
+}
+
+__global__ void __launch_bounds__(kThreads) k_norm2(const double* __restrict__ v, long long n,
+                                                    double* __restrict__ partials) {
+    double acc = 0.0;
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x)
+        acc += v[r] * v[r];
+    const double t = block_sum(acc);
+    if (threadIdx.x == 0) partials[blockIdx.x] = t;
+}
+
+// bhat = T(dinv * b) (start of an FP64 solve: hadamard_to, multigrid_core.hpp:208)
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_scale(const double* __restrict__ b, const double* __restrict__ dinv,
+                                                    T* __restrict__ out, long long n) {
+    const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < n) out[r] = T(dinv[r] * b[r]);
+}
+
+// x += double(e)  (sycl_multigrid32f_gpu.cpp:153-155)
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_correct(double* __restrict__ x, const T* __restrict__ e, long long n,
+                                                      const MGState* __restrict__ st) {
+    if (st->done) return;
+    const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < n) x[r] += (double)e[r];
+}
+
+__global__ void k_addback(double* __restrict__ b, const unsigned long long* __restrict__ idx,
+                          const double* __restrict__ v, long long n) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) atomicAdd(b + idx[i], v[i]);   // several add-back terms may hit one node, as in cuda_multigrid_gpu.cu:36-44
+}
+
+__global__ void k_replace(double* __restrict__ b, const unsigned long long* __restrict__ idx,
+                          const double* __restrict__ v, long long n) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[idx[i]] = v[i];
+}
+
+// Single-block state update. phase 0: start of solve (partials hold ||b||^2);
+// phase 1: convergence check (partials hold ||r||^2); phase 2: final residual.
+__global__ void k_check(const double* __restrict__ partials, int nparts, MGState* st, int phase, double tol,
+                        int cycles, int refinements) {
+    __shared__ double sh[32];
+    double v = 0.0;
+    // fixed-order two-level sum: thread t sums partials t, t+32, ...
+    if (threadIdx.x < 32) {
+        for (int q = threadIdx.x; q < nparts; q += 32) v += partials[q];
+        sh[threadIdx.x] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    double s = 0.0;
+    for (int q = 0; q < 32; ++q) s += sh[q];
+    if (phase == 0) {
+        st->bnorm2 = s;
+        st->rnorm2_first = -1.0;
+        st->rnorm2_last = -1.0;
+        st->done = 0;
+        st->cycles = 0;
+        st->refinements = 0;
+        st->status = 0;
+        return;
+    }
+    if (phase == 1) {
+        if (st->done) return;
+        if (st->rnorm2_first < 0) st->rnorm2_first = s;
+        st->rnorm2_last = s;
+        st->cycles = cycles;
+        st->refinements = refinements;
+        const double bn = st->bnorm2 > 0 ? st->bnorm2 : 1.0;
+        if (!(s == s) || s > 1e300 || (st->rnorm2_first > 0 && s > 1e12 * st->rnorm2_first)) {
+            st->status = PSUM_ERR_DIVERGED;
+            st->done = 1;
+        } else if (tol > 0 && s <= tol * tol * bn) {
+            st->done = 1;
+        }
+        return;
+    }
+    // phase 2: final
+    if (st->rnorm2_first < 0) st->rnorm2_first = s;
+    st->rnorm2_last = s;
+    if (!st->done) {
+        st->cycles = cycles;
+        st->refinements = refinements;
+    }
+    const double bn = st->bnorm2 > 0 ? st->bnorm2 : 1.0;
+    if (!(s == s) || s > 1e300) st->status = PSUM_ERR_DIVERGED;
+    else if (st->status == 0 && tol > 0 && s > tol * tol * bn) st->status = PSUM_ERR_NOT_CONVERGED;
+}
+
+}  // namespace psum_b200

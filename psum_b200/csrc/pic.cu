@@ -1,0 +1,1444 @@
+// pic.cu -- particle-kernel set of the B200 electrostatic PIC step and its C ABI
+// (include/psum_pic.h).
+//
+// Mixed-precision step per species, one kernel: for every particle read the
+// SoA state with 128-bit loads (4 particles per thread), gather E = -grad phi
+// from FP32 edge differences of the FP64 potential, push (leapfrog or Boris),
+// apply the particle boundary, and deposit the new position as exact
+// fixed-point CIC weights.  Particles are kept sorted by cell with a stable
+// LSD radix sort of the int32 cell key every `sort_interval` steps.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/psum_pic.h"
+#include "common.hpp"
+#include "mg_backend.hpp"
+#include "pic.hpp"
+#include "pic_fp64.hpp"
+
+using psum_b200::DevBuf;
+using psum_b200::Error;
+using psum_b200::GridView;
+using psum_b200::Species;
+using psum_b200::cuda_check;
+
+namespace psum_b200 {
+
+namespace {
+
+inline unsigned blocks_for(long long n, int threads) {
+    return (unsigned)std::max<long long>(1, (n + threads - 1) / threads);
+}
+inline unsigned capped_blocks(long long n_items_per_block_unit, long long n) {
+    const long long b = (n + n_items_per_block_unit - 1) / n_items_per_block_unit;
+    return (unsigned)std::max<long long>(1, std::min<long long>(b, 148LL * 32));
+}
+
+// ------------------------------------------------------------ edge field --
+// edges[node*S + a] = phi(node + e_a) - phi(node) in FP64, stored as FP32
+// (S = 2 in 2-D, 4 in 3-D).  The CIC gradient of PSuM's interp_diff
+// (simple_interpolation.hpp:58-98) is a bilinear/trilinear blend of exactly
+// these differences, so the FP32 gather loses no precision to cancellation.
+template <int D>
+__global__ void k_edges(GridView g, const double* __restrict__ phi, float* __restrict__ edges) {
+    const long long node = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= g.n_nodes) return;
+    const int n12 = g.N[1] * g.N[2];
+    const int i = (int)(node / n12);
+    const int rem = (int)(node - (long long)i * n12);
+    const int j = rem / g.N[2];
+    const int k = rem - j * g.N[2];
+    const double p0 = phi[node];
+    float e[4] = {0.f, 0.f, 0.f, 0.f};
+    const int idx[3] = {i, j, k};
+    for (int a = 0; a < D; ++a) {
+        int q[3] = {idx[0], idx[1], idx[2]};
+        q[a] += 1;
+        if (q[a] >= g.N[a]) {
+            if (!g.periodic[a]) continue;
+            q[a] = 0;
+        }
+        e[a] = (float)(phi[node_index(g, q[0], q[1], q[2])] - p0);
+    }
+    if (D == 2) reinterpret_cast<float2*>(edges)[node] = make_float2(e[0], e[1]);
+    else reinterpret_cast<float4*>(edges)[node] = make_float4(e[0], e[1], e[2], 0.f);
+}
+
+// ------------------------------------------------------------ mixed push --
+struct PushArgs {
+    GridView g;
+    int* key;
+    float* off[3];
+    float* vel[3];
+    const long long* count;
+    const float* edges;
+    float kE[3];        // q/m * dt * dr_a  (velocity kick per unit edge difference)
+    float dtdr[3];      // dt * dr_a        (offset change per unit velocity)
+    float qmdt_half;    // q/m * dt / 2 (Boris)
+    float Bt[3];        // B * q/m * dt / 2 (Boris t vector)
+    float dr[3];
+    unsigned long long* acc;
+    float scale;        // 2^dep_shift
+    unsigned long long* losses;
+    unsigned* err;
+};
+
+template <int D>
+__device__ __forceinline__ void gather_grad(const PushArgs& a, int c0, int c1, int c2, float f0, float f1, float f2,
+                                            float G[3]) {
+    const GridView& g = a.g;
+    if (D == 2) {
+        const float2* E = reinterpret_cast<const float2*>(a.edges);
+        const int n0p = next_node(g, 0, c0), n1p = next_node(g, 1, c1);
+        const float2 e00 = __ldg(E + node_index(g, c0, c1, 0));
+        const float2 e01 = __ldg(E + node_index(g, c0, n1p, 0));
+        const float2 e10 = __ldg(E + node_index(g, n0p, c1, 0));
+        G[0] = e00.x * (1.f - f1) + e01.x * f1;
+        G[1] = e00.y * (1.f - f0) + e10.y * f0;
+        G[2] = 0.f;
+    } else {
+        const float4* E = reinterpret_cast<const float4*>(a.edges);
+        const int n0p = next_node(g, 0, c0), n1p = next_node(g, 1, c1), n2p = next_node(g, 2, c2);
+        const float4 e000 = __ldg(E + node_index(g, c0, c1, c2));
+        const float4 e001 = __ldg(E + node_index(g, c0, c1, n2p));
+        const float4 e010 = __ldg(E + node_index(g, c0, n1p, c2));
+        const float4 e011 = __ldg(E + node_index(g, c0, n1p, n2p));
+        const float4 e100 = __ldg(E + node_index(g, n0p, c1, c2));
+        const float4 e101 = __ldg(E + node_index(g, n0p, c1, n2p));
+        const float4 e110 = __ldg(E + node_index(g, n0p, n1p, c2));
+        const float g1 = 1.f - f1, g2 = 1.f - f2, g0 = 1.f - f0;
+        G[0] = (e000.x * g2 + e001.x * f2) * g1 + (e010.x * g2 + e011.x * f2) * f1;
+        G[1] = (e000.y * g2 + e001.y * f2) * g0 + (e100.y * g2 + e101.y * f2) * f0;
+        G[2] = (e000.z * g1 + e010.z * f1) * g0 + (e100.z * g1 + e110.z * f1) * f0;
+    }
+}
+
+// One particle: gather, push, boundary.  Returns the loss code (-1 none).
+template <int D, int PUSHER>
+__device__ __forceinline__ int push_one(const PushArgs& a, int& key, float f[3], float v[3]) {
+    const GridView& g = a.g;
+    int c[3];
+    key_to_cell(g, key, c[0], c[1], c[2]);
+    float G[3];
+    gather_grad<D>(a, c[0], c[1], c[2], f[0], f[1], f[2], G);
+    if (PUSHER == PSUM_PIC_LEAPFROG) {
+#pragma unroll
+        for (int d = 0; d < D; ++d) v[d] -= a.kE[d] * G[d];   // v += (q/m) E dt, E = -dr * G
+    } else {
+        float E[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int d = 0; d < D; ++d) E[d] = -a.dr[d] * G[d];
+        float vm[3], vp[3], vq[3], s[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) vm[q] = v[q] + E[q] * a.qmdt_half;
+        const float t2 = a.Bt[0] * a.Bt[0] + a.Bt[1] * a.Bt[1] + a.Bt[2] * a.Bt[2];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) s[q] = 2.f * a.Bt[q] / (1.f + t2);
+        vq[0] = vm[0] + (vm[1] * a.Bt[2] - vm[2] * a.Bt[1]);
+        vq[1] = vm[1] + (vm[2] * a.Bt[0] - vm[0] * a.Bt[2]);
+        vq[2] = vm[2] + (vm[0] * a.Bt[1] - vm[1] * a.Bt[0]);
+        vp[0] = vm[0] + (vq[1] * s[2] - vq[2] * s[1]);
+        vp[1] = vm[1] + (vq[2] * s[0] - vq[0] * s[2]);
+        vp[2] = vm[2] + (vq[0] * s[1] - vq[1] * s[0]);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) v[q] = vp[q] + E[q] * a.qmdt_half;
+    }
+    // position in cell units; offset carry rule: an offset that rounds to
+    // 1.0f moves to the next cell with offset 0.
+    int lost = -1;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        const float sd = f[d] + v[d] * a.dtdr[d];
+        if (!(fabsf(sd) < 1.0e9f)) {
+            atomicOr(a.err, kErrNonFinite);
+            key = -1;
+            return -1;
+        }
+        const float fl = floorf(sd);
+        float nf = sd - fl;
+        int dc = (int)fl;
+        if (nf >= 1.0f) {
+            nf = 0.0f;
+            dc += 1;
+        }
+        f[d] = nf;
+        c[d] += dc;
+    }
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        if (g.periodic[d]) {
+            if (c[d] < 0 || c[d] >= g.M[d]) {
+                c[d] %= g.M[d];
+                if (c[d] < 0) c[d] += g.M[d];
+            }
+        } else if (lost < 0) {
+            if (c[d] < 0) lost = 2 * d;
+            else if (c[d] >= g.cells[d]) lost = 2 * d + 1;
+        }
+    }
+    key = lost >= 0 ? -1 : cell_to_key(g, c[0], c[1], c[2]);
+    return lost;
+}
+
+template <int D>
+__device__ __forceinline__ void deposit_one(const PushArgs& a, int key, const float f[3]) {
+    const GridView& g = a.g;
+    int c[3] = {0, 0, 0};
+    if (key >= 0) key_to_cell(g, key, c[0], c[1], c[2]);
+    const int n0p = key >= 0 ? next_node(g, 0, c[0]) : 0;
+    const int n1p = key >= 0 ? next_node(g, 1, c[1]) : 0;
+    const int n2p = (D == 3 && key >= 0) ? next_node(g, 2, c[2]) : 0;
+#pragma unroll
+    for (int k = 0; k < (1 << D); ++k) {
+        // corner bits: bit 0 -> last axis (PSuM's support order, simple_grid.hpp:330-343)
+        const int b0 = (D == 2) ? (k >> 1) & 1 : (k >> 2) & 1;
+        const int b1 = (D == 2) ? k & 1 : (k >> 1) & 1;
+        const int b2 = (D == 2) ? 0 : k & 1;
+        long long node = -1, val = 0;
+        if (key >= 0) {
+            const float w0 = b0 ? f[0] : 1.f - f[0];
+            const float w1 = b1 ? f[1] : 1.f - f[1];
+            float w = w0 * w1;
+            if (D == 3) w *= b2 ? f[2] : 1.f - f[2];
+            node = node_index(g, b0 ? n0p : c[0], b1 ? n1p : c[1], D == 3 ? (b2 ? n2p : c[2]) : 0);
+            val = __float2ll_rn(w * a.scale);
+        }
+        warp_deposit(a.acc, node, val);
+    }
+}
+
+// 4 particles per thread, 128-bit loads/stores of every SoA array.
+template <int D, int PUSHER, bool DEPOSIT_ONLY>
+__global__ void __launch_bounds__(kPicThreads) k_push_mixed(PushArgs a) {
+    const long long count = *a.count;
+    const int lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * blockDim.x * 4;
+    for (long long base = ((long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) * 4; base < count;
+         base += stride) {
+        const long long i0 = base + 4 * lane;
+        int key[4];
+        float f[4][3], v[4][3];
+        const bool full = i0 + 3 < count;
+        if (full) {
+            const int4 k4 = *reinterpret_cast<const int4*>(a.key + i0);
+            key[0] = k4.x; key[1] = k4.y; key[2] = k4.z; key[3] = k4.w;
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                const float4 t = *reinterpret_cast<const float4*>(a.off[d] + i0);
+                f[0][d] = t.x; f[1][d] = t.y; f[2][d] = t.z; f[3][d] = t.w;
+            }
+            if (!DEPOSIT_ONLY) {
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    const float4 t = *reinterpret_cast<const float4*>(a.vel[q] + i0);
+                    v[0][q] = t.x; v[1][q] = t.y; v[2][q] = t.z; v[3][q] = t.w;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const long long i = i0 + j;
+                key[j] = i < count ? a.key[i] : -1;
+#pragma unroll
+                for (int d = 0; d < D; ++d) f[j][d] = i < count ? a.off[d][i] : 0.f;
+                if (!DEPOSIT_ONLY)
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) v[j][q] = i < count ? a.vel[q][i] : 0.f;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (D == 2) f[j][2] = 0.f;
+            if (!DEPOSIT_ONLY) {
+                int lost = -1;
+                if (key[j] >= 0) lost = push_one<D, PUSHER>(a, key[j], f[j], v[j]);
+                warp_count_losses(a.losses, D, lost);
+            }
+            if (a.acc) deposit_one<D>(a, key[j], f[j]);
+        }
+        if (DEPOSIT_ONLY) continue;
+        if (full) {
+            *reinterpret_cast<int4*>(a.key + i0) = make_int4(key[0], key[1], key[2], key[3]);
+#pragma unroll
+            for (int d = 0; d < D; ++d)
+                *reinterpret_cast<float4*>(a.off[d] + i0) = make_float4(f[0][d], f[1][d], f[2][d], f[3][d]);
+#pragma unroll
+            for (int q = 0; q < 3; ++q)
+                *reinterpret_cast<float4*>(a.vel[q] + i0) = make_float4(v[0][q], v[1][q], v[2][q], v[3][q]);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const long long i = i0 + j;
+                if (i >= count) break;
+                a.key[i] = key[j];
+#pragma unroll
+                for (int d = 0; d < D; ++d) a.off[d][i] = f[j][d];
+#pragma unroll
+                for (int q = 0; q < 3; ++q) a.vel[q][i] = v[j][q];
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------- load / export --
+__global__ void k_load_mixed(GridView g, long long n, const double* __restrict__ pos, const double* __restrict__ vel,
+                             int* __restrict__ key, float* __restrict__ o0, float* __restrict__ o1,
+                             float* __restrict__ o2, float* __restrict__ v0, float* __restrict__ v1,
+                             float* __restrict__ v2) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float* off[3] = {o0, o1, o2};
+    int c[3] = {0, 0, 0};
+    bool valid = isfinite(pos[i]);
+    for (int a = 0; a < g.dim && valid; ++a) {
+        double u = (pos[(long long)a * n + i] - g.lo[a]) * g.dr[a];
+        if (!isfinite(u)) {
+            valid = false;
+            break;
+        }
+        if (g.periodic[a]) {
+            u = u - floor(u / g.M[a]) * g.M[a];
+        } else if (u < 0.0 || u >= (double)g.cells[a]) {
+            valid = false;
+            break;
+        }
+        double fl = floor(u);
+        int ci = (int)fl;
+        float f = (float)(u - fl);
+        if (f >= 1.0f) {   // carry rule
+            f = 0.0f;
+            ci += 1;
+        }
+        if (g.periodic[a]) ci = ci >= g.M[a] ? ci - g.M[a] : ci;
+        else if (ci >= g.cells[a]) {
+            valid = false;
+            break;
+        }
+        c[a] = ci;
+        off[a][i] = f;
+    }
+    if (!valid)
+        for (int a = 0; a < g.dim; ++a) off[a][i] = 0.f;
+    key[i] = valid ? cell_to_key(g, c[0], c[1], c[2]) : -1;
+    v0[i] = (float)vel[i];
+    v1[i] = (float)vel[n + i];
+    v2[i] = (float)vel[2 * n + i];
+}
+
+__global__ void k_export_mixed(GridView g, long long n, const int* __restrict__ key, const float* __restrict__ o0,
+                               const float* __restrict__ o1, const float* __restrict__ o2,
+                               const float* __restrict__ v0, const float* __restrict__ v1,
+                               const float* __restrict__ v2, double* __restrict__ pos, double* __restrict__ vel) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* off[3] = {o0, o1, o2};
+    const int k = key[i];
+    if (k < 0) {
+        for (int a = 0; a < g.dim; ++a) pos[(long long)a * n + i] = 0.0;
+        pos[i] = __longlong_as_double(0x7ff8000000000000LL);
+    } else {
+        int c[3];
+        key_to_cell(g, k, c[0], c[1], c[2]);
+        for (int a = 0; a < g.dim; ++a)
+            pos[(long long)a * n + i] = g.lo[a] + ((double)c[a] + (double)off[a][i]) * g.dx[a];
+    }
+    vel[i] = v0[i];
+    vel[n + i] = v1[i];
+    vel[2 * n + i] = v2[i];
+}
+
+__global__ void k_load64(GridView g, long long n, const double* __restrict__ pos, const double* __restrict__ vel,
+                         double* p0, double* p1, double* p2, double* v0, double* v1, double* v2) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double* P[3] = {p0, p1, p2};
+    bool valid = isfinite(pos[i]);
+    for (int a = 0; a < g.dim; ++a) {
+        double x = pos[(long long)a * n + i];
+        if (valid && !isfinite(x)) valid = false;
+        if (valid && g.periodic[a]) {
+            const double L = (g.cells[a] + 1) * g.dx[a];
+            const double top = g.lo[a] + L;
+            int guard = 0;
+            while (x < g.lo[a] && guard++ < 64) x += L;
+            while (x >= top && guard++ < 128) x -= L;
+        } else if (valid && (x < g.lo[a] || x >= g.lo[a] + g.cells[a] * g.dx[a])) {
+            valid = false;
+        }
+        P[a][i] = x;
+    }
+    if (!valid) p0[i] = __longlong_as_double(0x7ff8000000000000LL);
+    v0[i] = vel[i];
+    v1[i] = vel[n + i];
+    v2[i] = vel[2 * n + i];
+}
+
+// ---------------------------------------------------- scans and sorting --
+constexpr int kScanBlock = 1024;
+
+// exclusive scan of `n` uint32 values in blocks of kScanBlock; block totals out
+__global__ void k_scan_blocks(const unsigned* __restrict__ in, unsigned* __restrict__ out, long long n,
+                              unsigned* __restrict__ totals) {
+    __shared__ unsigned sh[kScanBlock];
+    const long long base = (long long)blockIdx.x * kScanBlock;
+    const int t = threadIdx.x;   // blockDim = 256, 4 items per thread
+    unsigned v[4], s = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const long long i = base + t * 4 + q;
+        v[q] = i < n ? in[i] : 0u;
+        s += v[q];
+    }
+    sh[t] = s;
+    __syncthreads();
+    for (int d = 1; d < 256; d <<= 1) {
+        const unsigned add = t >= d ? sh[t - d] : 0u;
+        __syncthreads();
+        sh[t] += add;
+        __syncthreads();
+    }
+    unsigned run = sh[t] - s;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const long long i = base + t * 4 + q;
+        if (i < n) out[i] = run;
+        run += v[q];
+    }
+    if (t == 255) totals[blockIdx.x] = sh[255];
+}
+
+__global__ void k_scan_add(unsigned* __restrict__ out, long long n, const unsigned* __restrict__ offsets) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] += offsets[i / kScanBlock];
+}
+
+// Single-block sequential-by-chunk scan of up to a few million totals.
+__global__ void k_scan_single(unsigned* __restrict__ v, long long n) {
+    __shared__ unsigned sh[1024];
+    __shared__ unsigned carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (long long base = 0; base < n; base += 1024) {
+        const long long i = base + threadIdx.x;
+        const unsigned x = i < n ? v[i] : 0u;
+        sh[threadIdx.x] = x;
+        __syncthreads();
+        for (int d = 1; d < 1024; d <<= 1) {
+            const unsigned add = threadIdx.x >= d ? sh[threadIdx.x - d] : 0u;
+            __syncthreads();
+            sh[threadIdx.x] += add;
+            __syncthreads();
+        }
+        if (i < n) v[i] = carry + sh[threadIdx.x] - x;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry += sh[1023];
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+// exclusive scan (uint32), `tmp1`/`tmp2` scratch of ceil(n/1024) and
+// ceil(n/1024^2) entries
+void exclusive_scan_u32(const unsigned* in, unsigned* out, long long n, unsigned* tmp1, unsigned* tmp2,
+                        cudaStream_t s) {
+    if (n <= 0) return;
+    const long long nb = (n + kScanBlock - 1) / kScanBlock;
+    { k_scan_blocks<<<(unsigned)nb, 256, 0, s>>>(in, out, n, tmp1); count_launch(); }
+    if (nb > 1) {
+        if (nb <= 4 * 1024 * 1024) {
+            { k_scan_single<<<1, 1024, 0, s>>>(tmp1, nb); count_launch(); }
+        } else {
+            throw Error(PSUM_ERR_INVALID_ARGUMENT, "scan: input too large");
+        }
+        (void)tmp2;
+        { k_scan_add<<<blocks_for(n, 256), 256, 0, s>>>(out, n, tmp1); count_launch(); }
+    }
+}
+
+namespace {
+
+constexpr int kRsThreads = 256;
+constexpr int kRsItems = 16;
+constexpr int kRsTile = kRsThreads * kRsItems;   // 4096
+constexpr int kRsBits = 8;
+constexpr int kRsBuckets = 1 << kRsBits;
+
+__global__ void __launch_bounds__(kRsThreads) k_rs_hist(const unsigned* __restrict__ keys, long long n, int shift,
+                                                        unsigned* __restrict__ hist, int nblocks) {
+    __shared__ unsigned h[kRsBuckets];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const long long base = (long long)blockIdx.x * kRsTile;
+#pragma unroll 4
+    for (int r = 0; r < kRsItems; ++r) {
+        const long long i = base + r * kRsThreads + threadIdx.x;
+        if (i < n) atomicAdd(&h[(keys[i] >> shift) & (kRsBuckets - 1)], 1u);
+    }
+    __syncthreads();
+    hist[(long long)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+// Stable scatter: items are ranked in (round, thread) order, i.e. ascending
+// input index within a tile; tiles are ordered by the digit-major scan.
+__global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const unsigned* __restrict__ kin,
+                                                           const int* __restrict__ vin, unsigned* __restrict__ kout,
+                                                           int* __restrict__ vout, long long n, int shift,
+                                                           const unsigned* __restrict__ offs, int nblocks) {
+    __shared__ unsigned wcnt[kRsThreads / 32][kRsBuckets];
+    __shared__ unsigned running[kRsBuckets];
+    __shared__ unsigned base_off[kRsBuckets];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    running[t] = 0;
+    base_off[t] = offs[(long long)t * nblocks + blockIdx.x];
+    const long long tile = (long long)blockIdx.x * kRsTile;
+    for (int r = 0; r < kRsItems; ++r) {
+#pragma unroll
+        for (int w = 0; w < kRsThreads / 32; ++w) wcnt[w][t] = 0;
+        __syncthreads();
+        const long long i = tile + r * kRsThreads + t;
+        const bool valid = i < n;
+        const unsigned key = valid ? kin[i] : 0u;
+        const int dig = valid ? (int)((key >> shift) & (kRsBuckets - 1)) : kRsBuckets;   // kRsBuckets = none
+        const unsigned peers = __match_any_sync(0xffffffffu, dig);
+        const unsigned lt = (1u << lane) - 1u;
+        const int rank_w = __popc(peers & lt);
+        if (valid && rank_w == 0) wcnt[warp][dig] = __popc(peers);
+        __syncthreads();
+        // exclusive prefix over warps for digit t, plus the round total
+        {
+            unsigned acc = 0;
+#pragma unroll
+            for (int w = 0; w < kRsThreads / 32; ++w) {
+                const unsigned c = wcnt[w][t];
+                wcnt[w][t] = acc;
+                acc += c;
+            }
+            __syncthreads();
+            if (valid) {
+                const unsigned pos = base_off[dig] + running[dig] + wcnt[warp][dig] + (unsigned)rank_w;
+                kout[pos] = key;
+                vout[pos] = vin[i];
+            }
+            __syncthreads();
+            running[t] += acc;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_make_sort_keys(const int* __restrict__ key, long long n, unsigned sentinel,
+                                 unsigned* __restrict__ skey, int* __restrict__ sidx) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int k = key[i];
+    skey[i] = k < 0 ? sentinel : (unsigned)k;
+    sidx[i] = (int)i;
+}
+
+template <class T>
+__global__ void k_gather(const T* __restrict__ in, T* __restrict__ out, const int* __restrict__ perm, long long n) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = in[perm[i]];
+}
+
+__global__ void k_count_valid(const unsigned* __restrict__ sorted_keys, long long n, unsigned sentinel,
+                              long long* __restrict__ count) {
+    // first index holding the sentinel (keys are sorted ascending)
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const bool here = sorted_keys[i] == sentinel && (i == 0 || sorted_keys[i - 1] != sentinel);
+    if (here) *count = i;
+    if (i == n - 1 && sorted_keys[i] != sentinel) *count = n;
+}
+
+__global__ void k_set_count(long long* count, long long v) { *count = v; }
+
+// ------------------------------------------------------- charge density --
+struct RhoArgs {
+    const unsigned long long* acc[8];
+    double coef[8];
+    int ns;
+    double background;
+};
+
+__global__ void k_rho(RhoArgs a, double* __restrict__ rho, long long n) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double r = a.background;
+    for (int s = 0; s < a.ns; ++s) r += a.coef[s] * (double)(long long)a.acc[s][i];
+    rho[i] = r;
+}
+
+// ------------------------------------------------------------ binning ---
+__global__ void k_bin_keys_mixed(GridView g, const int* __restrict__ key, const float* __restrict__ o0,
+                                 long long n, long long* __restrict__ keys_out, unsigned* __restrict__ skey,
+                                 int* __restrict__ sidx, unsigned sentinel) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int k = key[i];
+    long long ref = -1;
+    if (k >= 0) {
+        int c[3];
+        key_to_cell(g, k, c[0], c[1], c[2]);
+        bool in = true;
+        for (int a = 0; a < g.dim; ++a) in = in && c[a] < g.cells[a];   // the wrap cell is outside [lo, hi)
+        if (in) ref = ((long long)c[0] * g.cells[1] + c[1]) * g.cells[2] + c[2];
+    }
+    (void)o0;
+    keys_out[i] = ref;
+    skey[i] = ref < 0 ? sentinel : (unsigned)ref;
+    sidx[i] = (int)i;
+}
+
+__global__ void k_bin_keys64(GridView g, const double* __restrict__ x, const double* __restrict__ y,
+                             const double* __restrict__ z, long long n, long long* __restrict__ keys_out,
+                             unsigned* __restrict__ skey, int* __restrict__ sidx, unsigned sentinel, const double* hi) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double p[3] = {x[i], g.dim > 1 ? y[i] : 0.0, g.dim > 2 ? z[i] : 0.0};
+    long long ref = -1;
+    bool in = isfinite(p[0]);
+    for (int a = 0; a < g.dim && in; ++a) in = p[a] >= g.lo[a] && p[a] < hi[a];   // inGrid, simple_grid.hpp:168-174
+    if (in) {
+        int c[3] = {0, 0, 0};
+        for (int a = 0; a < g.dim; ++a) c[a] = (int)((p[a] - g.lo[a]) * g.dr[a]);   // nC: truncation, :99-104
+        ref = ((long long)c[0] * g.cells[1] + c[1]) * g.cells[2] + c[2];
+    }
+    keys_out[i] = ref;
+    skey[i] = ref < 0 ? sentinel : (unsigned)ref;
+    sidx[i] = (int)i;
+}
+
+__global__ void k_hist_u32(const long long* __restrict__ keys, long long n, unsigned* __restrict__ counts) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && keys[i] >= 0) atomicAdd(counts + keys[i], 1u);
+}
+
+__global__ void k_u32_to_u64(const unsigned* __restrict__ in, unsigned long long* __restrict__ out, long long n) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = in[i];
+}
+
+__global__ void k_i32_to_u64(const int* __restrict__ in, unsigned long long* __restrict__ out, long long n) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (unsigned long long)in[i];
+}
+
+// ------------------------------------------------------- diagnostics ----
+__global__ void __launch_bounds__(256) k_kinetic_mixed(const int* __restrict__ key, const float* __restrict__ v0,
+                                                       const float* __restrict__ v1, const float* __restrict__ v2,
+                                                       const long long* __restrict__ count, double mw,
+                                                       double* __restrict__ partials) {
+    __shared__ double sh[8];
+    double acc = 0.0;
+    const long long n = *count;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        if (key[i] >= 0) {
+            const double a = v0[i], b = v1[i], c = v2[i];
+            acc += 0.5 * mw * (a * a + b * b + c * c);
+        }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0;
+        for (int w = 0; w < 8; ++w) s += sh[w];
+        partials[blockIdx.x] = s;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_kinetic64(const double* __restrict__ x, const double* __restrict__ v0,
+                                                   const double* __restrict__ v1, const double* __restrict__ v2,
+                                                   const long long* __restrict__ count, double mw,
+                                                   double* __restrict__ partials) {
+    __shared__ double sh[8];
+    double acc = 0.0;
+    const long long n = *count;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        if (isfinite(x[i])) acc += 0.5 * mw * (v0[i] * v0[i] + v1[i] * v1[i] + v2[i] * v2[i]);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0;
+        for (int w = 0; w < 8; ++w) s += sh[w];
+        partials[blockIdx.x] = s;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_field_energy(GridView g, const double* __restrict__ phi,
+                                                      double* __restrict__ partials) {
+    __shared__ double sh[8];
+    double acc = 0.0;
+    for (long long node = (long long)blockIdx.x * blockDim.x + threadIdx.x; node < g.n_nodes;
+         node += (long long)gridDim.x * blockDim.x) {
+        const int n12 = g.N[1] * g.N[2];
+        const int i = (int)(node / n12);
+        const int rem = (int)(node - (long long)i * n12);
+        const int idx[3] = {i, rem / g.N[2], rem % g.N[2]};
+        for (int a = 0; a < g.dim; ++a) {
+            int q[3] = {idx[0], idx[1], idx[2]};
+            q[a] += 1;
+            if (q[a] >= g.N[a]) {
+                if (!g.periodic[a]) continue;
+                q[a] = 0;
+            }
+            const double gr = (phi[node_index(g, q[0], q[1], q[2])] - phi[node]) * g.dr[a];
+            acc += gr * gr;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0;
+        for (int w = 0; w < 8; ++w) s += sh[w];
+        partials[blockIdx.x] = s;
+    }
+}
+
+__global__ void k_acc_sum(const unsigned long long* __restrict__ acc, long long n, long long* __restrict__ out) {
+    long long s = 0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        s += (long long)acc[i];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(reinterpret_cast<unsigned long long*>(out), (unsigned long long)s);
+}
+
+constexpr int kDiagBlocks = 296;
+
+}  // namespace
+
+// ============================================================ host side ===
+
+static psum_pic_ctx* ctx_check(psum_pic_ctx* c) {
+    if (!c || c->magic != kPicMagic) throw Error(PSUM_ERR_INVALID_ARGUMENT, "not a particle context of this library");
+    return c;
+}
+
+static Species& species_at(psum_pic_ctx* c, int s) {
+    if (s < 0 || s >= (int)c->sp.size()) throw Error(PSUM_ERR_INVALID_ARGUMENT, "species index out of range");
+    return *c->sp[s];
+}
+
+static int bits_for(unsigned long long v) {
+    int b = 0;
+    while (b < 64 && (1ULL << b) <= v) ++b;
+    return b;
+}
+
+static void ensure_sort_scratch(psum_pic_ctx* c, long long n) {
+    SortScratch& S = c->sort;
+    if (S.cap >= n) return;
+    S.keyA.alloc(n);
+    S.keyB.alloc(n);
+    S.idxA.alloc(n);
+    S.idxB.alloc(n);
+    const long long nb = (n + kRsTile - 1) / kRsTile;
+    S.hist.alloc((size_t)kRsBuckets * nb);
+    S.hist_scan.alloc((size_t)kRsBuckets * nb);
+    S.block_sums.alloc((size_t)((kRsBuckets * nb + kScanBlock - 1) / kScanBlock) + 1);
+    S.block_sums2.alloc(16);
+    S.cap = n;
+}
+
+// Stable LSD radix sort of (skey, sidx) pairs in S.keyA/S.idxA; result in
+// the returned pair of buffers.
+static void radix_sort(psum_pic_ctx* c, long long n, unsigned max_key, unsigned** keys_out, int** idx_out) {
+    SortScratch& S = c->sort;
+    cudaStream_t s = c->stream;
+    unsigned* kin = S.keyA.p;
+    unsigned* kout = S.keyB.p;
+    int* vin = S.idxA.p;
+    int* vout = S.idxB.p;
+    const int nbits = std::max(1, bits_for(max_key));
+    const int nb = (int)((n + kRsTile - 1) / kRsTile);
+    for (int shift = 0; shift < nbits; shift += kRsBits) {
+        { k_rs_hist<<<nb, kRsThreads, 0, s>>>(kin, n, shift, S.hist.p, nb); count_launch(); }
+        exclusive_scan_u32(S.hist.p, S.hist_scan.p, (long long)kRsBuckets * nb, S.block_sums.p, S.block_sums2.p, s);
+        { k_rs_scatter<<<nb, kRsThreads, 0, s>>>(kin, vin, kout, vout, n, shift, S.hist_scan.p, nb); count_launch(); }
+        std::swap(kin, kout);
+        std::swap(vin, vout);
+    }
+    cuda_check(cudaGetLastError(), "radix sort launch");
+    *keys_out = kin;
+    *idx_out = vin;
+}
+
+static void sort_species(psum_pic_ctx* c, Species& sp, int sidx) {
+    const long long n = sp.n;
+    if (n <= 0) return;
+    cudaStream_t s = c->stream;
+    ensure_sort_scratch(c, n);
+    const int cur = sp.cur, nxt = 1 - sp.cur;
+    const unsigned sentinel = (unsigned)c->g.n_cells;
+    { k_make_sort_keys<<<blocks_for(n, 256), 256, 0, s>>>(sp.key[cur].p, n, sentinel, c->sort.keyA.p, c->sort.idxA.p); count_launch(); }
+    unsigned* skeys;
+    int* perm;
+    radix_sort(c, n, sentinel, &skeys, &perm);
+    const unsigned gb = blocks_for(n, 256);
+    { k_gather<int><<<gb, 256, 0, s>>>(sp.key[cur].p, sp.key[nxt].p, perm, n); count_launch(); }
+    if (c->precision == PSUM_PIC_MIXED) {
+        for (int a = 0; a < c->g.dim; ++a) { k_gather<float><<<gb, 256, 0, s>>>(sp.off[a][cur].p, sp.off[a][nxt].p, perm, n); count_launch(); }
+        for (int q = 0; q < 3; ++q) { k_gather<float><<<gb, 256, 0, s>>>(sp.vel[q][cur].p, sp.vel[q][nxt].p, perm, n); count_launch(); }
+    } else {
+        for (int a = 0; a < c->g.dim; ++a)
+            { k_gather<double><<<gb, 256, 0, s>>>(sp.pos64[a][cur].p, sp.pos64[a][nxt].p, perm, n); count_launch(); }
+        for (int q = 0; q < 3; ++q) { k_gather<double><<<gb, 256, 0, s>>>(sp.vel64[q][cur].p, sp.vel64[q][nxt].p, perm, n); count_launch(); }
+    }
+    { k_count_valid<<<gb, 256, 0, s>>>(skeys, n, sentinel, c->count.p + sidx); count_launch(); }
+    sp.cur = nxt;
+    cuda_check(cudaGetLastError(), "sort launch");
+}
+
+static void alloc_species_state(psum_pic_ctx* c, Species& sp) {
+    for (int b = 0; b < 2; ++b) {
+        sp.key[b].alloc(sp.cap);
+        if (c->precision == PSUM_PIC_MIXED) {
+            for (int a = 0; a < c->g.dim; ++a) sp.off[a][b].alloc(sp.cap);
+            for (int q = 0; q < 3; ++q) sp.vel[q][b].alloc(sp.cap);
+        } else {
+            for (int a = 0; a < c->g.dim; ++a) sp.pos64[a][b].alloc(sp.cap);
+            for (int q = 0; q < 3; ++q) sp.vel64[q][b].alloc(sp.cap);
+        }
+    }
+    sp.acc.alloc(c->g.n_nodes);
+    cuda_check(cudaMemsetAsync(sp.acc.p, 0, sizeof(unsigned long long) * c->g.n_nodes, c->stream), "memset acc");
+}
+
+static PushArgs make_push_args(psum_pic_ctx* c, Species& sp, int sidx, double dt, int pusher, const double* B) {
+    PushArgs a{};
+    a.g = c->g;
+    a.key = sp.key[sp.cur].p;
+    for (int d = 0; d < 3; ++d) {
+        a.off[d] = d < c->g.dim ? sp.off[d][sp.cur].p : nullptr;
+        a.vel[d] = sp.vel[d][sp.cur].p;
+    }
+    a.count = c->count.p + sidx;
+    a.edges = c->edges.p;
+    const double qm = sp.q / sp.m;
+    for (int d = 0; d < 3; ++d) {
+        a.kE[d] = (float)(qm * dt * c->g.dr[d]);
+        a.dtdr[d] = (float)(dt * c->g.dr[d]);
+        a.dr[d] = (float)c->g.dr[d];
+        a.Bt[d] = (float)((B ? B[d] : 0.0) * qm * dt * 0.5);
+    }
+    a.qmdt_half = (float)(qm * dt * 0.5);
+    a.acc = sp.acc.p;
+    a.scale = std::ldexp(1.0f, sp.dep_shift);
+    a.losses = c->losses.p + (size_t)sidx * 6;
+    a.err = c->err.p;
+    (void)pusher;
+    return a;
+}
+
+static void launch_mixed(const PushArgs& a, int dim, int pusher, bool deposit_only, long long n, cudaStream_t s) {
+    const unsigned blocks = capped_blocks(4LL * kPicThreads, n);
+    if (deposit_only) {
+        if (dim == 2) { k_push_mixed<2, 0, true><<<blocks, kPicThreads, 0, s>>>(a); count_launch(); }
+        else { k_push_mixed<3, 0, true><<<blocks, kPicThreads, 0, s>>>(a); count_launch(); }
+        return;
+    }
+    if (dim == 2) {
+        if (pusher == PSUM_PIC_BORIS) { k_push_mixed<2, PSUM_PIC_BORIS, false><<<blocks, kPicThreads, 0, s>>>(a); count_launch(); }
+        else { k_push_mixed<2, PSUM_PIC_LEAPFROG, false><<<blocks, kPicThreads, 0, s>>>(a); count_launch(); }
+    } else {
+        if (pusher == PSUM_PIC_BORIS) { k_push_mixed<3, PSUM_PIC_BORIS, false><<<blocks, kPicThreads, 0, s>>>(a); count_launch(); }
+        else { k_push_mixed<3, PSUM_PIC_LEAPFROG, false><<<blocks, kPicThreads, 0, s>>>(a); count_launch(); }
+    }
+}
+
+static void zero_accumulators(psum_pic_ctx* c) {
+    for (auto& sp : c->sp)
+        cuda_check(cudaMemsetAsync(sp->acc.p, 0, sizeof(unsigned long long) * c->g.n_nodes, c->stream), "memset acc");
+}
+
+static void deposit_all(psum_pic_ctx* c) {
+    zero_accumulators(c);
+    for (int s = 0; s < (int)c->sp.size(); ++s) {
+        Species& sp = *c->sp[s];
+        if (sp.n <= 0) continue;
+        if (c->precision == PSUM_PIC_MIXED) {
+            PushArgs a = make_push_args(c, sp, s, 0.0, 0, nullptr);
+            launch_mixed(a, c->g.dim, 0, true, sp.n, c->stream);
+        } else {
+            Deposit64Args a{};
+            a.g = c->g;
+            for (int d = 0; d < 3; ++d) a.pos[d] = d < c->g.dim ? sp.pos64[d][sp.cur].p : nullptr;
+            a.count = c->count.p + s;
+            a.acc = sp.acc.p;
+            a.scale = std::ldexp(1.0, sp.dep_shift);
+            launch_deposit64(a, sp.n, c->stream);
+        }
+    }
+    cuda_check(cudaGetLastError(), "deposit launch");
+}
+
+static void push_all(psum_pic_ctx* c, const double* phi, double dt, int pusher, const double* B) {
+    if (!phi) throw std::invalid_argument("push: null phi");
+    if (pusher != PSUM_PIC_LEAPFROG && pusher != PSUM_PIC_BORIS) throw std::invalid_argument("push: unknown pusher");
+    if (!(std::isfinite(dt))) throw Error(PSUM_ERR_NONFINITE, "push: non-finite dt");
+    cudaStream_t s = c->stream;
+    zero_accumulators(c);
+    if (c->precision == PSUM_PIC_MIXED) {
+        if (c->g.dim == 2) { k_edges<2><<<blocks_for(c->g.n_nodes, 256), 256, 0, s>>>(c->g, phi, c->edges.p); count_launch(); }
+        else { k_edges<3><<<blocks_for(c->g.n_nodes, 256), 256, 0, s>>>(c->g, phi, c->edges.p); count_launch(); }
+    }
+    for (int si = 0; si < (int)c->sp.size(); ++si) {
+        Species& sp = *c->sp[si];
+        if (sp.n <= 0) continue;
+        if (c->precision == PSUM_PIC_MIXED) {
+            PushArgs a = make_push_args(c, sp, si, dt, pusher, B);
+            launch_mixed(a, c->g.dim, pusher, false, sp.n, s);
+        } else {
+            Push64Args a{};
+            a.g = c->g;
+            for (int d = 0; d < 3; ++d) {
+                a.hi[d] = c->g.lo[d] + c->g.cells[d] * c->g.dx[d];
+                a.pos[d] = d < c->g.dim ? sp.pos64[d][sp.cur].p : nullptr;
+                a.vel[d] = sp.vel64[d][sp.cur].p;
+                a.B[d] = B ? B[d] : 0.0;
+            }
+            a.key = sp.key[sp.cur].p;
+            a.count = c->count.p + si;
+            a.phi = phi;
+            a.q_m = sp.q / sp.m;
+            a.dt = dt;
+            a.pusher = pusher;
+            a.acc = sp.acc.p;
+            a.scale = std::ldexp(1.0, sp.dep_shift);
+            a.losses = c->losses.p + (size_t)si * 6;
+            a.err = c->err.p;
+            launch_push64(a, sp.n, s);
+        }
+    }
+    cuda_check(cudaGetLastError(), "push launch");
+}
+
+static void sort_all(psum_pic_ctx* c) {
+    for (int s = 0; s < (int)c->sp.size(); ++s) sort_species(c, *c->sp[s], s);
+}
+
+static void rho_into(psum_pic_ctx* c, double background, double* rho, int only_species, bool with_charge) {
+    if (!rho) throw std::invalid_argument("rho: null output");
+    RhoArgs a{};
+    a.background = background;
+    double vol = 1.0;
+    for (int d = 0; d < c->g.dim; ++d) vol *= c->g.dx[d];
+    for (int s = 0; s < (int)c->sp.size(); ++s) {
+        if (only_species >= 0 && s != only_species) continue;
+        if (a.ns >= 8) throw Error(PSUM_ERR_INVALID_ARGUMENT, "rho: more than 8 species");
+        Species& sp = *c->sp[s];
+        a.acc[a.ns] = sp.acc.p;
+        a.coef[a.ns] = (with_charge ? sp.q : 1.0) * sp.w / vol * std::ldexp(1.0, -sp.dep_shift);
+        a.ns++;
+    }
+    { k_rho<<<blocks_for(c->g.n_nodes, 256), 256, 0, c->stream>>>(a, rho, c->g.n_nodes); count_launch(); }
+    cuda_check(cudaGetLastError(), "rho launch");
+}
+
+}  // namespace psum_b200
+
+// =================================================================== ABI ==
+using namespace psum_b200;
+
+extern "C" {
+
+EXPORT int psum_pic_create(const psum_pic_grid_desc* gd, int precision, psum_pic_ctx** out) {
+    return guarded([&] {
+        if (!gd || !out) throw std::invalid_argument("psum_pic_create: null argument");
+        *out = nullptr;
+        if (gd->dim != 2 && gd->dim != 3) throw std::invalid_argument("psum_pic_create: dim must be 2 or 3");
+        if (precision != PSUM_PIC_MIXED && precision != PSUM_PIC_FP64)
+            throw std::invalid_argument("psum_pic_create: unknown precision");
+        auto c = std::make_unique<psum_pic_ctx>();
+        GridView& g = c->g;
+        g.dim = gd->dim;
+        long long nn = 1, nc = 1;
+        for (int a = 0; a < 3; ++a) {
+            if (a < gd->dim) {
+                if (gd->cells[a] < 1) throw std::invalid_argument("psum_pic_create: cells must be positive");
+                if (!(gd->lower[a] < gd->upper[a])) throw std::invalid_argument("psum_pic_create: lower >= upper");
+                g.cells[a] = gd->cells[a];
+                g.periodic[a] = gd->periodic[a] ? 1 : 0;
+                g.M[a] = g.periodic[a] ? g.cells[a] + 1 : g.cells[a];
+                g.N[a] = g.cells[a] + 1;
+                g.lo[a] = gd->lower[a];
+                g.dx[a] = (gd->upper[a] - gd->lower[a]) / gd->cells[a];   // simple_grid.hpp:47
+                g.dr[a] = 1.0 / g.dx[a];
+            } else {
+                g.cells[a] = g.M[a] = g.N[a] = 1;
+                g.periodic[a] = 0;
+                g.lo[a] = 0.0;
+                g.dx[a] = g.dr[a] = 1.0;
+            }
+            nn *= g.N[a];
+            nc *= g.M[a];
+        }
+        if (nc >= 0x7fffffffLL) throw std::invalid_argument("psum_pic_create: more than 2^31-1 cells");
+        g.n_nodes = nn;
+        g.n_cells = nc;
+        c->precision = precision;
+        cuda_check(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        c->stream = c->own_stream;
+        if (precision == PSUM_PIC_MIXED) c->edges.alloc((size_t)nn * (g.dim == 2 ? 2 : 4));
+        c->losses.alloc(8 * 6);
+        c->err.alloc(1);
+        c->count.alloc(8);
+        c->partials.alloc(kDiagBlocks);
+        c->ipartials.alloc(1);
+        cuda_check(cudaMemsetAsync(c->losses.p, 0, sizeof(unsigned long long) * 48, c->stream), "memset");
+        cuda_check(cudaMemsetAsync(c->err.p, 0, sizeof(unsigned), c->stream), "memset");
+        cuda_check(cudaMemsetAsync(c->count.p, 0, sizeof(long long) * 8, c->stream), "memset");
+        cuda_check(cudaStreamSynchronize(c->stream), "create sync");
+        *out = c.release();
+    });
+}
+
+EXPORT int psum_pic_destroy(psum_pic_ctx* ctx) {
+    return guarded([&] {
+        if (!ctx) return;
+        ctx_check(ctx);
+        cudaStreamSynchronize(ctx->stream);
+        ctx->magic = 0;
+        delete ctx;
+    });
+}
+
+EXPORT int psum_pic_set_stream(psum_pic_ctx* ctx, void* stream) {
+    return guarded([&] {
+        ctx_check(ctx);
+        ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    });
+}
+
+EXPORT int psum_pic_set_options(psum_pic_ctx* ctx, const char* options) {
+    return guarded([&] {
+        ctx_check(ctx);
+        if (!options) throw std::invalid_argument("set_options: null option string");
+        std::istringstream iss(options);
+        std::string key;
+        while (iss >> key) {
+            int v;
+            if (!(iss >> v)) throw std::invalid_argument("set_options: option '" + key + "' needs an integer value");
+            if (key == "sort_interval") {
+                if (v < 0) throw std::invalid_argument("sort_interval must be >= 0");
+                ctx->sort_interval = v;
+            } else {
+                throw std::invalid_argument("set_options: unknown particle option '" + key + "'");
+            }
+        }
+    });
+}
+
+EXPORT int psum_pic_add_species(psum_pic_ctx* ctx, const psum_pic_species_desc* d, unsigned long long capacity,
+                                int* id) {
+    return guarded([&] {
+        ctx_check(ctx);
+        if (!d || !id) throw std::invalid_argument("add_species: null argument");
+        if (ctx->sp.size() >= 8) throw std::invalid_argument("add_species: at most 8 species");
+        if (!(d->mass > 0) || !std::isfinite(d->charge) || !std::isfinite(d->weight))
+            throw std::invalid_argument("add_species: mass must be positive, charge and weight finite");
+        if (capacity == 0 || capacity >= 0x7fffffffULL) throw std::invalid_argument("add_species: capacity out of range");
+        auto sp = std::make_unique<Species>();
+        sp->q = d->charge;
+        sp->m = d->mass;
+        sp->w = d->weight;
+        sp->cap = (long long)((capacity + 3) & ~3ULL);
+        // fixed point: every node sum stays below 2^62 even if all particles share one node
+        sp->dep_shift = 62 - bits_for((unsigned long long)sp->cap);
+        alloc_species_state(ctx, *sp);
+        ctx->sp.push_back(std::move(sp));
+        *id = (int)ctx->sp.size() - 1;
+        cuda_check(cudaStreamSynchronize(ctx->stream), "add_species sync");
+    });
+}
+
+static void load_common(psum_pic_ctx* ctx, int species, unsigned long long n, const double* pos_dev,
+                        const double* vel_dev) {
+    Species& sp = species_at(ctx, species);
+    if ((long long)n > sp.cap) throw Error(PSUM_ERR_OVERFLOW, "load: more particles than the species capacity");
+    cudaStream_t s = ctx->stream;
+    sp.cur = 0;
+    if (n > 0) {
+        const unsigned gb = blocks_for((long long)n, 256);
+        if (ctx->precision == PSUM_PIC_MIXED) {
+            { k_load_mixed<<<gb, 256, 0, s>>>(ctx->g, (long long)n, pos_dev, vel_dev, sp.key[0].p, sp.off[0][0].p,
+                                            ctx->g.dim > 1 ? sp.off[1][0].p : nullptr,
+                                            ctx->g.dim > 2 ? sp.off[2][0].p : sp.off[0][1].p, sp.vel[0][0].p,
+                                            sp.vel[1][0].p, sp.vel[2][0].p); count_launch(); }
+        } else {
+            { k_load64<<<gb, 256, 0, s>>>(ctx->g, (long long)n, pos_dev, vel_dev, sp.pos64[0][0].p,
+                                        ctx->g.dim > 1 ? sp.pos64[1][0].p : nullptr,
+                                        ctx->g.dim > 2 ? sp.pos64[2][0].p : sp.pos64[0][1].p, sp.vel64[0][0].p,
+                                        sp.vel64[1][0].p, sp.vel64[2][0].p); count_launch(); }
+        }
+    }
+    { k_set_count<<<1, 1, 0, s>>>(ctx->count.p + species, (long long)n); count_launch(); }
+    sp.n = (long long)n;
+    if (ctx->precision == PSUM_PIC_FP64 && n > 0) {
+        double* p3[3] = {sp.pos64[0][0].p, ctx->g.dim > 1 ? sp.pos64[1][0].p : nullptr,
+                         ctx->g.dim > 2 ? sp.pos64[2][0].p : nullptr};
+        launch_keys64(ctx->g, p3, sp.key[0].p, ctx->count.p + species, (long long)n, s);
+    }
+    cuda_check(cudaGetLastError(), "load launch");
+}
+
+EXPORT int psum_pic_load(psum_pic_ctx* ctx, int species, unsigned long long n, const double* pos_host,
+                         const double* vel_host) {
+    return guarded([&] {
+        ctx_check(ctx);
+        if (n > 0 && (!pos_host || !vel_host)) throw std::invalid_argument("load: null host array");
+        const int D = ctx->g.dim;
+        DevBuf<double> dp, dv;
+        dp.upload(pos_host, (size_t)n * D, ctx->stream);
+        dv.upload(vel_host, (size_t)n * 3, ctx->stream);
+        load_common(ctx, species, n, dp.p, dv.p);
+        cuda_check(cudaStreamSynchronize(ctx->stream), "load sync");
+    });
+}
+
+EXPORT int psum_pic_load_device(psum_pic_ctx* ctx, int species, unsigned long long n, const double* pos_dev,
+                                const double* vel_dev) {
+    return guarded([&] {
+        ctx_check(ctx);
+        if (n > 0 && (!pos_dev || !vel_dev)) throw std::invalid_argument("load: null device array");
+        load_common(ctx, species, n, pos_dev, vel_dev);
+    });
+}
+
+EXPORT int psum_pic_count(psum_pic_ctx* ctx, int species, unsigned long long* n_stored, unsigned long long* n_valid) {
+    return guarded([&] {
+        ctx_check(ctx);
+        Species& sp = species_at(ctx, species);
+        long long dc = 0;
+        cuda_check(cudaMemcpyAsync(&dc, ctx->count.p + species, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream),
+                   "count copy");
+        cuda_check(cudaStreamSynchronize(ctx->stream), "count sync");
+        sp.n = dc;
+        if (n_stored) *n_stored = (unsigned long long)dc;
+        if (n_valid) {
+            std::vector<int> keys(dc);
+            if (dc > 0)
+                cuda_check(cudaMemcpy(keys.data(), sp.key[sp.cur].p, sizeof(int) * dc, cudaMemcpyDeviceToHost),
+                           "keys copy");
+            unsigned long long v = 0;
+            for (long long i = 0; i < dc; ++i) v += keys[i] >= 0;
+            *n_valid = v;
+        }
+    });
+}
+
+EXPORT int psum_pic_get_state(psum_pic_ctx* ctx, int species, double* pos_host, double* vel_host) {
+    return guarded([&] {
+        ctx_check(ctx);
+        Species& sp = species_at(ctx, species);
+        long long n = 0;
+        cuda_check(cudaMemcpyAsync(&n, ctx->count.p + species, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream),
+                   "count copy");
+        cuda_check(cudaStreamSynchronize(ctx->stream), "count sync");
+        sp.n = n;
+        if (n == 0) return;
+        if (!pos_host || !vel_host) throw std::invalid_argument("get_state: null host array");
+        const int D = ctx->g.dim;
+        DevBuf<double> dp, dv;
+        dp.alloc((size_t)n * D);
+        dv.alloc((size_t)n * 3);
+        const int cur = sp.cur;
+        if (ctx->precision == PSUM_PIC_MIXED) {
+            { k_export_mixed<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(
+                ctx->g, n, sp.key[cur].p, sp.off[0][cur].p, D > 1 ? sp.off[1][cur].p : nullptr,
+                D > 2 ? sp.off[2][cur].p : nullptr, sp.vel[0][cur].p, sp.vel[1][cur].p, sp.vel[2][cur].p, dp.p, dv.p); count_launch(); }
+        } else {
+            for (int a = 0; a < D; ++a)
+                cuda_check(cudaMemcpyAsync(dp.p + (size_t)a * n, sp.pos64[a][cur].p, sizeof(double) * n,
+                                           cudaMemcpyDeviceToDevice, ctx->stream),
+                           "copy");
+            for (int q = 0; q < 3; ++q)
+                cuda_check(cudaMemcpyAsync(dv.p + (size_t)q * n, sp.vel64[q][cur].p, sizeof(double) * n,
+                                           cudaMemcpyDeviceToDevice, ctx->stream),
+                           "copy");
+        }
+        cuda_check(cudaMemcpyAsync(pos_host, dp.p, sizeof(double) * n * D, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        cuda_check(cudaMemcpyAsync(vel_host, dv.p, sizeof(double) * n * 3, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        cuda_check(cudaStreamSynchronize(ctx->stream), "get_state sync");
+    });
+}
+
+EXPORT int psum_pic_get_keys(psum_pic_ctx* ctx, int species, int* keys_dev) {
+    return guarded([&] {
+        ctx_check(ctx);
+        Species& sp = species_at(ctx, species);
+        if (!keys_dev) throw std::invalid_argument("get_keys: null output");
+        if (sp.n > 0)
+            cuda_check(cudaMemcpyAsync(keys_dev, sp.key[sp.cur].p, sizeof(int) * sp.n, cudaMemcpyDeviceToDevice,
+                                       ctx->stream),
+                       "keys copy");
+        cuda_check(cudaStreamSynchronize(ctx->stream), "keys sync");
+    });
+}
+
+EXPORT int psum_pic_sort(psum_pic_ctx* ctx) {
+    return guarded([&] {
+        ctx_check(ctx);
+        sort_all(ctx);
+    });
+}
+
+EXPORT int psum_pic_bin(psum_pic_ctx* ctx, int species, long long* keys_dev, unsigned long long* counts_dev,
+                        unsigned long long* offsets_dev, unsigned long long* perm_dev, unsigned long long* n_in_grid) {
+    return guarded([&] {
+        ctx_check(ctx);
+        Species& sp = species_at(ctx, species);
+        if (!keys_dev || !counts_dev || !offsets_dev || !perm_dev || !n_in_grid)
+            throw std::invalid_argument("bin: null argument");
+        cudaStream_t s = ctx->stream;
+        const GridView& g = ctx->g;
+        long long n = 0;
+        cuda_check(cudaMemcpyAsync(&n, ctx->count.p + species, sizeof(long long), cudaMemcpyDeviceToHost, s), "count");
+        cuda_check(cudaStreamSynchronize(s), "bin sync");
+        long long ncell = 1;
+        for (int a = 0; a < g.dim; ++a) ncell *= g.cells[a];
+        const unsigned sentinel = (unsigned)ncell;
+        ensure_sort_scratch(ctx, std::max<long long>(n, ncell));
+        const int cur = sp.cur;
+        if (n > 0) {
+            if (ctx->precision == PSUM_PIC_MIXED) {
+                { k_bin_keys_mixed<<<blocks_for(n, 256), 256, 0, s>>>(g, sp.key[cur].p, sp.off[0][cur].p, n, keys_dev,
+                                                                     ctx->sort.keyA.p, ctx->sort.idxA.p, sentinel); count_launch(); }
+            } else {
+                DevBuf<double> hi;
+                double h[3];
+                for (int a = 0; a < 3; ++a) h[a] = g.lo[a] + g.cells[a] * g.dx[a];
+                hi.upload(h, 3, s);
+                { k_bin_keys64<<<blocks_for(n, 256), 256, 0, s>>>(g, sp.pos64[0][cur].p,
+                                                                 g.dim > 1 ? sp.pos64[1][cur].p : nullptr,
+                                                                 g.dim > 2 ? sp.pos64[2][cur].p : nullptr, n, keys_dev,
+                                                                 ctx->sort.keyA.p, ctx->sort.idxA.p, sentinel, hi.p); count_launch(); }
+                cuda_check(cudaStreamSynchronize(s), "bin keys");
+            }
+        }
+        // counts per reference cell and their exclusive prefix
+        DevBuf<unsigned> cnt, off;
+        cnt.alloc(ncell);
+        off.alloc(ncell);
+        cuda_check(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned) * ncell, s), "memset");
+        if (n > 0) { k_hist_u32<<<blocks_for(n, 256), 256, 0, s>>>(keys_dev, n, cnt.p); count_launch(); }
+        DevBuf<unsigned> t1, t2;
+        t1.alloc((ncell + kScanBlock - 1) / kScanBlock + 1);
+        t2.alloc(16);
+        exclusive_scan_u32(cnt.p, off.p, ncell, t1.p, t2.p, s);
+        { k_u32_to_u64<<<blocks_for(ncell, 256), 256, 0, s>>>(cnt.p, counts_dev, ncell); count_launch(); }
+        { k_u32_to_u64<<<blocks_for(ncell, 256), 256, 0, s>>>(off.p, offsets_dev, ncell); count_launch(); }
+        unsigned long long total = 0;
+        if (n > 0) {
+            unsigned* skeys;
+            int* perm;
+            radix_sort(ctx, n, sentinel, &skeys, &perm);
+            // number of in-grid particles = sum of counts
+            unsigned last_off = 0, last_cnt = 0;
+            cuda_check(cudaMemcpyAsync(&last_off, off.p + ncell - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, s), "D2H");
+            cuda_check(cudaMemcpyAsync(&last_cnt, cnt.p + ncell - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, s), "D2H");
+            cuda_check(cudaStreamSynchronize(s), "bin sync");
+            total = (unsigned long long)last_off + last_cnt;
+            if (total > 0) { k_i32_to_u64<<<blocks_for((long long)total, 256), 256, 0, s>>>(perm, perm_dev, (long long)total); count_launch(); }
+        }
+        cuda_check(cudaStreamSynchronize(s), "bin sync");
+        *n_in_grid = total;
+    });
+}
+
+EXPORT int psum_pic_deposit(psum_pic_ctx* ctx) {
+    return guarded([&] {
+        ctx_check(ctx);
+        deposit_all(ctx);
+    });
+}
+
+EXPORT int psum_pic_rho(psum_pic_ctx* ctx, double background, double* rho_dev) {
+    return guarded([&] {
+        ctx_check(ctx);
+        rho_into(ctx, background, rho_dev, -1, true);
+    });
+}
+
+EXPORT int psum_pic_density(psum_pic_ctx* ctx, int species, double* n_dev) {
+    return guarded([&] {
+        ctx_check(ctx);
+        species_at(ctx, species);
+        rho_into(ctx, 0.0, n_dev, species, false);
+    });
+}
+
+EXPORT int psum_pic_push(psum_pic_ctx* ctx, const double* phi_dev, double dt, int pusher, const double* B) {
+    return guarded([&] {
+        ctx_check(ctx);
+        push_all(ctx, phi_dev, dt, pusher, B);
+    });
+}
+
+EXPORT int psum_pic_get_losses(psum_pic_ctx* ctx, unsigned long long* losses_host, int reset) {
+    return guarded([&] {
+        ctx_check(ctx);
+        if (!losses_host) throw std::invalid_argument("get_losses: null output");
+        std::vector<unsigned long long> all(48);
+        cuda_check(cudaMemcpyAsync(all.data(), ctx->losses.p, sizeof(unsigned long long) * 48, cudaMemcpyDeviceToHost,
+                                   ctx->stream),
+                   "losses D2H");
+        cuda_check(cudaStreamSynchronize(ctx->stream), "losses sync");
+        const int D = ctx->g.dim;
+        for (int s = 0; s < (int)ctx->sp.size(); ++s)
+            for (int k = 0; k < 2 * D; ++k) losses_host[s * 2 * D + k] = all[s * 6 + k];
+        if (reset)
+            cuda_check(cudaMemsetAsync(ctx->losses.p, 0, sizeof(unsigned long long) * 48, ctx->stream), "memset");
+    });
+}
+
+namespace {
+struct PhaseTimer {
+    psum_pic_ctx* c;
+    int phase;
+    cudaEvent_t a = nullptr, b = nullptr;
+    PhaseTimer(psum_pic_ctx* ctx, int ph) : c(ctx), phase(ph) {
+        if (!c->timing) return;
+        cuda_check(cudaEventCreate(&a), "cudaEventCreate");
+        cuda_check(cudaEventCreate(&b), "cudaEventCreate");
+        cuda_check(cudaEventRecord(a, c->stream), "cudaEventRecord");
+    }
+    void stop() {
+        if (!c->timing) return;
+        cuda_check(cudaEventRecord(b, c->stream), "cudaEventRecord");
+        c->events.push_back({phase, {a, b}});
+    }
+};
+}  // namespace
+
+EXPORT int psum_pic_step(psum_pic_ctx* ctx, psum_field_solver_handle solver, double background, double* rho_dev,
+                         double* phi_dev, double dt, int pusher, const double* B) {
+    return guarded([&] {
+        ctx_check(ctx);
+        SolverBase* sv = solver_from_handle(solver);
+        if (!rho_dev || !phi_dev) throw std::invalid_argument("step: null field");
+        {
+            PhaseTimer t(ctx, 0);
+            rho_into(ctx, background, rho_dev, -1, true);
+            t.stop();
+        }
+        {
+            PhaseTimer t(ctx, 1);
+            solver_solve_async(sv, rho_dev, phi_dev, ctx->stream);
+            t.stop();
+        }
+        {
+            PhaseTimer t(ctx, 2);
+            push_all(ctx, phi_dev, dt, pusher, B);
+            t.stop();
+        }
+        ctx->steps++;
+        if (ctx->sort_interval > 0 && ctx->steps % ctx->sort_interval == 0) {
+            PhaseTimer t(ctx, 3);
+            sort_all(ctx);
+            t.stop();
+        }
+    });
+}
+
+EXPORT int psum_pic_set_timing(psum_pic_ctx* ctx, int enable) {
+    return guarded([&] {
+        ctx_check(ctx);
+        ctx->timing = enable != 0;
+    });
+}
+
+EXPORT int psum_pic_get_timing(psum_pic_ctx* ctx, double* ms_host, int* count_host, int reset) {
+    return guarded([&] {
+        ctx_check(ctx);
+        if (!ms_host) throw std::invalid_argument("get_timing: null output");
+        cuda_check(cudaStreamSynchronize(ctx->stream), "timing sync");
+        for (int p = 0; p < 4; ++p) {
+            ms_host[p] = 0.0;
+            if (count_host) count_host[p] = 0;
+        }
+        for (auto& e : ctx->events) {
+            float ms = 0.f;
+            cuda_check(cudaEventElapsedTime(&ms, e.second.first, e.second.second), "cudaEventElapsedTime");
+            ms_host[e.first] += ms;
+            if (count_host) count_host[e.first] += 1;
+        }
+        if (reset) ctx->drop_events();
+    });
+}
+
+EXPORT int psum_pic_diagnostics(psum_pic_ctx* ctx, const double* phi_dev, double epsilon, double* out_host) {
+    return guarded([&] {
+        ctx_check(ctx);
+        if (!out_host) throw std::invalid_argument("diagnostics: null output");
+        cudaStream_t s = ctx->stream;
+        const int ns = (int)ctx->sp.size();
+        std::vector<double> part(kDiagBlocks);
+        for (int si = 0; si < ns; ++si) {
+            Species& sp = *ctx->sp[si];
+            const int cur = sp.cur;
+            if (ctx->precision == PSUM_PIC_MIXED)
+                { k_kinetic_mixed<<<kDiagBlocks, 256, 0, s>>>(sp.key[cur].p, sp.vel[0][cur].p, sp.vel[1][cur].p,
+                                                          sp.vel[2][cur].p, ctx->count.p + si, sp.m * sp.w,
+                                                          ctx->partials.p); count_launch(); }
+            else
+                { k_kinetic64<<<kDiagBlocks, 256, 0, s>>>(sp.pos64[0][cur].p, sp.vel64[0][cur].p, sp.vel64[1][cur].p,
+                                                      sp.vel64[2][cur].p, ctx->count.p + si, sp.m * sp.w,
+                                                      ctx->partials.p); count_launch(); }
+            cuda_check(cudaMemcpyAsync(part.data(), ctx->partials.p, sizeof(double) * kDiagBlocks,
+                                       cudaMemcpyDeviceToHost, s),
+                       "D2H");
+            cuda_check(cudaStreamSynchronize(s), "diag sync");
+            double t = 0;
+            for (double v : part) t += v;
+            out_host[si] = t;
+        }
+        double fe = 0;
+        if (phi_dev) {
+            { k_field_energy<<<kDiagBlocks, 256, 0, s>>>(ctx->g, phi_dev, ctx->partials.p); count_launch(); }
+            cuda_check(cudaMemcpyAsync(part.data(), ctx->partials.p, sizeof(double) * kDiagBlocks,
+                                       cudaMemcpyDeviceToHost, s),
+                       "D2H");
+            cuda_check(cudaStreamSynchronize(s), "diag sync");
+            for (double v : part) fe += v;
+            double vol = 1;
+            for (int a = 0; a < ctx->g.dim; ++a) vol *= ctx->g.dx[a];
+            fe = 0.5 * epsilon * fe * vol;
+        }
+        out_host[ns] = fe;
+        double charge = 0;
+        for (int si = 0; si < ns; ++si) {
+            Species& sp = *ctx->sp[si];
+            cuda_check(cudaMemsetAsync(ctx->ipartials.p, 0, sizeof(long long), s), "memset");
+            { k_acc_sum<<<kDiagBlocks, 256, 0, s>>>(sp.acc.p, ctx->g.n_nodes, ctx->ipartials.p); count_launch(); }
+            long long tot = 0;
+            cuda_check(cudaMemcpyAsync(&tot, ctx->ipartials.p, sizeof(long long), cudaMemcpyDeviceToHost, s), "D2H");
+            cuda_check(cudaStreamSynchronize(s), "diag sync");
+            charge += sp.q * sp.w * std::ldexp((double)tot, -sp.dep_shift);
+        }
+        out_host[ns + 1] = charge;
+    });
+}
+
+EXPORT int psum_pic_device_errors(psum_pic_ctx* ctx, unsigned int* flags) {
+    return guarded([&] {
+        ctx_check(ctx);
+        if (!flags) throw std::invalid_argument("device_errors: null output");
+        unsigned v = 0;
+        cuda_check(cudaMemcpyAsync(&v, ctx->err.p, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        cuda_check(cudaMemsetAsync(ctx->err.p, 0, sizeof(unsigned), ctx->stream), "memset");
+        cuda_check(cudaStreamSynchronize(ctx->stream), "errors sync");
+        *flags = v;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,42 @@
+// pic_fp64.hpp -- launchers of the FP64 particle kernels (pic_fp64.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "pic_common.cuh"
+
+namespace psum_b200 {
+
+struct Push64Args {
+    GridView g;
+    double hi[3];
+    double* pos[3];
+    double* vel[3];
+    int* key;
+    const long long* count;
+    const double* phi;
+    double q_m, dt;
+    int pusher;
+    double B[3];
+    unsigned long long* acc;   // null: no deposit
+    double scale;
+    unsigned long long* losses;
+    unsigned* err;
+};
+
+struct Deposit64Args {
+    GridView g;
+    const double* pos[3];
+    const long long* count;
+    unsigned long long* acc;
+    double scale;
+};
+
+void launch_push64(const Push64Args& a, long long n_upper, cudaStream_t s);
+void launch_deposit64(const Deposit64Args& a, long long n_upper, cudaStream_t s);
+void launch_keys64(const GridView& g, double* const pos[3], int* key, const long long* count, long long n_upper,
+                   cudaStream_t s);
+
+}  // namespace psum_b200

@@ -1,0 +1,142 @@
+"""Python mirror of the particle-kernel set (include/psum_pic.h).
+
+``ParticleContext`` owns one ``psum_pic_ctx``: a grid (``simple_grid<D>``
+conventions), one or more species, and the device state.  It plays the role
+of PSuM's ``particle_group`` + ``device_field`` pair for the electrostatic
+step (src/particle_container/particle_group.hpp, src/field/device_field.hpp):
+load particles, push with the CIC gather, deposit, sort/bin by cell, and run
+whole steps through a solver handle.
+"""
+import ctypes as C
+
+import numpy as np
+
+from ._lib import GridDesc, SpeciesDesc, check, lib
+from .field_solver import _ptr
+
+MIXED, FP64 = 0, 1
+LEAPFROG, BORIS = 0, 1
+
+
+class ParticleContext:
+    def __init__(self, cells, lower, upper, periodic, precision=MIXED):
+        g = GridDesc()
+        g.dim = len(cells)
+        for a in range(3):
+            g.cells[a] = int(cells[a]) if a < g.dim else 1
+            g.lower[a] = float(lower[a]) if a < g.dim else 0.0
+            g.upper[a] = float(upper[a]) if a < g.dim else 1.0
+            g.periodic[a] = int(bool(periodic[a])) if a < g.dim else 0
+        self.desc = g
+        self.dim = g.dim
+        self.cells = list(cells)
+        self.precision = precision
+        self.n_nodes = int(np.prod([c + 1 for c in cells]))
+        self.species = []
+        h = C.c_void_p()
+        check(lib().psum_pic_create(C.byref(g), precision, C.byref(h)))
+        self.handle = h
+
+    def close(self):
+        if getattr(self, "handle", None):
+            check(lib().psum_pic_destroy(self.handle))
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream):
+        s = None if stream is None else (stream if isinstance(stream, int) else stream.cuda_stream)
+        check(lib().psum_pic_set_stream(self.handle, s))
+
+    def set_options(self, options):
+        check(lib().psum_pic_set_options(self.handle, options.encode()))
+
+    def add_species(self, charge, mass, weight, capacity):
+        d = SpeciesDesc(float(charge), float(mass), float(weight))
+        sid = C.c_int()
+        check(lib().psum_pic_add_species(self.handle, C.byref(d), int(capacity), C.byref(sid)))
+        self.species.append((charge, mass, weight))
+        return sid.value
+
+    def load(self, species, pos, vel):
+        """pos: (dim, n) float64, vel: (3, n) float64 host arrays (numpy) or
+        device tensors (torch, float64, contiguous)."""
+        if hasattr(pos, "data_ptr") and getattr(pos, "is_cuda", False):
+            n = pos.shape[1]
+            check(lib().psum_pic_load_device(self.handle, species, n, pos.data_ptr(), vel.data_ptr()))
+        else:
+            pos = np.ascontiguousarray(pos, np.float64)
+            vel = np.ascontiguousarray(vel, np.float64)
+            n = pos.shape[1]
+            check(lib().psum_pic_load(self.handle, species, n, _ptr(pos), _ptr(vel)))
+
+    def count(self, species):
+        ns, nv = C.c_ulonglong(), C.c_ulonglong()
+        check(lib().psum_pic_count(self.handle, species, C.byref(ns), C.byref(nv)))
+        return ns.value, nv.value
+
+    def get_state(self, species):
+        ns, _ = self.count(species)
+        pos = np.zeros((self.dim, ns))
+        vel = np.zeros((3, ns))
+        check(lib().psum_pic_get_state(self.handle, species, _ptr(pos), _ptr(vel)))
+        return pos, vel
+
+    def get_keys(self, species, out):
+        check(lib().psum_pic_get_keys(self.handle, species, _ptr(out)))
+
+    def sort(self):
+        check(lib().psum_pic_sort(self.handle))
+
+    def bin(self, species, keys, counts, offsets, perm):
+        n = C.c_ulonglong()
+        check(lib().psum_pic_bin(self.handle, species, _ptr(keys), _ptr(counts), _ptr(offsets), _ptr(perm),
+                                 C.byref(n)))
+        return n.value
+
+    def deposit(self):
+        check(lib().psum_pic_deposit(self.handle))
+
+    def rho(self, background, out):
+        check(lib().psum_pic_rho(self.handle, float(background), _ptr(out)))
+
+    def density(self, species, out):
+        check(lib().psum_pic_density(self.handle, species, _ptr(out)))
+
+    def push(self, phi, dt, pusher=LEAPFROG, B=(0.0, 0.0, 0.0)):
+        Bv = (C.c_double * 3)(*B)
+        check(lib().psum_pic_push(self.handle, _ptr(phi), float(dt), pusher, Bv))
+
+    def losses(self, reset=True):
+        out = np.zeros(len(self.species) * 2 * self.dim, np.uint64)
+        check(lib().psum_pic_get_losses(self.handle, _ptr(out), int(reset)))
+        return out.reshape(len(self.species), self.dim, 2)
+
+    def step(self, solver, background, rho, phi, dt, pusher=LEAPFROG, B=(0.0, 0.0, 0.0)):
+        Bv = (C.c_double * 3)(*B)
+        check(lib().psum_pic_step(self.handle, solver.handle, float(background), _ptr(rho), _ptr(phi), float(dt),
+                                  pusher, Bv))
+
+    def set_timing(self, enable=True):
+        check(lib().psum_pic_set_timing(self.handle, int(bool(enable))))
+
+    def get_timing(self, reset=True):
+        """Accumulated ms and counts per step phase: rho, solve, push, sort."""
+        ms = np.zeros(4)
+        cnt = np.zeros(4, np.int32)
+        check(lib().psum_pic_get_timing(self.handle, _ptr(ms), _ptr(cnt), int(reset)))
+        return dict(zip(("rho", "solve", "push", "sort"), zip(ms.tolist(), cnt.tolist())))
+
+    def diagnostics(self, phi, epsilon):
+        out = np.zeros(len(self.species) + 2)
+        check(lib().psum_pic_diagnostics(self.handle, _ptr(phi), float(epsilon), _ptr(out)))
+        return {"kinetic": out[:len(self.species)].copy(), "field": out[-2], "charge": out[-1]}
+
+    def device_errors(self):
+        f = C.c_uint()
+        check(lib().psum_pic_device_errors(self.handle, C.byref(f)))
+        return f.value

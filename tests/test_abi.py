@@ -1,0 +1,123 @@
+"""C-ABI boundary and host logic, without a GPU: symbol export, registry,
+option grammar, status codes, and bit-exact FD operator assembly."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import psum_b200 as P
+from oracle import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for h in ("psum_field_solver.h", "psum_pic.h"):
+        text = open(os.path.join(ROOT, "include", h)).read()
+        for m in re.finditer(r"EXPORT\s+[\w\s\*]+?\b(\w+)\s*\(", text):
+            names.add(m.group(1))
+    return names
+
+
+def test_every_declared_symbol_is_exported():
+    names = declared_symbols()
+    assert {"register_solver", "get_solver_funcs", "psum_mg_solve", "psum_pic_step"} <= names
+    lib = P.lib()
+    for n in sorted(names):
+        assert hasattr(lib, n), n
+        assert n in P.PROTOTYPES, n
+
+
+def test_registry_names_and_unknown():
+    for name in ("cuda_multigrid32f_gpu", "cuda_multigrid64_gpu"):
+        assert bool(P.registered_table(name).init)
+        assert bool(P.registered_table(name).solve)
+        assert bool(P.registered_table(name).free)
+    assert not bool(P.registered_table("sycl_multigrid32f_gpu").init)   # registry.cpp:17-21
+
+
+def test_register_solver_roundtrip():
+    t = P.registered_table("cuda_multigrid64_gpu")
+    P.lib().register_solver(b"alias_for_test", t)
+    assert bool(P.registered_table("alias_for_test").init)
+
+
+def test_option_grammar_and_errors():
+    s = P.solver_backend("cuda_multigrid32f_gpu")
+    s.set_options("I 17 J 17 depth 3 pre_relax 2 post_relax 2 max_cycles 8 num_conv_mask 8 num_threads 4 foo 3")
+    s.set_options("tol 1e-8 correction_interval 2 periodic_I 1")
+    for bad in ("correction_interval 0", "tol -1", "depth x", "max_cycles"):
+        with pytest.raises(P.PsumError) as e:
+            s.set_options(bad)
+        assert e.value.code == 1
+    # solve before set_matrix -> PSUM_ERR_NOT_READY
+    code = P.lib().psum_mg_solve(s.handle, None, None)
+    assert code == 2
+
+
+def test_unknown_backend_and_null_handle():
+    with pytest.raises(P.PsumError):
+        P.solver_backend("eigen_sparselu_cpu")
+    empty = P.solver_backend()
+    with pytest.raises(P.PsumError):
+        empty.set_options("I 3")
+
+
+@pytest.mark.parametrize("case", ["2d_dirichlet", "2d_periodic_pin", "3d_periodic_pin", "2d_aniso_eps"])
+def test_assembly_bit_identical_to_oracle(case):
+    if case == "2d_dirichlet":
+        g = P.simple_grid((0, 0), (1, 1), (24, 24))
+        fixed = np.unique(np.concatenate([P.Dirichlet_line(g, d, 0)[0] for d in "NSEW"]))
+        eps = 8.854e-12
+    elif case == "2d_periodic_pin":
+        g = P.simple_grid((0.5, 0.5), (63.5, 63.5), (63, 63))
+        fixed, eps = np.array([0], np.uint64), 1.0
+    elif case == "3d_periodic_pin":
+        g = P.simple_grid((0.5,) * 3, (15.5,) * 3, (15, 15, 15))
+        fixed, eps = np.array([0], np.uint64), 1.0
+    else:
+        g = P.simple_grid((0.0, -1.0), (3.0, 2.0), (17, 9))
+        fixed = P.Dirichlet_line(g, "W", 0)[0]
+        eps = 2.5
+    r, c, v = P.assemble_poisson(g, fixed, eps)
+    r2, c2, v2 = O.poisson_assemble(g.cells, g.lower, g.upper, eps, fixed)
+    assert (r == r2).all() and (c == c2).all()
+    assert (v.view(np.int64) == v2.view(np.int64)).all()
+
+
+def test_dirichlet_creators_match_reference_indexing():
+    g = P.simple_grid((0, 0), (4, 3), (4, 3))
+    # Dirichlet.hpp:58-99: S = j=0 (stride J+1), N = j=J, W = i=0 (first J+1), E = i=I
+    assert P.Dirichlet_line(g, "S", 0)[0].tolist() == [0, 4, 8, 12, 16]
+    assert P.Dirichlet_line(g, "N", 0)[0].tolist() == [3, 7, 11, 15, 19]
+    assert P.Dirichlet_line(g, "W", 0)[0].tolist() == [0, 1, 2, 3]
+    assert P.Dirichlet_line(g, "E", 0)[0].tolist() == [16, 17, 18, 19]
+    g3 = P.simple_grid((0, 0, 0), (2, 2, 2), (2, 2, 2))
+    assert len(P.Dirichlet_plane(g3, "Zpos", 1.0)[0]) == 9
+    assert all(i % 3 == 2 for i in P.Dirichlet_plane(g3, "Zpos", 1.0)[0].tolist())
+
+
+def test_assembly_rejects_bad_input():
+    with pytest.raises(P.PsumError):
+        P.assemble_poisson(P.simple_grid((0, 0), (1, 1), (4, 4)), [1000], 1.0)
+    nnz = C.c_ulonglong()
+    cells = np.array([4, 4, 1], np.int32)
+    lo = np.zeros(3)
+    hi = np.ones(3)
+    code = P.lib().psum_poisson_assemble(4, cells.ctypes.data, lo.ctypes.data, hi.ctypes.data, 1.0, 0, None,
+                                         C.byref(nnz), None, None, None)
+    assert code == 1
+
+
+def test_pic_create_rejects_bad_grid_without_gpu():
+    g = P._lib.GridDesc()
+    g.dim = 4
+    h = C.c_void_p()
+    assert P.lib().psum_pic_create(C.byref(g), 0, C.byref(h)) == 1
+    g.dim = 2
+    g.cells[0] = 0
+    assert P.lib().psum_pic_create(C.byref(g), 0, C.byref(h)) == 1
+    assert b"cells" in P.lib().psum_last_error()

@@ -1,0 +1,354 @@
+"""GPU parity of the particle-kernel set against the FP64 oracle (through the C ABI).
+
+FP64 mode: positions, velocities, cell keys, loss counts, binning and sort
+permutations are compared bit-exactly.  Mixed mode (int32 cell + FP32 offset,
+FP32 velocity): fields and particle states within the stated tolerances,
+cell keys exactly except for particles within FP32 reach of a cell face.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import psum_b200 as P
+from oracle import oracle as O
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "known_answers.npz"))
+
+
+def dev(a, dtype=torch.float64):
+    return torch.tensor(np.asarray(a), device="cuda", dtype=dtype)
+
+
+def random_particles(rng, n, lo, hi, vth=1.0):
+    dim = len(lo)
+    pos = np.stack([rng.uniform(lo[a], hi[a], n) for a in range(dim)])
+    vel = rng.normal(0.0, vth, size=(3, n))
+    return pos, vel
+
+
+def make_case(kind, precision, seed=0, n=20000):
+    rng = np.random.default_rng(seed)
+    if kind == "2d_absorb":
+        cells, lo, hi, per = (32, 24), (0.0, 0.0), (32.0, 24.0), (0, 0)
+        plo, phi_ = lo, hi
+    elif kind == "2d_periodic":
+        cells, lo, hi, per = (63, 63), (0.5, 0.5), (63.5, 63.5), (1, 1)
+        plo, phi_ = (0.0, 0.0), (64.0, 64.0)
+    elif kind == "2d_mixed_bc":
+        cells, lo, hi, per = (20, 16), (0.0, -2.0), (5.0, 2.0), (0, 1)
+        plo, phi_ = (0.0, -2.0), (5.0, 2.0 + 4.0 / 16)
+    else:  # 3d_periodic
+        cells, lo, hi, per = (15, 15, 15), (0.5,) * 3, (15.5,) * 3, (1, 1, 1)
+        plo, phi_ = (0.0,) * 3, (16.0,) * 3
+    ctx = P.ParticleContext(cells, lo, hi, per, precision)
+    g = O.make_grid(cells, lo, hi, per)
+    pos, vel = random_particles(rng, n, plo, phi_)
+    nn = int(np.prod([c + 1 for c in cells]))
+    phi = rng.normal(0.0, 0.3, nn)
+    return ctx, g, pos, vel, phi
+
+
+def wrap_into(pos, g):
+    """Positions into [lo, lo + period) on periodic axes (the oracle's convention)."""
+    out = pos.copy()
+    for a in range(g.dim):
+        if g.periodic[a]:
+            dx = (g.upper[a] - g.lower[a]) / g.cells[a]
+            L = (g.cells[a] + 1) * dx
+            out[a] = g.lower[a] + np.mod(out[a] - g.lower[a], L)
+    return out
+
+
+@pytest.mark.parametrize("kind", ["2d_absorb", "2d_periodic", "2d_mixed_bc", "3d_periodic"])
+@pytest.mark.parametrize("pusher", [P.LEAPFROG, P.BORIS])
+def test_fp64_push_bit_exact(kind, pusher):
+    ctx, g, pos, vel, phi = make_case(kind, P.FP64, seed=11)
+    pos = wrap_into(pos, g)
+    qm, dt, B = -1.0, 0.2, (0.3, -0.2, 0.5)
+    sp = ctx.add_species(-1.0, 1.0, 1.0, pos.shape[1])
+    ctx.load(sp, pos, vel)
+    ctx.push(dev(phi), dt, pusher, B)
+    got_pos, got_vel = ctx.get_state(sp)
+    exp_pos, exp_vel, exp_loss = O.push(g, pos, vel, phi, qm, dt, pusher, B)
+    assert np.array_equal(np.isnan(got_pos[0]), np.isnan(exp_pos[0]))
+    alive = ~np.isnan(exp_pos[0])
+    assert (got_pos[:, alive].view(np.int64) == exp_pos[:, alive].view(np.int64)).all()
+    assert (got_vel.view(np.int64) == exp_vel.view(np.int64)).all()
+    assert (ctx.losses()[0] == exp_loss).all()
+    # cell keys of the survivors (internal lattice) follow from the positions
+    keys = torch.zeros(pos.shape[1], dtype=torch.int32, device="cuda")
+    ctx.get_keys(sp, keys)
+    keys = keys.cpu().numpy()
+    assert (keys[~alive] == -1).all()
+
+
+def internal_keys(pos, g):
+    M = [g.cells[a] + 1 if g.periodic[a] else g.cells[a] for a in range(g.dim)]
+    key = np.zeros(pos.shape[1], np.int64)
+    for a in range(g.dim):
+        dx = (g.upper[a] - g.lower[a]) / g.cells[a]
+        c = np.clip(np.floor((pos[a] - g.lower[a]) * (1.0 / dx)).astype(np.int64), 0, M[a] - 1)
+        key = key * M[a] + c
+    return key
+
+
+@pytest.mark.parametrize("kind", ["2d_absorb", "2d_periodic", "3d_periodic"])
+def test_mixed_push_within_tolerance(kind):
+    ctx, g, pos, vel, phi = make_case(kind, P.MIXED, seed=12)
+    pos = wrap_into(pos, g)
+    qm, dt = -1.0, 0.2
+    sp = ctx.add_species(-1.0, 1.0, 1.0, pos.shape[1])
+    ctx.load(sp, pos, vel)
+    # the loaded state is the FP64 input rounded to (cell, FP32 offset, FP32 v)
+    pos0, vel0 = ctx.get_state(sp)
+    assert np.abs(pos0 - pos).max() < 1e-6
+    ctx.push(dev(phi), dt)
+    got_pos, got_vel = ctx.get_state(sp)
+    exp_pos, exp_vel, exp_loss = O.push(g, pos0, vel0, phi, qm, dt)
+    dead_exp = np.isnan(exp_pos[0])
+    dead_got = np.isnan(got_pos[0])
+    # a particle within FP32 reach of an absorbing wall may go either way
+    ambiguous = np.zeros_like(dead_exp)
+    for a in range(g.dim):
+        if not g.periodic[a]:
+            ambiguous |= (np.abs(exp_pos[a] - g.lower[a]) < 1e-5) | (np.abs(exp_pos[a] - g.upper[a]) < 1e-5)
+    assert (dead_exp[~ambiguous] == dead_got[~ambiguous]).all()
+    ok = ~dead_exp & ~dead_got
+    d = got_pos[:, ok] - exp_pos[:, ok]
+    for a in range(g.dim):
+        if g.periodic[a]:
+            dx = (g.upper[a] - g.lower[a]) / g.cells[a]
+            L = (g.cells[a] + 1) * dx
+            d[a] = (d[a] + L / 2) % L - L / 2
+    assert np.abs(d).max() < 2e-6
+    assert np.abs(got_vel[:, ok] - exp_vel[:, ok]).max() < 2e-5
+    # cell keys: identical except where the FP64 position is within 1e-5 cells of a face
+    kg = torch.zeros(pos.shape[1], dtype=torch.int32, device="cuda")
+    ctx.get_keys(sp, kg)
+    kg = kg.cpu().numpy()
+    ke = internal_keys(exp_pos[:, ok], g)
+    near = np.zeros(ok.sum(), bool)
+    for a in range(g.dim):
+        dx = (g.upper[a] - g.lower[a]) / g.cells[a]
+        u = (exp_pos[a, ok] - g.lower[a]) / dx
+        near |= np.abs(u - np.round(u)) < 1e-5
+    assert (kg[ok][~near] == ke[~near]).all()
+
+
+@pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
+@pytest.mark.parametrize("kind", ["2d_absorb", "2d_periodic", "3d_periodic"])
+def test_deposit_matches_oracle(precision, kind):
+    ctx, g, pos, vel, phi = make_case(kind, precision, seed=13, n=50000)
+    pos = wrap_into(pos, g)
+    w = 0.37
+    sp = ctx.add_species(1.0, 1.0, w, pos.shape[1])
+    ctx.load(sp, pos, vel)
+    pos0, _ = ctx.get_state(sp)
+    ctx.deposit()
+    nn = ctx.n_nodes
+    dens = dev(np.zeros(nn))
+    ctx.density(sp, dens)
+    vol = np.prod([(g.upper[a] - g.lower[a]) / g.cells[a] for a in range(g.dim)])
+    exp = O.deposit(g, pos0, w / vol, nn)
+    got = dens.cpu().numpy()
+    tol = 1e-12 if precision == P.FP64 else 2e-6
+    assert np.abs(got - exp).max() <= tol * np.abs(exp).max()
+    # total deposited charge: CIC weights sum to one per particle
+    diag = ctx.diagnostics(None, 1.0)
+    n_valid = (~np.isnan(pos0[0])).sum()
+    assert abs(diag["charge"] - n_valid * w) < 1e-6 * n_valid * w
+
+
+def test_golden_known_answers_fp64():
+    ctx = P.ParticleContext((16, 16), (0, 0), (16, 16), (0, 0), P.FP64)
+    qm, dt = GOLD["push_qm_dt"]
+    sp = ctx.add_species(qm, 1.0, 1.0, GOLD["push_pos0"].shape[1])
+    ctx.load(sp, GOLD["push_pos0"], GOLD["push_vel0"])
+    ctx.push(dev(GOLD["push_phi"]), dt)
+    pos, vel = ctx.get_state(sp)
+    np.testing.assert_allclose(pos, GOLD["push_pos1"], rtol=0, atol=1e-13)
+    np.testing.assert_allclose(vel, GOLD["push_vel1"], rtol=0, atol=1e-13)
+    # deposit
+    c2 = P.ParticleContext((8, 8), (0, 0), (1, 1), (0, 0), P.FP64)
+    s2 = c2.add_species(1.0, 1.0, 1.0 / 64, 3)   # weight/volume = 1
+    c2.load(s2, GOLD["dep_points"].T, np.zeros((3, 3)))
+    c2.deposit()
+    d = dev(np.zeros(81))
+    c2.density(s2, d)
+    np.testing.assert_allclose(d.cpu().numpy(), GOLD["dep_rho"], atol=1e-12)
+
+
+@pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
+def test_binning_golden_and_oracle(precision):
+    # golden binning case (grid_mapped_device_vector.hpp:47-87); dx = 1 grids
+    ctx = P.ParticleContext((4, 3), (0, 0), (4, 3), (0, 0), precision)
+    bp = GOLD["bin_pos"]
+    n = bp.shape[1]
+    sp = ctx.add_species(1.0, 1.0, 1.0, n)
+    ctx.load(sp, bp, np.zeros((3, n)))
+    keys = torch.zeros(n, dtype=torch.int64, device="cuda")
+    counts = torch.zeros(12, dtype=torch.int64, device="cuda")
+    offs = torch.zeros(12, dtype=torch.int64, device="cuda")
+    perm = torch.zeros(n, dtype=torch.int64, device="cuda")
+    m = ctx.bin(sp, keys, counts, offs, perm)
+    assert (keys.cpu().numpy() == GOLD["bin_keys"]).all()
+    assert (counts.cpu().numpy() == GOLD["bin_counts"].astype(np.int64)).all()
+    assert (offs.cpu().numpy() == GOLD["bin_offsets"].astype(np.int64)).all()
+    assert (perm.cpu().numpy()[:m] == GOLD["bin_perm"].astype(np.int64)).all()
+    # a larger random case against the oracle
+    rng = np.random.default_rng(14)
+    cells = (40, 30)
+    ctx = P.ParticleContext(cells, (0.0, 0.0), (40.0, 30.0), (0, 0), precision)
+    N = 100000
+    pos = np.stack([rng.uniform(-1, 41, N), rng.uniform(-1, 31, N)])
+    sp = ctx.add_species(1.0, 1.0, 1.0, N)
+    ctx.load(sp, pos, np.zeros((3, N)))
+    pos0, _ = ctx.get_state(sp)
+    g = O.make_grid(cells, (0, 0), (40, 30), (0, 0))
+    ek, ec, eo, ep = O.bin_particles(g, pos0)
+    keys = torch.zeros(N, dtype=torch.int64, device="cuda")
+    counts = torch.zeros(1200, dtype=torch.int64, device="cuda")
+    offs = torch.zeros(1200, dtype=torch.int64, device="cuda")
+    perm = torch.zeros(N, dtype=torch.int64, device="cuda")
+    m = ctx.bin(sp, keys, counts, offs, perm)
+    assert m == ep.size
+    assert (keys.cpu().numpy() == ek).all()
+    assert (counts.cpu().numpy() == ec.astype(np.int64)).all()
+    assert (offs.cpu().numpy() == eo.astype(np.int64)).all()
+    assert (perm.cpu().numpy()[:m] == ep.astype(np.int64)).all()
+
+
+@pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
+def test_sort_is_stable_by_cell_and_compacts(precision):
+    ctx, g, pos, vel, phi = make_case("2d_absorb", precision, seed=15, n=30000)
+    sp = ctx.add_species(-1.0, 1.0, 1.0, pos.shape[1])
+    pos = pos.copy()
+    pos[0, ::7] = np.nan          # invalid particles (validator.hpp:19-26)
+    ctx.load(sp, pos, vel)
+    before_pos, before_vel = ctx.get_state(sp)
+    keys = torch.zeros(pos.shape[1], dtype=torch.int32, device="cuda")
+    ctx.get_keys(sp, keys)
+    k = keys.cpu().numpy().astype(np.int64)
+    k[k < 0] = np.iinfo(np.int64).max
+    order = np.argsort(k, kind="stable")
+    n_valid = int((keys.cpu().numpy() >= 0).sum())
+    ctx.sort()
+    ns, nv = ctx.count(sp)
+    assert ns == n_valid and nv == n_valid
+    after_pos, after_vel = ctx.get_state(sp)
+    exp_pos = before_pos[:, order[:n_valid]]
+    exp_vel = before_vel[:, order[:n_valid]]
+    assert (after_pos.view(np.int64) == exp_pos.view(np.int64)).all()
+    assert (after_vel.view(np.int64) == exp_vel.view(np.int64)).all()
+
+
+def test_full_step_fp64_matches_oracle():
+    # one electrostatic step: rho -> solve -> push (+deposit) on a periodic
+    # 2-D grid pinned at node 0, against the oracle with a direct solve
+    import scipy.sparse as sps
+    import scipy.sparse.linalg as spl
+    rng = np.random.default_rng(16)
+    n1 = 32
+    cells, lo, hi = (n1 - 1, n1 - 1), (0.5, 0.5), (n1 - 0.5, n1 - 0.5)
+    ctx = P.ParticleContext(cells, lo, hi, (1, 1), P.FP64)
+    N = 64 * n1 * n1
+    pos = np.stack([rng.uniform(0, n1, N), rng.uniform(0, n1, N)])
+    vel = rng.normal(size=(3, N))
+    w = 1.0 / 64
+    sp = ctx.add_species(-1.0, 1.0, w, N)
+    ctx.load(sp, pos, vel)
+    pos0, vel0 = ctx.get_state(sp)
+    ctx.deposit()
+    gsolv = P.Poisson_solver_2d()
+    grid = P.simple_grid(lo, hi, cells)
+    gsolv.set_options(f"I {n1} J {n1} depth 4 pre_relax 2 post_relax 2 max_cycles 60 correction_interval 4 "
+                      f"tol 1e-13 periodic_I 1 periodic_J 1")
+    gsolv.init("cuda_multigrid64_gpu", grid, P.Poisson_solver_2d.Cartesian, [P.Dirichlet_nodes(grid, [(0, 0)], 0.0)],
+               1.0)
+    gsolv.make_righthand_item()
+    rho = dev(np.zeros(n1 * n1))
+    phi = dev(np.zeros(n1 * n1))
+    ctx.step(gsolv.backend, 1.0, rho, phi, 0.1)
+    ctx.sort()
+    # oracle: deposit, solve directly, push
+    g = O.make_grid(cells, lo, hi, (1, 1))
+    rho_e = 1.0 + O.deposit(g, pos0, -1.0 * w, n1 * n1)
+    r, c, v = gsolv.coeff_matrix()
+    A = sps.csr_matrix((v, (r.astype(np.int64), c.astype(np.int64))), shape=(n1 * n1,) * 2)
+    b = rho_e.copy()
+    b[0] = 0.0
+    phi_e = spl.spsolve(A.tocsc(), b)
+    phi_g = phi.cpu().numpy()
+    assert np.abs(phi_g - phi_e).max() < 1e-9 * np.abs(phi_e).max()
+    exp_pos, exp_vel, _ = O.push(g, pos0, vel0, phi_g, -1.0, 0.1)
+    got_pos, got_vel = ctx.get_state(sp)
+    # after the sort the order follows the internal keys; compare as sets via lexsort
+    ke = np.lexsort((exp_vel[2], exp_vel[1], exp_vel[0]))
+    kg = np.lexsort((got_vel[2], got_vel[1], got_vel[0]))
+    assert np.abs(got_vel[:, kg] - exp_vel[:, ke]).max() == 0.0
+    assert np.abs(got_pos[:, kg] - exp_pos[:, ke]).max() == 0.0
+
+
+@pytest.mark.parametrize("precision", [P.MIXED, P.FP64])
+def test_repeat_runs_bitwise_identical(precision):
+    outs = []
+    for _ in range(2):
+        rng = np.random.default_rng(17)
+        cells = (64, 64)
+        ctx = P.ParticleContext(cells, (0, 0), (64, 64), (0, 0), precision)
+        N = 256 * 64 * 64 // 4
+        e = ctx.add_species(-1.0, 1.0, 1.0 / 64, N)
+        i = ctx.add_species(1.0, 1836.0, 1.0 / 64, N)
+        ctx.load(e, np.stack([rng.uniform(0, 64, N), rng.uniform(0, 64, N)]), rng.normal(size=(3, N)))
+        ctx.load(i, np.stack([rng.uniform(0, 64, N), rng.uniform(0, 64, N)]), rng.normal(size=(3, N)) / 42.8)
+        ctx.deposit()
+        grid = P.simple_grid((0, 0), (64, 64), cells)
+        ps = P.Poisson_solver_2d()
+        ps.set_options("I 65 J 65 depth 5 pre_relax 2 post_relax 2 max_cycles 12 correction_interval 3 tol 1e-8")
+        ps.init("cuda_multigrid32f_gpu", grid, P.Poisson_solver_2d.Cartesian,
+                [P.Dirichlet_line(grid, d, 0.0) for d in "NSEW"], 1.0)
+        ps.make_righthand_item()
+        rho = dev(np.zeros(65 * 65))
+        phi = dev(np.zeros(65 * 65))
+        for _s in range(3):
+            ctx.step(ps.backend, 0.0, rho, phi, 0.1)
+        torch.cuda.synchronize()
+        pe, ve = ctx.get_state(e)
+        outs.append((rho.cpu().numpy(), phi.cpu().numpy(), pe, ve, ctx.losses()))
+    a, b = outs
+    for x, y in zip(a[:4], b[:4]):
+        assert x.shape == y.shape
+        assert (np.nan_to_num(x).view(np.int64) == np.nan_to_num(y).view(np.int64)).all()
+    assert (a[4] == b[4]).all()
+
+
+def test_nonfinite_velocity_flags_error_without_fault():
+    ctx = P.ParticleContext((8, 8), (0, 0), (8, 8), (1, 1), P.MIXED)
+    sp = ctx.add_species(-1.0, 1.0, 1.0, 16)
+    rng = np.random.default_rng(18)
+    pos = rng.uniform(0, 8, (2, 16))
+    vel = rng.normal(size=(3, 16))
+    vel[0, 3] = np.nan
+    vel[1, 5] = np.inf
+    ctx.load(sp, pos, vel)
+    ctx.push(dev(np.zeros(81)), 0.1)
+    flags = ctx.device_errors()
+    assert flags & (1 << 7)
+    p, _ = ctx.get_state(sp)
+    assert np.isnan(p[0, 3]) and np.isnan(p[0, 5])
+    assert np.isfinite(np.delete(p[0], [3, 5])).all()
+    assert ctx.device_errors() == 0       # the word resets after reading
+    ctx.push(dev(np.zeros(81)), 0.1)      # the context keeps working
+    torch.cuda.synchronize()
+
+
+def test_capacity_overflow_is_an_error_status():
+    ctx = P.ParticleContext((8, 8), (0, 0), (8, 8), (0, 0), P.MIXED)
+    sp = ctx.add_species(-1.0, 1.0, 1.0, 8)
+    with pytest.raises(P.PsumError) as e:
+        ctx.load(sp, np.zeros((2, 100)) + 1.0, np.zeros((3, 100)))
+    assert e.value.code == 6

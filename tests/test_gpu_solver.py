@@ -1,0 +1,207 @@
+"""GPU parity of the multigrid backends against the FP64 oracle (through the C ABI)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spl
+
+import psum_b200 as P
+from oracle import oracle as O
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+def dev(a):
+    return torch.tensor(np.asarray(a, np.float64), device="cuda")
+
+
+def csr(rows, cols, vals, n):
+    return sp.csr_matrix((vals, (rows.astype(np.int64), cols.astype(np.int64))), shape=(n, n))
+
+
+def dirichlet_case(N, eps=1.0, seed=0):
+    g = P.simple_grid((0, 0), (1, 1), (N, N))
+    fixed = np.unique(np.concatenate([P.Dirichlet_line(g, d, 0)[0] for d in "NSEW"]))
+    r, c, v = P.assemble_poisson(g, fixed, eps)
+    n = (N + 1) ** 2
+    rng = np.random.default_rng(seed)
+    b = rng.normal(size=n)
+    b[fixed.astype(np.int64)] = 0.0
+    return g, fixed, r, c, v, n, b
+
+
+def periodic_case(dim, n1, seed=1):
+    g = P.simple_grid((0.5,) * dim, (n1 - 0.5,) * dim, (n1 - 1,) * dim)
+    r, c, v = P.assemble_poisson(g, [0], 1.0)
+    n = n1 ** dim
+    rng = np.random.default_rng(seed)
+    b = rng.normal(size=n)
+    b -= b.mean()
+    b[0] = 0.0
+    return g, r, c, v, n, b
+
+
+@pytest.mark.parametrize("N,depth,cycles", [(32, 3, 1), (32, 3, 6), (64, 4, 5)])
+def test_fp64_vcycles_match_oracle(N, depth, cycles):
+    g, fixed, r, c, v, n, b = dirichlet_case(N)
+    s = P.solver_backend("cuda_multigrid64_gpu")
+    s.set_options(f"I {N + 1} J {N + 1} K 1 depth {depth} pre_relax 2 post_relax 2 max_cycles {cycles}")
+    s.set_matrix(n, n, r.size, r, c, v)
+    x0 = np.random.default_rng(5).normal(size=n) * 0.1
+    bd, xd = dev(b), dev(x0)
+    s.solve(bd, xd)
+    mg = O.Multigrid(r, c, v, n, N + 1, N + 1, 1, depth)
+    ref = mg.vcycles(b, x0, cycles, 2, 2)
+    got = xd.cpu().numpy()
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-12
+
+
+def test_fp64_vcycles_match_oracle_3d_periodic():
+    g, r, c, v, n, b = periodic_case(3, 16)
+    s = P.solver_backend("cuda_multigrid64_gpu")
+    s.set_options("I 16 J 16 K 16 depth 3 pre_relax 2 post_relax 1 max_cycles 4 periodic_I 1 periodic_J 1 periodic_K 1")
+    s.set_matrix(n, n, r.size, r, c, v)
+    bd, xd = dev(b), dev(np.zeros(n))
+    s.solve(bd, xd)
+    mg = O.Multigrid(r, c, v, n, 16, 16, 16, 3, periodic=(1, 1, 1))
+    ref = mg.vcycles(b, np.zeros(n), 4, 2, 1)
+    assert np.linalg.norm(xd.cpu().numpy() - ref) / np.linalg.norm(ref) < 1e-12
+    info = s.hierarchy_info()
+    assert info["levels"] == 4 and info["coarse_rows"] == 8
+
+
+def test_mixed_refinement_converges_to_direct():
+    g, fixed, r, c, v, n, b = dirichlet_case(128)
+    s = P.solver_backend("cuda_multigrid32f_gpu")
+    s.set_options("I 129 J 129 depth 5 pre_relax 2 post_relax 2 max_cycles 40 correction_interval 4 tol 1e-12")
+    s.set_matrix(n, n, r.size, r, c, v)
+    bd, xd = dev(b), dev(np.zeros(n))
+    code = s.solve(bd, xd)
+    st = s.last_stats()
+    direct = spl.spsolve(csr(r, c, v, n).tocsc(), b)
+    err = np.linalg.norm(xd.cpu().numpy() - direct) / np.linalg.norm(direct)
+    assert code == 0, st
+    assert st["rel_residual"] <= 1e-12
+    assert err < 1e-10
+    assert st["cycles"] < 40
+
+
+def test_mixed_matches_reference_mixed_algorithm():
+    # Same batches as the oracle's restatement of sycl_multigrid32f_gpu::solve:
+    # per-batch FP64 residual history agrees to FP32 roundoff.
+    g, fixed, r, c, v, n, b = dirichlet_case(64)
+    s = P.solver_backend("cuda_multigrid32f_gpu")
+    s.set_options("I 65 J 65 depth 4 pre_relax 2 post_relax 1 max_cycles 12 correction_interval 4")
+    s.set_matrix(n, n, r.size, r, c, v)
+    bd, xd = dev(b), dev(np.zeros(n))
+    s.solve(bd, xd)
+    mg = O.Multigrid(r, c, v, n, 65, 65, 1, 4)
+    ref, hist = mg.solve_mixed(b, np.zeros(n), 12, 4, 2, 1)
+    got = xd.cpu().numpy()
+    rel = mg.rel_residual(b, got)
+    assert rel < 10 * hist[-1] + 1e-12
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-6
+
+
+def test_manufactured_within_1e4_in_5_cycles():
+    # test_native_vs_mg_2d_manufactured.cpp:22-129 through the frontend mirror
+    N = 64
+    g = P.simple_grid((0, 0), (1, 1), (N, N))
+    ps = P.Poisson_solver_2d()
+    ps.set_options(f"I {N + 1} J {N + 1} K 1 depth 3 pre_relax 2 post_relax 2 max_cycles 5")
+    bcs = [P.Dirichlet_line(g, d, 0.0) for d in "NSEW"]
+    ps.init("cuda_multigrid64_gpu", g, P.Poisson_solver_2d.Cartesian, bcs)
+    x = np.linspace(0, 1, N + 1)
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    rho = (-8.854e-12 * (-2 * np.pi ** 2 * np.sin(np.pi * X) * np.sin(np.pi * Y))).ravel()
+    r, c, v = ps.coeff_matrix()
+    b = rho.copy()
+    b[ps.replace_idx.astype(np.int64)] = 0.0
+    direct = spl.spsolve(csr(r, c, v, (N + 1) ** 2).tocsc(), b)
+    rho_d, phi_d = dev(rho), dev(np.zeros_like(rho))
+    ps.solve(phi_d, rho_d)
+    got = phi_d.cpu().numpy()
+    assert np.linalg.norm(got - direct) / np.linalg.norm(direct) < 1e-4
+    # b is overwritten in place by set_source_replace (sycl_multigrid_gpu.cpp:98-118)
+    assert np.allclose(rho_d.cpu().numpy(), b)
+
+
+def test_source_addback_then_replace_order():
+    g, fixed, r, c, v, n, b = dirichlet_case(16)
+    s = P.solver_backend("cuda_multigrid64_gpu")
+    s.set_options("I 17 J 17 depth 2 max_cycles 1")
+    s.set_matrix(n, n, r.size, r, c, v)
+    s.set_source_addback([20, 20, 21], [1.0, 2.0, 4.0])
+    s.set_source_replace([21, 0], [7.0, -1.0])
+    bd, xd = dev(b), dev(np.zeros(n))
+    s.solve(bd, xd)
+    got = bd.cpu().numpy()
+    exp = b.copy()
+    exp[20] += 3.0
+    exp[21] = 7.0
+    exp[0] = -1.0
+    assert np.allclose(got, exp, rtol=0, atol=1e-15)
+
+
+def test_five_point_check_solvers_residual_gpu():
+    # check_solvers.cpp: n^2 interior unknowns, b = 1, max residual < 1e-7 on GPU
+    n = 63
+    h = 1.0 / (n + 1)
+    rows, cols, vals = [], [], []
+    for j in range(n):
+        for i in range(n):
+            idx = j * n + i
+            rows.append(idx); cols.append(idx); vals.append(4.0 / h / h)
+            for di, ok in ((-1, i > 0), (1, i < n - 1), (-n, j > 0), (n, j < n - 1)):
+                if ok:
+                    rows.append(idx); cols.append(idx + di); vals.append(-1.0 / h / h)
+    rows, cols, vals = np.array(rows, np.uint64), np.array(cols, np.uint64), np.array(vals)
+    N = n * n
+    for kind in ("cuda_multigrid64_gpu", "cuda_multigrid32f_gpu"):
+        s = P.solver_backend(kind)
+        s.set_options(f"I {n} J {n} depth 4 pre_relax 4 post_relax 2 max_cycles 40 tol 1e-13")
+        s.set_matrix(N, N, rows.size, rows, cols, vals)
+        bd, xd = dev(np.ones(N)), dev(np.zeros(N))
+        s.solve(bd, xd)
+        res = np.abs(csr(rows, cols, vals, N) @ xd.cpu().numpy() - 1.0).max()
+        assert res < 1e-7, (kind, res)
+
+
+def test_func_table_path_through_ctypes():
+    # the raw func_table, as check_solvers.cpp:177-260 drives it
+    t = P.registered_table("cuda_multigrid32f_gpu")
+    g, fixed, r, c, v, n, b = dirichlet_case(32)
+    h = t.init()
+    assert h
+    t.set_options(h, b"I 33 J 33 depth 3 max_cycles 20 tol 1e-10")
+    t.set_matrix(h, n, n, r.size, r.ctypes.data, c.ctypes.data, v.ctypes.data)
+    bd, xd = dev(b), dev(np.zeros(n))
+    t.solve(h, bd.data_ptr(), xd.data_ptr())
+    t.free(h)
+    direct = spl.spsolve(csr(r, c, v, n).tocsc(), b)
+    assert np.linalg.norm(xd.cpu().numpy() - direct) / np.linalg.norm(direct) < 1e-8
+
+
+def test_not_converged_status_and_tol_stop():
+    g, fixed, r, c, v, n, b = dirichlet_case(64)
+    s = P.solver_backend("cuda_multigrid32f_gpu")
+    s.set_options("I 65 J 65 depth 4 max_cycles 2 correction_interval 1 tol 1e-14")
+    s.set_matrix(n, n, r.size, r, c, v)
+    bd, xd = dev(b), dev(np.zeros(n))
+    assert s.solve(bd, xd) == 4        # PSUM_ERR_NOT_CONVERGED, x holds the last iterate
+    assert np.isfinite(xd.cpu().numpy()).all()
+
+
+def test_repeat_solves_bitwise_identical():
+    g, fixed, r, c, v, n, b = dirichlet_case(64)
+    s = P.solver_backend("cuda_multigrid32f_gpu")
+    s.set_options("I 65 J 65 depth 4 max_cycles 8 tol 1e-10")
+    s.set_matrix(n, n, r.size, r, c, v)
+    outs = []
+    for _ in range(2):
+        bd, xd = dev(b), dev(np.zeros(n))
+        s.solve(bd, xd)
+        outs.append(xd.cpu().numpy())
+    assert (outs[0].view(np.int64) == outs[1].view(np.int64)).all()
