@@ -33,6 +33,10 @@
  *
  * Bulk arguments named *_dev are device pointers; *_host are host pointers.
  * Every function returns a psum_status (include/psum_field_solver.h).
+ * Work is enqueued on the context's stream (psum_pic_set_stream); a *_dev
+ * argument of an asynchronous call (push, step, rho, density) must stay
+ * valid and unmodified until that stream reaches the call.  Calls that
+ * return host data, and the loads, synchronise the stream.
  */
 #ifndef PSUM_B200_PIC_H
 #define PSUM_B200_PIC_H
@@ -80,7 +84,8 @@ EXPORT int psum_pic_add_species(psum_pic_ctx* ctx, const psum_pic_species_desc* 
  * absorbing axis are loaded as invalid. */
 EXPORT int psum_pic_load(psum_pic_ctx* ctx, int species, unsigned long long n,
                          const double* pos_host, const double* vel_host);
-/* Same, from FP64 SoA device arrays (no host staging). */
+/* Same, from FP64 SoA device arrays (no host staging); returns after the
+ * arrays have been consumed, so the caller may free them right away. */
 EXPORT int psum_pic_load_device(psum_pic_ctx* ctx, int species, unsigned long long n,
                                 const double* pos_dev, const double* vel_dev);
 /* Current array length (valid + not yet compacted invalid) and valid count. */

@@ -1110,7 +1110,11 @@ EXPORT int psum_pic_load_device(psum_pic_ctx* ctx, int species, unsigned long lo
     return guarded([&] {
         ctx_check(ctx);
         if (n > 0 && (!pos_dev || !vel_dev)) throw std::invalid_argument("load: null device array");
+        // The caller may free or reuse pos_dev/vel_dev as soon as this returns
+        // (PSuM's particle_group::insert is synchronous as well).
+        cuda_check(cudaStreamSynchronize(ctx->stream), "load sync");   // prior work that may write them
         load_common(ctx, species, n, pos_dev, vel_dev);
+        cuda_check(cudaStreamSynchronize(ctx->stream), "load sync");
     });
 }
 

@@ -352,3 +352,21 @@ def test_capacity_overflow_is_an_error_status():
     with pytest.raises(P.PsumError) as e:
         ctx.load(sp, np.zeros((2, 100)) + 1.0, np.zeros((3, 100)))
     assert e.value.code == 6
+
+
+def test_load_device_buffers_reusable_immediately():
+    # the device load consumes its inputs before returning: overwriting the
+    # source tensors right after the call must not change the loaded state
+    rng = np.random.default_rng(19)
+    ctx = P.ParticleContext((64, 64), (0, 0), (64, 64), (0, 0), P.MIXED)
+    n = 1 << 20
+    sp = ctx.add_species(-1.0, 1.0, 1.0, n)
+    pos = rng.uniform(0, 64, (2, n))
+    vel = rng.normal(size=(3, n))
+    pd, vd = dev(pos), dev(vel)
+    ctx.load(sp, pd, vd)
+    pd.fill_(-5.0)
+    vd.fill_(1e30)
+    got_pos, got_vel = ctx.get_state(sp)
+    assert np.abs(got_pos - pos).max() < 1e-5
+    assert np.abs(got_vel - vel.astype(np.float32)).max() == 0.0
