@@ -33,10 +33,12 @@
  *
  * Bulk arguments named *_dev are device pointers; *_host are host pointers.
  * Every function returns a psum_status (include/psum_field_solver.h).
- * Work is enqueued on the context's stream (psum_pic_set_stream); a *_dev
- * argument of an asynchronous call (push, step, rho, density) must stay
- * valid and unmodified until that stream reaches the call.  Calls that
- * return host data, and the loads, synchronise the stream.
+ * Work is enqueued on the context's stream (psum_pic_set_stream); every
+ * *_dev input must be complete with respect to that stream when the call is
+ * made (the library does not wait for other streams), and a *_dev argument
+ * of an asynchronous call (push, step, rho, density) must stay valid and
+ * unmodified until the stream reaches the call.  Calls that return host
+ * data, and the loads, synchronise the context's stream before returning.
  */
 #ifndef PSUM_B200_PIC_H
 #define PSUM_B200_PIC_H
@@ -68,7 +70,8 @@ typedef struct psum_pic_ctx psum_pic_ctx;
 
 EXPORT int psum_pic_create(const psum_pic_grid_desc* grid, int precision, psum_pic_ctx** out);
 EXPORT int psum_pic_destroy(psum_pic_ctx* ctx);
-/* Run all later work of this context on `stream` (a cudaStream_t; NULL = own stream). */
+/* Run all later work of this context on `stream` (a cudaStream_t such as
+ * cudaStreamLegacy or a user stream; NULL = the context's own stream). */
 EXPORT int psum_pic_set_stream(psum_pic_ctx* ctx, void* stream);
 /* Options as whitespace `key value` pairs (the solver option grammar):
  *   sort_interval N   re-sort by cell every N steps (default 1; 0 = never) */

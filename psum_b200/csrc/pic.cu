@@ -119,12 +119,12 @@ __device__ __forceinline__ void gather_grad(const PushArgs& a, int c0, int c1, i
     }
 }
 
-// One particle: gather, push, boundary.  Returns the loss code (-1 none).
+// One particle: gather, push, boundary.  c[] holds the cell on entry and the
+// new cell on exit.  Returns the loss code (axis*2+side), -1 when the
+// particle stays, or -2 when its state became non-finite.
 template <int D, int PUSHER>
-__device__ __forceinline__ int push_one(const PushArgs& a, int& key, float f[3], float v[3]) {
+__device__ __forceinline__ int push_one(const PushArgs& a, int c[3], float f[3], float v[3]) {
     const GridView& g = a.g;
-    int c[3];
-    key_to_cell(g, key, c[0], c[1], c[2]);
     float G[3];
     gather_grad<D>(a, c[0], c[1], c[2], f[0], f[1], f[2], G);
     if (PUSHER == PSUM_PIC_LEAPFROG) {
@@ -151,14 +151,12 @@ __device__ __forceinline__ int push_one(const PushArgs& a, int& key, float f[3],
     }
     // position in cell units; offset carry rule: an offset that rounds to
     // 1.0f moves to the next cell with offset 0.
-    int lost = -1;
 #pragma unroll
     for (int d = 0; d < D; ++d) {
         const float sd = f[d] + v[d] * a.dtdr[d];
         if (!(fabsf(sd) < 1.0e9f)) {
             atomicOr(a.err, kErrNonFinite);
-            key = -1;
-            return -1;
+            return -2;
         }
         const float fl = floorf(sd);
         float nf = sd - fl;
@@ -170,6 +168,7 @@ __device__ __forceinline__ int push_one(const PushArgs& a, int& key, float f[3],
         f[d] = nf;
         c[d] += dc;
     }
+    int lost = -1;
 #pragma unroll
     for (int d = 0; d < D; ++d) {
         if (g.periodic[d]) {
@@ -182,48 +181,49 @@ __device__ __forceinline__ int push_one(const PushArgs& a, int& key, float f[3],
             else if (c[d] >= g.cells[d]) lost = 2 * d + 1;
         }
     }
-    key = lost >= 0 ? -1 : cell_to_key(g, c[0], c[1], c[2]);
     return lost;
 }
 
+// CIC corner k of a particle in cell c with offsets f: node index and
+// fixed-point weight.  Corner bits: bit 0 -> last axis (PSuM's support
+// order, simple_grid.hpp:330-343).
 template <int D>
-__device__ __forceinline__ void deposit_one(const PushArgs& a, int key, const float f[3]) {
+__device__ __forceinline__ long long corner(const PushArgs& a, int k, const int c[3], const float f[3],
+                                            long long& val) {
     const GridView& g = a.g;
-    int c[3] = {0, 0, 0};
-    if (key >= 0) key_to_cell(g, key, c[0], c[1], c[2]);
-    const int n0p = key >= 0 ? next_node(g, 0, c[0]) : 0;
-    const int n1p = key >= 0 ? next_node(g, 1, c[1]) : 0;
-    const int n2p = (D == 3 && key >= 0) ? next_node(g, 2, c[2]) : 0;
-#pragma unroll
-    for (int k = 0; k < (1 << D); ++k) {
-        // corner bits: bit 0 -> last axis (PSuM's support order, simple_grid.hpp:330-343)
-        const int b0 = (D == 2) ? (k >> 1) & 1 : (k >> 2) & 1;
-        const int b1 = (D == 2) ? k & 1 : (k >> 1) & 1;
-        const int b2 = (D == 2) ? 0 : k & 1;
-        long long node = -1, val = 0;
-        if (key >= 0) {
-            const float w0 = b0 ? f[0] : 1.f - f[0];
-            const float w1 = b1 ? f[1] : 1.f - f[1];
-            float w = w0 * w1;
-            if (D == 3) w *= b2 ? f[2] : 1.f - f[2];
-            node = node_index(g, b0 ? n0p : c[0], b1 ? n1p : c[1], D == 3 ? (b2 ? n2p : c[2]) : 0);
-            val = __float2ll_rn(w * a.scale);
-        }
-        warp_deposit(a.acc, node, val);
-    }
+    const int b0 = (D == 2) ? (k >> 1) & 1 : (k >> 2) & 1;
+    const int b1 = (D == 2) ? k & 1 : (k >> 1) & 1;
+    const int b2 = (D == 2) ? 0 : k & 1;
+    const float w0 = b0 ? f[0] : 1.f - f[0];
+    const float w1 = b1 ? f[1] : 1.f - f[1];
+    float w = w0 * w1;
+    if (D == 3) w *= b2 ? f[2] : 1.f - f[2];
+    val = __float2ll_rn(w * a.scale);
+    const int i = b0 ? next_node(g, 0, c[0]) : c[0];
+    const int j = b1 ? next_node(g, 1, c[1]) : c[1];
+    const int kk = (D == 3) ? (b2 ? next_node(g, 2, c[2]) : c[2]) : 0;
+    return node_index(g, i, j, kk);
 }
 
-// 4 particles per thread, 128-bit loads/stores of every SoA array.
+// 4 particles per thread, 128-bit loads/stores of every SoA array.  The
+// deposit first sums, per CIC corner, the lane's particles that share the
+// lane's first node (consecutive particles are usually in one cell because
+// the arrays are sorted by cell), then runs one warp segmented scan per
+// corner; the rare other nodes take a direct integer atomic.
 template <int D, int PUSHER, bool DEPOSIT_ONLY>
 __global__ void __launch_bounds__(kPicThreads) k_push_mixed(PushArgs a) {
     const long long count = *a.count;
     const int lane = threadIdx.x & 31;
     const long long stride = (long long)gridDim.x * blockDim.x * 4;
+    unsigned lost_cnt[2 * D];
+#pragma unroll
+    for (int q = 0; q < 2 * D; ++q) lost_cnt[q] = 0u;
     for (long long base = ((long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) * 4; base < count;
          base += stride) {
         const long long i0 = base + 4 * lane;
         int key[4];
         float f[4][3], v[4][3];
+        int cell[4][3];
         const bool full = i0 + 3 < count;
         if (full) {
             const int4 k4 = *reinterpret_cast<const int4*>(a.key + i0);
@@ -255,12 +255,38 @@ __global__ void __launch_bounds__(kPicThreads) k_push_mixed(PushArgs a) {
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             if (D == 2) f[j][2] = 0.f;
+            cell[j][0] = cell[j][1] = cell[j][2] = 0;
+            if (key[j] < 0) continue;
+            key_to_cell(a.g, key[j], cell[j][0], cell[j][1], cell[j][2]);
             if (!DEPOSIT_ONLY) {
-                int lost = -1;
-                if (key[j] >= 0) lost = push_one<D, PUSHER>(a, key[j], f[j], v[j]);
-                warp_count_losses(a.losses, D, lost);
+                const int lost = push_one<D, PUSHER>(a, cell[j], f[j], v[j]);
+                if (lost >= 0) {
+#pragma unroll
+                    for (int q = 0; q < 2 * D; ++q) lost_cnt[q] += (lost == q);
+                }
+                key[j] = lost == -1 ? cell_to_key(a.g, cell[j][0], cell[j][1], cell[j][2]) : -1;
             }
-            if (a.acc) deposit_one<D>(a, key[j], f[j]);
+        }
+        if (a.acc) {
+#pragma unroll
+            for (int k = 0; k < (1 << D); ++k) {
+                long long node0 = -1, sum = 0;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    if (key[j] < 0) continue;
+                    long long val;
+                    const long long node = corner<D>(a, k, cell[j], f[j], val);
+                    if (node0 < 0) {
+                        node0 = node;
+                        sum = val;
+                    } else if (node == node0) {
+                        sum += val;
+                    } else if (val != 0) {
+                        atomicAdd(a.acc + node, (unsigned long long)val);
+                    }
+                }
+                warp_deposit(a.acc, node0, sum);
+            }
         }
         if (DEPOSIT_ONLY) continue;
         if (full) {
@@ -282,6 +308,16 @@ __global__ void __launch_bounds__(kPicThreads) k_push_mixed(PushArgs a) {
 #pragma unroll
                 for (int q = 0; q < 3; ++q) a.vel[q][i] = v[j][q];
             }
+        }
+    }
+    if (!DEPOSIT_ONLY) {
+        // per-thread loss counters -> one integer atomic per warp and counter
+#pragma unroll
+        for (int q = 0; q < 2 * D; ++q) {
+            unsigned t = lost_cnt[q];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+            if (lane == 0 && t) atomicAdd(a.losses + q, (unsigned long long)t);
         }
     }
 }
@@ -985,6 +1021,8 @@ EXPORT int psum_pic_create(const psum_pic_grid_desc* gd, int precision, psum_pic
         if (nc >= 0x7fffffffLL) throw std::invalid_argument("psum_pic_create: more than 2^31-1 cells");
         g.n_nodes = nn;
         g.n_cells = nc;
+        g.div_m12 = make_fastdiv((unsigned)(g.M[1] * g.M[2]));
+        g.div_m2 = make_fastdiv((unsigned)g.M[2]);
         c->precision = precision;
         cuda_check(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
         c->stream = c->own_stream;

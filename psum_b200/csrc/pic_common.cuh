@@ -25,6 +25,31 @@ constexpr unsigned kErrNonFinite = 1u << 7;   // PSUM_ERR_NONFINITE
 constexpr unsigned kErrOverflow = 1u << 6;    // PSUM_ERR_OVERFLOW
 constexpr unsigned kErrKeyRange = 1u << 8;    // internal key out of range
 
+// Unsigned division by a run-time invariant divisor d >= 1 with one
+// multiply-high (Granlund & Montgomery, "Division by invariant integers
+// using multiplication", PLDI 1994, Fig. 4.1): for l = ceil(log2 d) and
+// m = floor(2^32 (2^l - d) / d) + 1, q = (t + ((n - t) >> 1)) >> (l - 1)
+// with t = mulhi(m, n), exact for every 32-bit n.
+struct FastDiv {
+    unsigned d, m;
+    int l;
+};
+
+inline FastDiv make_fastdiv(unsigned d) {
+    FastDiv f{d, 0u, 0};
+    int l = 0;
+    while ((1ull << l) < d) ++l;
+    f.l = l;
+    f.m = d <= 1 ? 0u : (unsigned)((((1ull << l) - d) << 32) / d + 1);
+    return f;
+}
+
+__device__ __forceinline__ unsigned fastdiv(unsigned n, const FastDiv& f) {
+    if (f.d == 1) return n;
+    const unsigned t = __umulhi(f.m, n);
+    return (t + ((n - t) >> 1)) >> (f.l - 1);
+}
+
 struct GridView {
     int dim;
     int cells[3];     // PSuM cell counts (axis >= dim: 1)
@@ -34,6 +59,8 @@ struct GridView {
     double lo[3], dx[3], dr[3];
     long long n_nodes;
     long long n_cells;   // internal cells
+    FastDiv div_m12;     // by M[1]*M[2]
+    FastDiv div_m2;      // by M[2]
 };
 
 __device__ __forceinline__ long long node_index(const GridView& g, int i, int j, int k) {
@@ -45,12 +72,11 @@ __device__ __forceinline__ int next_node(const GridView& g, int a, int c) {
     return n == g.N[a] ? 0 : n;   // only reachable on periodic axes
 }
 
-// Decompose an internal cell key into per-axis cell indices.
+// Decompose an internal cell key (>= 0) into per-axis cell indices.
 __device__ __forceinline__ void key_to_cell(const GridView& g, int key, int& c0, int& c1, int& c2) {
-    const int m12 = g.M[1] * g.M[2];
-    c0 = key / m12;
-    const int rem = key - c0 * m12;
-    c1 = rem / g.M[2];
+    c0 = (int)fastdiv((unsigned)key, g.div_m12);
+    const int rem = key - c0 * (int)g.div_m12.d;
+    c1 = (int)fastdiv((unsigned)rem, g.div_m2);
     c2 = rem - c1 * g.M[2];
 }
 

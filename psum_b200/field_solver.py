@@ -36,6 +36,26 @@ def _ptr(a):
     return a.ctypes.data
 
 
+def _ready(*tensors):
+    """Order torch's producer work before the library reads or writes these
+    tensors: the library enqueues on its own stream, torch on its current
+    stream, and CUDA orders two streams only when told to."""
+    for t in tensors:
+        if getattr(t, "is_cuda", False):
+            import torch
+            torch.cuda.current_stream(t.device).synchronize()
+            return
+
+
+def _stream_handle(stream):
+    """cudaStream_t value for a torch stream / int; torch's default stream
+    (handle 0) maps to cudaStreamLegacy (1), since NULL means 'own stream'."""
+    if stream is None:
+        return None
+    h = stream if isinstance(stream, int) else stream.cuda_stream
+    return h if h != 0 else 1
+
+
 class simple_grid:
     """Node/cell indexing of ``simple_grid<D>`` (src/field/simple_grid.hpp:16-198)."""
 
@@ -179,14 +199,16 @@ class solver_backend:
     def solve(self, b, x):
         """Synchronous solve on device buffers; returns the status (0 or
         PSUM_ERR_NOT_CONVERGED = 4 when `tol` was set and not met)."""
+        _ready(b, x)
         code = lib().psum_mg_solve(self._h(), _ptr(b), _ptr(x))
         if code not in (0, 4):
             check(code)
         return code
 
     def solve_async(self, b, x, stream=None):
-        s = None if stream is None else (stream if isinstance(stream, int) else stream.cuda_stream)
-        check(lib().psum_mg_solve_async(self._h(), _ptr(b), _ptr(x), s))
+        if stream is None:
+            _ready(b, x)
+        check(lib().psum_mg_solve_async(self._h(), _ptr(b), _ptr(x), _stream_handle(stream)))
 
     def last_stats(self):
         cyc, ref = C.c_int(), C.c_int()

@@ -12,7 +12,7 @@ import ctypes as C
 import numpy as np
 
 from ._lib import GridDesc, SpeciesDesc, check, lib
-from .field_solver import _ptr
+from .field_solver import _ptr, _ready, _stream_handle
 
 MIXED, FP64 = 0, 1
 LEAPFROG, BORIS = 0, 1
@@ -49,8 +49,15 @@ class ParticleContext:
             pass
 
     def set_stream(self, stream):
-        s = None if stream is None else (stream if isinstance(stream, int) else stream.cuda_stream)
-        check(lib().psum_pic_set_stream(self.handle, s))
+        """Run later work on `stream` (torch stream or handle); None = own stream.
+        With the caller's stream set, torch work and library work are ordered
+        by that stream and no extra synchronisation is needed."""
+        self._stream = stream
+        check(lib().psum_pic_set_stream(self.handle, _stream_handle(stream)))
+
+    def _order(self, *tensors):
+        if getattr(self, "_stream", None) is None:
+            _ready(*tensors)
 
     def set_options(self, options):
         check(lib().psum_pic_set_options(self.handle, options.encode()))
@@ -67,6 +74,7 @@ class ParticleContext:
         device tensors (torch, float64, contiguous)."""
         if hasattr(pos, "data_ptr") and getattr(pos, "is_cuda", False):
             n = pos.shape[1]
+            _ready(pos, vel)
             check(lib().psum_pic_load_device(self.handle, species, n, pos.data_ptr(), vel.data_ptr()))
         else:
             pos = np.ascontiguousarray(pos, np.float64)
@@ -87,6 +95,7 @@ class ParticleContext:
         return pos, vel
 
     def get_keys(self, species, out):
+        self._order(out)
         check(lib().psum_pic_get_keys(self.handle, species, _ptr(out)))
 
     def sort(self):
@@ -94,6 +103,7 @@ class ParticleContext:
 
     def bin(self, species, keys, counts, offsets, perm):
         n = C.c_ulonglong()
+        self._order(keys, counts, offsets, perm)
         check(lib().psum_pic_bin(self.handle, species, _ptr(keys), _ptr(counts), _ptr(offsets), _ptr(perm),
                                  C.byref(n)))
         return n.value
@@ -102,13 +112,16 @@ class ParticleContext:
         check(lib().psum_pic_deposit(self.handle))
 
     def rho(self, background, out):
+        self._order(out)
         check(lib().psum_pic_rho(self.handle, float(background), _ptr(out)))
 
     def density(self, species, out):
+        self._order(out)
         check(lib().psum_pic_density(self.handle, species, _ptr(out)))
 
     def push(self, phi, dt, pusher=LEAPFROG, B=(0.0, 0.0, 0.0)):
         Bv = (C.c_double * 3)(*B)
+        self._order(phi)
         check(lib().psum_pic_push(self.handle, _ptr(phi), float(dt), pusher, Bv))
 
     def losses(self, reset=True):
@@ -118,6 +131,7 @@ class ParticleContext:
 
     def step(self, solver, background, rho, phi, dt, pusher=LEAPFROG, B=(0.0, 0.0, 0.0)):
         Bv = (C.c_double * 3)(*B)
+        self._order(rho, phi)
         check(lib().psum_pic_step(self.handle, solver.handle, float(background), _ptr(rho), _ptr(phi), float(dt),
                                   pusher, Bv))
 
@@ -133,6 +147,7 @@ class ParticleContext:
 
     def diagnostics(self, phi, epsilon):
         out = np.zeros(len(self.species) + 2)
+        self._order(phi)
         check(lib().psum_pic_diagnostics(self.handle, _ptr(phi), float(epsilon), _ptr(out)))
         return {"kinetic": out[:len(self.species)].copy(), "field": out[-2], "charge": out[-1]}
 
