@@ -156,6 +156,27 @@ EXPORT int psum_pic_diagnostics(psum_pic_ctx* ctx, const double* phi_dev, double
  * psum_status code: non-finite state, overflow, key out of range); resets it. */
 EXPORT int psum_pic_device_errors(psum_pic_ctx* ctx, unsigned int* flags);
 
+/* Allocation-free binning of caller-owned FP64 SoA device positions
+ * (pos_dev[d*n+i]) on a grid: the same keys, per-cell counts, offsets,
+ * stable permutation and in-grid count as psum_pic_bin, without a context
+ * and without allocating device memory.  It has no counterpart in the
+ * reference.  It exists for callers that cannot call cudaMalloc, e.g. a
+ * PSuM build whose device memory belongs to another runtime's pool, or a
+ * loop held to a fixed memory budget.  Its sort and scan scratch is one
+ * file-scope device array (about 12.6 MB) that every GPU loading this
+ * library keeps until the process exits; limits: n <= 262,144 particles and
+ * at most 1,048,576 grid cells (larger sizes return
+ * PSUM_ERR_INVALID_ARGUMENT).  The first call on a device looks the array's
+ * address up (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  All calls share the one array, so calls that overlap on the GPU
+ * (other host threads, other streams) race; serialise them.  Work runs on
+ * `stream` (a cudaStream_t, NULL = legacy default stream) and the call
+ * returns after it has finished. */
+EXPORT int psum_bin_positions_noalloc(const psum_pic_grid_desc* grid, unsigned long long n, const double* pos_dev,
+                                      long long* keys_dev, unsigned long long* counts_dev,
+                                      unsigned long long* offsets_dev, unsigned long long* perm_dev,
+                                      unsigned long long* n_in_grid, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

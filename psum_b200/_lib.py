@@ -82,6 +82,7 @@ PROTOTYPES = {
     "psum_pic_get_timing": (I, [P, P, P, I]),
     "psum_pic_diagnostics": (I, [P, P, D, P]),
     "psum_pic_device_errors": (I, [P, C.POINTER(C.c_uint)]),
+    "psum_bin_positions_noalloc": (I, [C.POINTER(GridDesc), ULL, P, P, P, P, P, C.POINTER(ULL), P]),
 }
 
 STATUS = {0: "PSUM_OK", 1: "PSUM_ERR_INVALID_ARGUMENT", 2: "PSUM_ERR_NOT_READY", 3: "PSUM_ERR_CUDA",

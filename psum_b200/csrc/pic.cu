@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -1484,3 +1485,163 @@ EXPORT int psum_pic_device_errors(psum_pic_ctx* ctx, unsigned int* flags) {
 }
 
 }  // extern "C"
+
+// ===================================================== allocation-free bin ==
+//
+// psum_bin_positions_noalloc: PSuM's cell binning of caller-owned FP64
+// positions with no device allocation at all.  Some callers cannot call
+// cudaMalloc: a PSuM build whose device memory is owned by another runtime
+// (AdaptiveCpp/SYCL USM pools, a framework's caching allocator) or a loop that
+// runs under a fixed memory budget, where an extra cudaMalloc either fails or
+// fragments the pool.  Those callers pass their own inputs and outputs, and
+// the sort/scan scratch lives in the file-scope array below, which every GPU
+// that loads this library holds until the process exits.
+namespace psum_b200 {
+namespace {
+
+constexpr long long kNoAllocMaxParticles = 1LL << 18;   // 262,144 particles
+constexpr long long kNoAllocMaxCells = 1LL << 20;       // 1,048,576 cells
+constexpr long long kNoAllocTiles = kNoAllocMaxParticles / kRsTile;
+// scratch layout (bytes): sort keys A/B, sort payload A/B, per-tile radix
+// histogram and its scan, per-cell counts and offsets, scan block totals
+constexpr size_t kNaKeyBytes = sizeof(unsigned) * kNoAllocMaxParticles;
+constexpr size_t kNaHistBytes = sizeof(unsigned) * kRsBuckets * kNoAllocTiles;
+constexpr size_t kNaCellBytes = sizeof(unsigned) * kNoAllocMaxCells;
+constexpr size_t kNaTotBytes = sizeof(unsigned) * (kNoAllocMaxCells / kScanBlock + 64);
+constexpr size_t kNoAllocScratchBytes = 4 * kNaKeyBytes + 2 * kNaHistBytes + 2 * kNaCellBytes + 2 * kNaTotBytes;
+
+static __device__ __align__(256) unsigned char g_noalloc_bin_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mutex;
+void* g_noalloc_addr[64] = {nullptr};   // device address of the scratch, per device ordinal
+
+// Device address of the scratch array for the current device; looked up
+// once per device (cudaGetSymbolAddress), with that device current.
+unsigned char* noalloc_scratch() {
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev < 0 || dev >= 64) throw Error(PSUM_ERR_INTERNAL, "device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        cuda_check(cudaGetSymbolAddress(&p, g_noalloc_bin_scratch), "cudaGetSymbolAddress");
+        g_noalloc_addr[dev] = p;
+    }
+    return static_cast<unsigned char*>(g_noalloc_addr[dev]);
+}
+
+struct BinKeyArgs {
+    GridView g;
+    double hi[3];
+    const double* pos;   // SoA [d*n + i]
+    long long n;
+};
+
+// keys c2i(nC(p)) for in-grid particles, -1 otherwise (grid_mapped_device_vector.hpp:58-67)
+__global__ void k_noalloc_keys(BinKeyArgs a, long long* __restrict__ keys_out, unsigned* __restrict__ skey,
+                               int* __restrict__ sidx, unsigned sentinel) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    double p[3] = {0.0, 0.0, 0.0};
+    for (int d = 0; d < a.g.dim; ++d) p[d] = a.pos[(long long)d * a.n + i];
+    bool in = isfinite(p[0]);
+    for (int d = 0; d < a.g.dim && in; ++d) in = p[d] >= a.g.lo[d] && p[d] < a.hi[d];
+    long long ref = -1;
+    if (in) {
+        int c[3] = {0, 0, 0};
+        for (int d = 0; d < a.g.dim; ++d) c[d] = (int)((p[d] - a.g.lo[d]) * a.g.dr[d]);
+        ref = ((long long)c[0] * a.g.cells[1] + c[1]) * a.g.cells[2] + c[2];
+    }
+    keys_out[i] = ref;
+    skey[i] = ref < 0 ? sentinel : (unsigned)ref;
+    sidx[i] = (int)i;
+}
+
+}  // namespace
+}  // namespace psum_b200
+
+extern "C" EXPORT int psum_bin_positions_noalloc(const psum_pic_grid_desc* grid, unsigned long long n,
+                                                 const double* pos_dev, long long* keys_dev,
+                                                 unsigned long long* counts_dev, unsigned long long* offsets_dev,
+                                                 unsigned long long* perm_dev, unsigned long long* n_in_grid,
+                                                 void* stream) {
+    return guarded([&] {
+        if (!grid || !n_in_grid || !counts_dev || !offsets_dev) throw std::invalid_argument("bin_noalloc: null argument");
+        if (n > 0 && (!pos_dev || !keys_dev || !perm_dev)) throw std::invalid_argument("bin_noalloc: null device array");
+        if (grid->dim != 2 && grid->dim != 3) throw std::invalid_argument("bin_noalloc: dim must be 2 or 3");
+        if ((long long)n > kNoAllocMaxParticles)
+            throw std::invalid_argument("bin_noalloc: n = " + std::to_string(n) + " exceeds the fixed scratch limit of " +
+                                        std::to_string(kNoAllocMaxParticles) + " particles");
+        BinKeyArgs a{};
+        long long ncell = 1;
+        for (int d = 0; d < 3; ++d) {
+            if (d < grid->dim) {
+                if (grid->cells[d] < 1 || !(grid->lower[d] < grid->upper[d]))
+                    throw std::invalid_argument("bin_noalloc: bad grid");
+                a.g.cells[d] = grid->cells[d];
+                a.g.lo[d] = grid->lower[d];
+                a.g.dx[d] = (grid->upper[d] - grid->lower[d]) / grid->cells[d];   // simple_grid.hpp:47
+                a.g.dr[d] = 1.0 / a.g.dx[d];
+                a.hi[d] = grid->upper[d];
+            } else {
+                a.g.cells[d] = 1;
+                a.g.dx[d] = a.g.dr[d] = 1.0;
+            }
+            ncell *= a.g.cells[d];
+        }
+        a.g.dim = grid->dim;
+        if (ncell > kNoAllocMaxCells)
+            throw std::invalid_argument("bin_noalloc: " + std::to_string(ncell) + " cells exceed the fixed scratch limit of " +
+                                        std::to_string(kNoAllocMaxCells) + " cells");
+        a.pos = pos_dev;
+        a.n = (long long)n;
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        unsigned char* base = noalloc_scratch();
+        unsigned* keyA = reinterpret_cast<unsigned*>(base);
+        unsigned* keyB = reinterpret_cast<unsigned*>(base + kNaKeyBytes);
+        int* idxA = reinterpret_cast<int*>(base + 2 * kNaKeyBytes);
+        int* idxB = reinterpret_cast<int*>(base + 3 * kNaKeyBytes);
+        unsigned* hist = reinterpret_cast<unsigned*>(base + 4 * kNaKeyBytes);
+        unsigned* hist_scan = reinterpret_cast<unsigned*>(base + 4 * kNaKeyBytes + kNaHistBytes);
+        unsigned* cnt = reinterpret_cast<unsigned*>(base + 4 * kNaKeyBytes + 2 * kNaHistBytes);
+        unsigned* off = reinterpret_cast<unsigned*>(base + 4 * kNaKeyBytes + 2 * kNaHistBytes + kNaCellBytes);
+        unsigned* tot1 = reinterpret_cast<unsigned*>(base + 4 * kNaKeyBytes + 2 * kNaHistBytes + 2 * kNaCellBytes);
+        unsigned* tot2 = tot1 + kNaTotBytes / sizeof(unsigned);
+        const unsigned sentinel = (unsigned)ncell;
+        // per-cell counts must start at zero: the scratch keeps the previous call's contents
+        cuda_check(cudaMemsetAsync(cnt, 0, sizeof(unsigned) * ncell, s), "cudaMemsetAsync");
+        if (n > 0) {
+            { k_noalloc_keys<<<blocks_for((long long)n, 256), 256, 0, s>>>(a, keys_dev, keyA, idxA, sentinel); count_launch(); }
+            { k_hist_u32<<<blocks_for((long long)n, 256), 256, 0, s>>>(keys_dev, (long long)n, cnt); count_launch(); }
+        }
+        exclusive_scan_u32(cnt, off, ncell, tot1, tot2, s);
+        { k_u32_to_u64<<<blocks_for(ncell, 256), 256, 0, s>>>(cnt, counts_dev, ncell); count_launch(); }
+        { k_u32_to_u64<<<blocks_for(ncell, 256), 256, 0, s>>>(off, offsets_dev, ncell); count_launch(); }
+        unsigned long long total = 0;
+        if (n > 0) {
+            // stable LSD radix sort of (key, index) in the scratch buffers
+            unsigned* kin = keyA;
+            unsigned* kout = keyB;
+            int* vin = idxA;
+            int* vout = idxB;
+            const int nbits = std::max(1, bits_for(sentinel));
+            const int nb = (int)(((long long)n + kRsTile - 1) / kRsTile);
+            for (int shift = 0; shift < nbits; shift += kRsBits) {
+                { k_rs_hist<<<nb, kRsThreads, 0, s>>>(kin, (long long)n, shift, hist, nb); count_launch(); }
+                exclusive_scan_u32(hist, hist_scan, (long long)kRsBuckets * nb, tot1, tot2, s);
+                { k_rs_scatter<<<nb, kRsThreads, 0, s>>>(kin, vin, kout, vout, (long long)n, shift, hist_scan, nb); count_launch(); }
+                std::swap(kin, kout);
+                std::swap(vin, vout);
+            }
+            unsigned last_off = 0, last_cnt = 0;
+            cuda_check(cudaMemcpyAsync(&last_off, off + ncell - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, s), "D2H");
+            cuda_check(cudaMemcpyAsync(&last_cnt, cnt + ncell - 1, sizeof(unsigned), cudaMemcpyDeviceToHost, s), "D2H");
+            cuda_check(cudaStreamSynchronize(s), "bin_noalloc sync");
+            total = (unsigned long long)last_off + last_cnt;
+            if (total > 0) { k_i32_to_u64<<<blocks_for((long long)total, 256), 256, 0, s>>>(vin, perm_dev, (long long)total); count_launch(); }
+        }
+        cuda_check(cudaGetLastError(), "bin_noalloc launch");
+        cuda_check(cudaStreamSynchronize(s), "bin_noalloc sync");
+        *n_in_grid = total;
+    });
+}
