@@ -100,8 +100,8 @@ __device__ __forceinline__ void gather_grad(const PushArgs& a, int c0, int c1, i
         const float2 e00 = __ldg(E + node_index(g, c0, c1, 0));
         const float2 e01 = __ldg(E + node_index(g, c0, n1p, 0));
         const float2 e10 = __ldg(E + node_index(g, n0p, c1, 0));
-        G[0] = e00.x * (1.f - f1) + e01.x * f1;
-        G[1] = e00.y * (1.f - f0) + e10.y * f0;
+        G[0] = __fadd_rn(__fmul_rn(e00.x, __fsub_rn(1.f, f1)), __fmul_rn(e01.x, f1));
+        G[1] = __fadd_rn(__fmul_rn(e00.y, __fsub_rn(1.f, f0)), __fmul_rn(e10.y, f0));
         G[2] = 0.f;
     } else {
         const float4* E = reinterpret_cast<const float4*>(a.edges);
@@ -113,10 +113,12 @@ __device__ __forceinline__ void gather_grad(const PushArgs& a, int c0, int c1, i
         const float4 e100 = __ldg(E + node_index(g, n0p, c1, c2));
         const float4 e101 = __ldg(E + node_index(g, n0p, c1, n2p));
         const float4 e110 = __ldg(E + node_index(g, n0p, n1p, c2));
-        const float g1 = 1.f - f1, g2 = 1.f - f2, g0 = 1.f - f0;
-        G[0] = (e000.x * g2 + e001.x * f2) * g1 + (e010.x * g2 + e011.x * f2) * f1;
-        G[1] = (e000.y * g2 + e001.y * f2) * g0 + (e100.y * g2 + e101.y * f2) * f0;
-        G[2] = (e000.z * g1 + e010.z * f1) * g0 + (e100.z * g1 + e110.z * f1) * f0;
+        const float g1 = __fsub_rn(1.f, f1), g2 = __fsub_rn(1.f, f2), g0 = __fsub_rn(1.f, f0);
+#define PSUM_LERP(a_, wa_, b_, wb_) __fadd_rn(__fmul_rn((a_), (wa_)), __fmul_rn((b_), (wb_)))
+        G[0] = PSUM_LERP(PSUM_LERP(e000.x, g2, e001.x, f2), g1, PSUM_LERP(e010.x, g2, e011.x, f2), f1);
+        G[1] = PSUM_LERP(PSUM_LERP(e000.y, g2, e001.y, f2), g0, PSUM_LERP(e100.y, g2, e101.y, f2), f0);
+        G[2] = PSUM_LERP(PSUM_LERP(e000.z, g1, e010.z, f1), g0, PSUM_LERP(e100.z, g1, e110.z, f1), f0);
+#undef PSUM_LERP
     }
 }
 
@@ -128,39 +130,45 @@ __device__ __forceinline__ int push_one(const PushArgs& a, int c[3], float f[3],
     const GridView& g = a.g;
     float G[3];
     gather_grad<D>(a, c[0], c[1], c[2], f[0], f[1], f[2], G);
+    // Every operation is an explicit round-to-nearest intrinsic (no
+    // contraction), so the same particle is moved bit-identically by every
+    // kernel that calls this function.
     if (PUSHER == PSUM_PIC_LEAPFROG) {
 #pragma unroll
-        for (int d = 0; d < D; ++d) v[d] -= a.kE[d] * G[d];   // v += (q/m) E dt, E = -dr * G
+        for (int d = 0; d < D; ++d) v[d] = __fsub_rn(v[d], __fmul_rn(a.kE[d], G[d]));   // v += (q/m) E dt, E = -dr G
     } else {
         float E[3] = {0.f, 0.f, 0.f};
 #pragma unroll
-        for (int d = 0; d < D; ++d) E[d] = -a.dr[d] * G[d];
+        for (int d = 0; d < D; ++d) E[d] = -__fmul_rn(a.dr[d], G[d]);
         float vm[3], vp[3], vq[3], s[3];
 #pragma unroll
-        for (int q = 0; q < 3; ++q) vm[q] = v[q] + E[q] * a.qmdt_half;
-        const float t2 = a.Bt[0] * a.Bt[0] + a.Bt[1] * a.Bt[1] + a.Bt[2] * a.Bt[2];
+        for (int q = 0; q < 3; ++q) vm[q] = __fadd_rn(v[q], __fmul_rn(E[q], a.qmdt_half));
+        const float t2 = __fadd_rn(__fadd_rn(__fmul_rn(a.Bt[0], a.Bt[0]), __fmul_rn(a.Bt[1], a.Bt[1])),
+                                   __fmul_rn(a.Bt[2], a.Bt[2]));
 #pragma unroll
-        for (int q = 0; q < 3; ++q) s[q] = 2.f * a.Bt[q] / (1.f + t2);
-        vq[0] = vm[0] + (vm[1] * a.Bt[2] - vm[2] * a.Bt[1]);
-        vq[1] = vm[1] + (vm[2] * a.Bt[0] - vm[0] * a.Bt[2]);
-        vq[2] = vm[2] + (vm[0] * a.Bt[1] - vm[1] * a.Bt[0]);
-        vp[0] = vm[0] + (vq[1] * s[2] - vq[2] * s[1]);
-        vp[1] = vm[1] + (vq[2] * s[0] - vq[0] * s[2]);
-        vp[2] = vm[2] + (vq[0] * s[1] - vq[1] * s[0]);
+        for (int q = 0; q < 3; ++q) s[q] = __fdiv_rn(__fmul_rn(2.f, a.Bt[q]), __fadd_rn(1.f, t2));
+#define PSUM_CROSS(x1, y1, x2, y2) __fsub_rn(__fmul_rn((x1), (y1)), __fmul_rn((x2), (y2)))
+        vq[0] = __fadd_rn(vm[0], PSUM_CROSS(vm[1], a.Bt[2], vm[2], a.Bt[1]));
+        vq[1] = __fadd_rn(vm[1], PSUM_CROSS(vm[2], a.Bt[0], vm[0], a.Bt[2]));
+        vq[2] = __fadd_rn(vm[2], PSUM_CROSS(vm[0], a.Bt[1], vm[1], a.Bt[0]));
+        vp[0] = __fadd_rn(vm[0], PSUM_CROSS(vq[1], s[2], vq[2], s[1]));
+        vp[1] = __fadd_rn(vm[1], PSUM_CROSS(vq[2], s[0], vq[0], s[2]));
+        vp[2] = __fadd_rn(vm[2], PSUM_CROSS(vq[0], s[1], vq[1], s[0]));
+#undef PSUM_CROSS
 #pragma unroll
-        for (int q = 0; q < 3; ++q) v[q] = vp[q] + E[q] * a.qmdt_half;
+        for (int q = 0; q < 3; ++q) v[q] = __fadd_rn(vp[q], __fmul_rn(E[q], a.qmdt_half));
     }
     // position in cell units; offset carry rule: an offset that rounds to
     // 1.0f moves to the next cell with offset 0.
 #pragma unroll
     for (int d = 0; d < D; ++d) {
-        const float sd = f[d] + v[d] * a.dtdr[d];
+        const float sd = __fadd_rn(f[d], __fmul_rn(v[d], a.dtdr[d]));
         if (!(fabsf(sd) < 1.0e9f)) {
             atomicOr(a.err, kErrNonFinite);
             return -2;
         }
         const float fl = floorf(sd);
-        float nf = sd - fl;
+        float nf = __fsub_rn(sd, fl);
         int dc = (int)fl;
         if (nf >= 1.0f) {
             nf = 0.0f;
@@ -322,6 +330,354 @@ __global__ void __launch_bounds__(kPicThreads) k_push_mixed(PushArgs a) {
         }
     }
 }
+
+// ------------------------------------------------ fused sorted step ------
+//
+// With the state sorted by cell, a particle can only move to one of the 3^D
+// neighbour cells (or further, or out).  Pass 1 pushes every particle without
+// writing it, counts particles per (old cell, move class), and deposits the
+// new positions.  The new cell counts follow from the class counts of the
+// 3^D source cells; their exclusive scan gives the new cell starts.  Pass 2
+// pushes again (bit-identical: every operation of push_one is an explicit
+// rounding intrinsic) and writes each particle to
+//   new_start[new cell] + (particles of earlier classes landing in that cell)
+//                       + (rank within its own (old cell, class) group)
+// in the other state buffer.  Within a new cell, particles are ordered by
+// move class, then by old position: a deterministic order.  A block owns a
+// particle-balanced run of whole cells and gives each cell to one warp, so
+// ranks and counts need no cross-warp synchronisation.
+constexpr int kClsBlockParticles = 2048;
+constexpr int kClsWarps = kPicThreads / 32;
+constexpr int kClsTileMax = 5120;   // int64 node accumulators in shared memory (40 KB)
+
+template <int D>
+struct MoveClasses {
+    static constexpr int N = D == 2 ? 9 : 27;
+};
+
+struct ClsArgs {
+    PushArgs p;                   // current state, fields, deposit, losses, error word
+    const unsigned* starts;       // n_cells + 1 cell offsets of the current state
+    unsigned* cls;                // n_cells * classes counts (pass 1 writes, pass 2 reads)
+    const unsigned* new_starts;   // n_cells + 1 offsets of the new state (pass 2)
+    int* far;                     // pass 1: 1 when a particle moved more than one cell on an axis
+    int* key_out;
+    float* off_out[3];
+    float* vel_out[3];
+    long long n_cells;
+};
+
+__device__ __forceinline__ long long lower_bound_u32(const unsigned* __restrict__ a, long long n,
+                                                     unsigned long long v) {
+    long long lo = 0, hi = n;
+    while (lo < hi) {
+        const long long mid = (lo + hi) >> 1;
+        if ((unsigned long long)__ldg(a + mid) < v) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Cells owned by this block: those whose first particle index lies in
+// [b*T, (b+1)*T) (empty cells belong to the block of the next particle).
+__device__ __forceinline__ void cls_block_cells(const ClsArgs& a, long long& ca, long long& cb) {
+    const unsigned long long v0 = (unsigned long long)blockIdx.x * kClsBlockParticles;
+    ca = lower_bound_u32(a.starts, a.n_cells + 1, v0);
+    cb = lower_bound_u32(a.starts, a.n_cells + 1, v0 + kClsBlockParticles);
+    if (ca > a.n_cells) ca = a.n_cells;
+    if (cb > a.n_cells) cb = a.n_cells;
+}
+
+// Move class of a step from cell co to cell cn: digits (delta_a + 1) in base 3,
+// axis 0 most significant; -1 when some axis moved by more than one cell.
+template <int D>
+__device__ __forceinline__ int move_class(const GridView& g, const int co[3], const int cn[3]) {
+    int d = 0;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        int dl = cn[a] - co[a];
+        if (g.periodic[a] && g.M[a] > 2) {
+            if (dl == g.M[a] - 1) dl = -1;
+            else if (dl == 1 - g.M[a]) dl = 1;
+        }
+        if (dl < -1 || dl > 1) return -1;
+        d = d * 3 + dl + 1;
+    }
+    return d;
+}
+
+__device__ __forceinline__ int class_delta(int d, int a, int D) {
+    int p = 1;
+    for (int q = a + 1; q < D; ++q) p *= 3;
+    return (d / p) % 3 - 1;
+}
+
+// Cell reached from cell c by class d (sign +1) or the source cell of class d
+// arriving in c (sign -1); false when it leaves an absorbing axis.
+template <int D>
+__device__ __forceinline__ bool class_step(const GridView& g, const int c[3], int d, int sign, int out[3]) {
+    out[0] = c[0];
+    out[1] = c[1];
+    out[2] = c[2];
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        int x = c[a] + sign * class_delta(d, a, D);
+        if (x < 0 || x >= g.M[a]) {
+            if (!g.periodic[a]) return false;
+            x = x < 0 ? x + g.M[a] : x - g.M[a];
+        }
+        out[a] = x;
+    }
+    return true;
+}
+
+struct NodeTile {
+    int lo[3], ext[3];
+    int on;
+    long long vol;
+};
+
+// Node box touched by particles of the block's cells after one move (cells
+// +-1, nodes +2), clamped to the node lattice.  Wrap-around nodes fall
+// outside the box and take the direct global path.
+template <int D>
+__device__ void node_tile_box(const GridView& g, long long ca, long long cb, NodeTile& t) {
+    t.on = 0;
+    if (ca >= cb) return;
+    int a[3], b[3];
+    key_to_cell(g, (int)ca, a[0], a[1], a[2]);
+    key_to_cell(g, (int)(cb - 1), b[0], b[1], b[2]);
+    int lo[3], hi[3];
+    for (int q = 0; q < 3; ++q) {
+        lo[q] = 0;
+        hi[q] = g.M[q] - 1;
+    }
+    lo[0] = a[0];
+    hi[0] = b[0];
+    if (a[0] == b[0]) {
+        lo[1] = a[1];
+        hi[1] = b[1];
+        if (D == 3 && a[1] == b[1]) {
+            lo[2] = a[2];
+            hi[2] = b[2];
+        }
+    }
+    t.vol = 1;
+    for (int q = 0; q < 3; ++q) {
+        if (q < D) {
+            t.lo[q] = max(lo[q] - 1, 0);
+            const int top = min(hi[q] + 2, g.N[q] - 1);
+            t.ext[q] = top - t.lo[q] + 1;
+        } else {
+            t.lo[q] = 0;
+            t.ext[q] = 1;
+        }
+        t.vol *= t.ext[q];
+    }
+    t.on = t.vol <= kClsTileMax;
+}
+
+template <int D, int PUSHER>
+__global__ void __launch_bounds__(kPicThreads) k_cls_pass1(ClsArgs a) {
+    constexpr int NC = MoveClasses<D>::N;
+    __shared__ unsigned cnt_w[kClsWarps][NC];
+    __shared__ unsigned long long tile[kClsTileMax];
+    __shared__ NodeTile box;
+    const GridView& g = a.p.g;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu;
+    long long ca, cb;
+    cls_block_cells(a, ca, cb);
+    if (threadIdx.x == 0) node_tile_box<D>(g, ca, cb, box);
+    __syncthreads();
+    if (box.on)
+        for (long long q = threadIdx.x; q < box.vol; q += blockDim.x) tile[q] = 0ull;
+    __syncthreads();
+    unsigned lost_cnt[2 * D];
+#pragma unroll
+    for (int q = 0; q < 2 * D; ++q) lost_cnt[q] = 0u;
+    for (long long c = ca + warp; c < cb; c += kClsWarps) {
+        if (lane < NC) cnt_w[warp][lane] = 0u;
+        __syncwarp();
+        const long long p0 = a.starts[c], p1 = a.starts[c + 1];
+        int co[3];
+        key_to_cell(g, (int)c, co[0], co[1], co[2]);
+        for (long long base = p0; base < p1; base += 32) {
+            const long long i = base + lane;
+            int cls = -2;       // -2 no particle, -3 absorbed or non-finite, -1 far, >= 0 move class
+            int newkey = -1;
+            int cn[3] = {co[0], co[1], co[2]};
+            float f[3] = {0.f, 0.f, 0.f}, v[3] = {0.f, 0.f, 0.f};
+            if (i < p1) {
+#pragma unroll
+                for (int d = 0; d < D; ++d) f[d] = a.p.off[d][i];
+#pragma unroll
+                for (int q = 0; q < 3; ++q) v[q] = a.p.vel[q][i];
+                const int lost = push_one<D, PUSHER>(a.p, cn, f, v);
+                if (lost == -1) {
+                    cls = move_class<D>(g, co, cn);
+                    newkey = cell_to_key(g, cn[0], cn[1], cn[2]);
+                    if (cls < 0) atomicOr(a.far, 1);
+                } else {
+                    cls = -3;
+                    if (lost >= 0) {
+#pragma unroll
+                        for (int q = 0; q < 2 * D; ++q) lost_cnt[q] += (lost == q);
+                    }
+                }
+            }
+            const unsigned cpeers = __match_any_sync(full, cls);
+            if (cls >= 0 && lane == __ffs(cpeers) - 1) cnt_w[warp][cls] += __popc(cpeers);
+            // deposit: lanes sharing the new cell share the CIC nodes; exact
+            // group sums of the int64 weights via three 22-bit-chunk reductions
+            const unsigned gpeers = __match_any_sync(full, newkey);
+            const bool leader = newkey >= 0 && lane == __ffs(gpeers) - 1;
+#pragma unroll
+            for (int k = 0; k < (1 << D); ++k) {
+                long long val = 0;
+                long long node = -1;
+                if (newkey >= 0) node = corner<D>(a.p, k, cn, f, val);
+                const unsigned long long u = (unsigned long long)val;
+                const unsigned lo = __reduce_add_sync(gpeers, (unsigned)(u & 0x3fffffull));
+                const unsigned mid = __reduce_add_sync(gpeers, (unsigned)((u >> 22) & 0x3fffffull));
+                const unsigned hi = __reduce_add_sync(gpeers, (unsigned)(u >> 44));
+                if (leader) {
+                    const unsigned long long sum =
+                        (unsigned long long)lo + ((unsigned long long)mid << 22) + ((unsigned long long)hi << 44);
+                    if (sum == 0ull) continue;
+                    const int b0 = (D == 2) ? (k >> 1) & 1 : (k >> 2) & 1;
+                    const int b1 = (D == 2) ? k & 1 : (k >> 1) & 1;
+                    const int b2 = (D == 2) ? 0 : k & 1;
+                    const int ni = b0 ? next_node(g, 0, cn[0]) : cn[0];
+                    const int nj = b1 ? next_node(g, 1, cn[1]) : cn[1];
+                    const int nk = (D == 3) ? (b2 ? next_node(g, 2, cn[2]) : cn[2]) : 0;
+                    const int ti = ni - box.lo[0], tj = nj - box.lo[1], tk = nk - box.lo[2];
+                    if (box.on && ti >= 0 && ti < box.ext[0] && tj >= 0 && tj < box.ext[1] && tk >= 0 &&
+                        tk < box.ext[2])
+                        atomicAdd(&tile[((long long)ti * box.ext[1] + tj) * box.ext[2] + tk], sum);
+                    else
+                        atomicAdd(a.p.acc + node, sum);
+                }
+            }
+        }
+        __syncwarp();
+        if (lane < NC) a.cls[c * NC + lane] = cnt_w[warp][lane];
+        __syncwarp();
+    }
+#pragma unroll
+    for (int q = 0; q < 2 * D; ++q) {
+        unsigned t = lost_cnt[q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(full, t, o);
+        if (lane == 0 && t) atomicAdd(a.p.losses + q, (unsigned long long)t);
+    }
+    __syncthreads();
+    if (box.on) {
+        for (long long q = threadIdx.x; q < box.vol; q += blockDim.x) {
+            const unsigned long long val = tile[q];
+            if (val == 0ull) continue;
+            const int tk = (int)(q % box.ext[2]);
+            const int tj = (int)((q / box.ext[2]) % box.ext[1]);
+            const int ti = (int)(q / ((long long)box.ext[1] * box.ext[2]));
+            atomicAdd(a.p.acc + node_index(g, ti + box.lo[0], tj + box.lo[1], tk + box.lo[2]), val);
+        }
+    }
+}
+
+// new cell counts from the class counts of the 3^D source cells
+template <int D>
+__global__ void k_cls_newcount(GridView g, const unsigned* __restrict__ cls, unsigned* __restrict__ newcount,
+                               long long n_cells) {
+    constexpr int NC = MoveClasses<D>::N;
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c > n_cells) return;
+    if (c == n_cells) {
+        newcount[c] = 0u;
+        return;
+    }
+    int cc[3];
+    key_to_cell(g, (int)c, cc[0], cc[1], cc[2]);
+    unsigned total = 0;
+    for (int d = 0; d < NC; ++d) {
+        int src[3];
+        if (!class_step<D>(g, cc, d, -1, src)) continue;
+        total += __ldg(cls + (long long)cell_to_key(g, src[0], src[1], src[2]) * NC + d);
+    }
+    newcount[c] = total;
+}
+
+template <int D, int PUSHER>
+__global__ void __launch_bounds__(kPicThreads) k_cls_pass2(ClsArgs a) {
+    constexpr int NC = MoveClasses<D>::N;
+    __shared__ unsigned base_w[kClsWarps][NC];
+    __shared__ unsigned run_w[kClsWarps][NC];
+    if (*a.far) return;   // some particle moved too far: the caller takes the general path
+    const GridView& g = a.p.g;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu;
+    long long ca, cb;
+    cls_block_cells(a, ca, cb);
+    for (long long c = ca + warp; c < cb; c += kClsWarps) {
+        int co[3];
+        key_to_cell(g, (int)c, co[0], co[1], co[2]);
+        if (lane < NC) {
+            run_w[warp][lane] = 0u;
+            if (__ldg(a.cls + c * NC + lane) != 0u) {
+                // group base: start of the new cell + earlier classes landing there
+                int cn[3], src[3];
+                class_step<D>(g, co, lane, +1, cn);
+                const long long kn = cell_to_key(g, cn[0], cn[1], cn[2]);
+                unsigned b = __ldg(a.new_starts + kn);
+                for (int d2 = 0; d2 < lane; ++d2)
+                    if (class_step<D>(g, cn, d2, -1, src))
+                        b += __ldg(a.cls + (long long)cell_to_key(g, src[0], src[1], src[2]) * NC + d2);
+                base_w[warp][lane] = b;
+            }
+        }
+        __syncwarp();
+        const long long p0 = a.starts[c], p1 = a.starts[c + 1];
+        for (long long base = p0; base < p1; base += 32) {
+            const long long i = base + lane;
+            int cls = -2;
+            int cn[3] = {co[0], co[1], co[2]};
+            float f[3] = {0.f, 0.f, 0.f}, v[3] = {0.f, 0.f, 0.f};
+            if (i < p1) {
+#pragma unroll
+                for (int d = 0; d < D; ++d) f[d] = a.p.off[d][i];
+#pragma unroll
+                for (int q = 0; q < 3; ++q) v[q] = a.p.vel[q][i];
+                const int lost = push_one<D, PUSHER>(a.p, cn, f, v);
+                cls = lost == -1 ? move_class<D>(g, co, cn) : -3;
+            }
+            const unsigned peers = __match_any_sync(full, cls);
+            if (cls >= 0) {
+                const unsigned dest =
+                    base_w[warp][cls] + run_w[warp][cls] + (unsigned)__popc(peers & ((1u << lane) - 1u));
+                a.key_out[dest] = cell_to_key(g, cn[0], cn[1], cn[2]);
+#pragma unroll
+                for (int d = 0; d < D; ++d) a.off_out[d][dest] = f[d];
+#pragma unroll
+                for (int q = 0; q < 3; ++q) a.vel_out[q][dest] = v[q];
+            }
+            __syncwarp();
+            if (cls >= 0 && lane == __ffs(peers) - 1) run_w[warp][cls] += __popc(peers);
+            __syncwarp();
+        }
+    }
+}
+
+// cell offsets of a sorted key array: starts[c] = first index with key >= c
+__global__ void k_cell_starts(const int* __restrict__ key, const long long* __restrict__ count, long long n_upper,
+                              unsigned* __restrict__ starts, long long n_cells) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long cnt = *count;
+    if (i > cnt || i > n_upper) return;
+    const long long ki = i < cnt ? key[i] : n_cells;
+    const long long kp = i == 0 ? -1 : key[i - 1];
+    for (long long c = kp + 1; c <= ki; ++c) starts[c] = (unsigned)i;
+}
+
+__global__ void k_count_from(long long* __restrict__ count, const unsigned* __restrict__ src) { *count = *src; }
 
 // ------------------------------------------------------- load / export --
 __global__ void k_load_mixed(GridView g, long long n, const double* __restrict__ pos, const double* __restrict__ vel,
@@ -832,6 +1188,12 @@ static void sort_species(psum_pic_ctx* c, Species& sp, int sidx) {
     }
     { k_count_valid<<<gb, 256, 0, s>>>(skeys, n, sentinel, c->count.p + sidx); count_launch(); }
     sp.cur = nxt;
+    if (c->precision == PSUM_PIC_MIXED) {
+        // cell offsets of the sorted state, for the fused sorted step
+        { k_cell_starts<<<blocks_for(n + 1, 256), 256, 0, s>>>(sp.key[nxt].p, c->count.p + sidx, n,
+                                                              sp.starts[sp.starts_cur].p, c->g.n_cells); count_launch(); }
+        sp.sorted = true;
+    }
     cuda_check(cudaGetLastError(), "sort launch");
 }
 
@@ -848,6 +1210,8 @@ static void alloc_species_state(psum_pic_ctx* c, Species& sp) {
     }
     sp.acc.alloc(c->g.n_nodes);
     cuda_check(cudaMemsetAsync(sp.acc.p, 0, sizeof(unsigned long long) * c->g.n_nodes, c->stream), "memset acc");
+    if (c->precision == PSUM_PIC_MIXED)
+        for (int b = 0; b < 2; ++b) sp.starts[b].alloc((size_t)c->g.n_cells + 1);
 }
 
 static PushArgs make_push_args(psum_pic_ctx* c, Species& sp, int sidx, double dt, int pusher, const double* B) {
@@ -931,6 +1295,7 @@ static void push_all(psum_pic_ctx* c, const double* phi, double dt, int pusher, 
     for (int si = 0; si < (int)c->sp.size(); ++si) {
         Species& sp = *c->sp[si];
         if (sp.n <= 0) continue;
+        sp.sorted = false;   // moved in place
         if (c->precision == PSUM_PIC_MIXED) {
             PushArgs a = make_push_args(c, sp, si, dt, pusher, B);
             launch_mixed(a, c->g.dim, pusher, false, sp.n, s);
@@ -961,6 +1326,91 @@ static void push_all(psum_pic_ctx* c, const double* phi, double dt, int pusher, 
 
 static void sort_all(psum_pic_ctx* c) {
     for (int s = 0; s < (int)c->sp.size(); ++s) sort_species(c, *c->sp[s], s);
+}
+
+// One fused sorted step (push + deposit + re-sort) of every species; see
+// k_cls_pass1 / k_cls_pass2.  Species in which some particle moved more
+// than one cell along an axis take the general path (in-place push, radix
+// sort) for this step; their deposit from pass 1 stands.
+static void launch_pass(psum_pic_ctx* c, const ClsArgs& a, int dim, int pusher, int pass, long long n) {
+    const unsigned blocks = (unsigned)(n / kClsBlockParticles + 1);
+    cudaStream_t s = c->stream;
+#define PSUM_PASS(D_, P_) \
+    do { \
+        if (pass == 1) { k_cls_pass1<D_, P_><<<blocks, kPicThreads, 0, s>>>(a); count_launch(); } \
+        else { k_cls_pass2<D_, P_><<<blocks, kPicThreads, 0, s>>>(a); count_launch(); } \
+    } while (0)
+    if (dim == 2) {
+        if (pusher == PSUM_PIC_BORIS) PSUM_PASS(2, PSUM_PIC_BORIS);
+        else PSUM_PASS(2, PSUM_PIC_LEAPFROG);
+    } else {
+        if (pusher == PSUM_PIC_BORIS) PSUM_PASS(3, PSUM_PIC_BORIS);
+        else PSUM_PASS(3, PSUM_PIC_LEAPFROG);
+    }
+#undef PSUM_PASS
+}
+
+static void ensure_cls_buffers(psum_pic_ctx* c) {
+    const long long nc = c->g.n_cells;
+    const int ncls = c->g.dim == 2 ? 9 : 27;
+    c->cls_count.alloc((size_t)nc * ncls);
+    c->newcount.alloc((size_t)nc + 1);
+    c->scan_tmp1.alloc((size_t)(nc + 1 + kScanBlock - 1) / kScanBlock + 1);
+    c->scan_tmp2.alloc(16);
+    c->far_flag.alloc(8);
+}
+
+static void cls_step(psum_pic_ctx* c, const double* phi, double dt, int pusher, const double* B) {
+    cudaStream_t s = c->stream;
+    ensure_cls_buffers(c);
+    zero_accumulators(c);
+    if (c->g.dim == 2) { k_edges<2><<<blocks_for(c->g.n_nodes, 256), 256, 0, s>>>(c->g, phi, c->edges.p); count_launch(); }
+    else { k_edges<3><<<blocks_for(c->g.n_nodes, 256), 256, 0, s>>>(c->g, phi, c->edges.p); count_launch(); }
+    cuda_check(cudaMemsetAsync(c->far_flag.p, 0, sizeof(int) * 8, s), "memset");
+    const int ns = (int)c->sp.size();
+    for (int si = 0; si < ns; ++si) {
+        Species& sp = *c->sp[si];
+        if (sp.n <= 0) continue;
+        ClsArgs a{};
+        a.p = make_push_args(c, sp, si, dt, pusher, B);
+        a.starts = sp.starts[sp.starts_cur].p;
+        a.cls = c->cls_count.p;
+        a.new_starts = sp.starts[1 - sp.starts_cur].p;
+        a.far = c->far_flag.p + si;
+        const int nxt = 1 - sp.cur;
+        a.key_out = sp.key[nxt].p;
+        for (int d = 0; d < 3; ++d) {
+            a.off_out[d] = d < c->g.dim ? sp.off[d][nxt].p : nullptr;
+            a.vel_out[d] = sp.vel[d][nxt].p;
+        }
+        a.n_cells = c->g.n_cells;
+        launch_pass(c, a, c->g.dim, pusher, 1, sp.n);
+        const long long nc = c->g.n_cells;
+        if (c->g.dim == 2) { k_cls_newcount<2><<<blocks_for(nc + 1, 256), 256, 0, s>>>(c->g, c->cls_count.p, c->newcount.p, nc); count_launch(); }
+        else { k_cls_newcount<3><<<blocks_for(nc + 1, 256), 256, 0, s>>>(c->g, c->cls_count.p, c->newcount.p, nc); count_launch(); }
+        exclusive_scan_u32(c->newcount.p, sp.starts[1 - sp.starts_cur].p, nc + 1, c->scan_tmp1.p, c->scan_tmp2.p, s);
+        launch_pass(c, a, c->g.dim, pusher, 2, sp.n);
+    }
+    int far[8] = {0};
+    cuda_check(cudaMemcpyAsync(far, c->far_flag.p, sizeof(int) * 8, cudaMemcpyDeviceToHost, s), "D2H");
+    cuda_check(cudaStreamSynchronize(s), "far flag sync");
+    for (int si = 0; si < ns; ++si) {
+        Species& sp = *c->sp[si];
+        if (sp.n <= 0) continue;
+        if (!far[si]) {
+            { k_count_from<<<1, 1, 0, s>>>(c->count.p + si, sp.starts[1 - sp.starts_cur].p + c->g.n_cells); count_launch(); }
+            sp.cur = 1 - sp.cur;
+            sp.starts_cur = 1 - sp.starts_cur;
+            continue;
+        }
+        // general path: move in place (no second deposit), then radix sort
+        PushArgs pa = make_push_args(c, sp, si, dt, pusher, B);
+        pa.acc = nullptr;
+        pa.losses = c->losses.p + 6 * 8;   // discard slot: pass 1 already counted this step's losses
+        launch_mixed(pa, c->g.dim, pusher, false, sp.n, s);
+        sort_species(c, sp, si);
+    }
+    cuda_check(cudaGetLastError(), "fused step launch");
 }
 
 static void rho_into(psum_pic_ctx* c, double background, double* rho, int only_species, bool with_charge) {
@@ -1028,7 +1478,7 @@ EXPORT int psum_pic_create(const psum_pic_grid_desc* gd, int precision, psum_pic
         cuda_check(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
         c->stream = c->own_stream;
         if (precision == PSUM_PIC_MIXED) c->edges.alloc((size_t)nn * (g.dim == 2 ? 2 : 4));
-        c->losses.alloc(8 * 6);
+        c->losses.alloc(9 * 6);   // 8 species + one discard slot
         c->err.alloc(1);
         c->count.alloc(8);
         c->partials.alloc(kDiagBlocks);
@@ -1122,6 +1572,7 @@ static void load_common(psum_pic_ctx* ctx, int species, unsigned long long n, co
     }
     { k_set_count<<<1, 1, 0, s>>>(ctx->count.p + species, (long long)n); count_launch(); }
     sp.n = (long long)n;
+    sp.sorted = false;
     if (ctx->precision == PSUM_PIC_FP64 && n > 0) {
         double* p3[3] = {sp.pos64[0][0].p, ctx->g.dim > 1 ? sp.pos64[1][0].p : nullptr,
                          ctx->g.dim > 2 ? sp.pos64[2][0].p : nullptr};
@@ -1379,16 +1830,27 @@ EXPORT int psum_pic_step(psum_pic_ctx* ctx, psum_field_solver_handle solver, dou
             solver_solve_async(sv, rho_dev, phi_dev, ctx->stream);
             t.stop();
         }
-        {
+        bool fused = ctx->precision == PSUM_PIC_MIXED && ctx->sort_interval == 1;
+        for (auto& sp : ctx->sp) fused = fused && (sp->sorted || sp->n == 0);
+        if (pusher != PSUM_PIC_LEAPFROG && pusher != PSUM_PIC_BORIS) throw std::invalid_argument("step: unknown pusher");
+        if (fused) {
+            // push, deposit and re-sort in the two passes of the fused step
             PhaseTimer t(ctx, 2);
-            push_all(ctx, phi_dev, dt, pusher, B);
+            cls_step(ctx, phi_dev, dt, pusher, B);
             t.stop();
-        }
-        ctx->steps++;
-        if (ctx->sort_interval > 0 && ctx->steps % ctx->sort_interval == 0) {
-            PhaseTimer t(ctx, 3);
-            sort_all(ctx);
-            t.stop();
+            ctx->steps++;
+        } else {
+            {
+                PhaseTimer t(ctx, 2);
+                push_all(ctx, phi_dev, dt, pusher, B);
+                t.stop();
+            }
+            ctx->steps++;
+            if (ctx->sort_interval > 0 && ctx->steps % ctx->sort_interval == 0) {
+                PhaseTimer t(ctx, 3);
+                sort_all(ctx);
+                t.stop();
+            }
         }
     });
 }

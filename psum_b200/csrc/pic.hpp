@@ -27,6 +27,10 @@ struct Species {
     DevBuf<double> pos64[3][2];
     DevBuf<double> vel64[3][2];
     DevBuf<unsigned long long> acc;   // deposit accumulator, one int64 per node
+    // cell offsets of the sorted state (n_cells + 1 entries, double buffered)
+    DevBuf<unsigned> starts[2];
+    int starts_cur = 0;
+    bool sorted = false;              // state sorted by cell and starts valid
 };
 
 struct SortScratch {
@@ -52,6 +56,10 @@ struct psum_pic_ctx {
     psum_b200::DevBuf<double> partials;
     psum_b200::DevBuf<long long> ipartials;
     psum_b200::SortScratch sort;
+    psum_b200::DevBuf<unsigned> cls_count;    // per (cell, move class) counts of the fused sorted step
+    psum_b200::DevBuf<unsigned> newcount;     // per new cell counts (n_cells + 1)
+    psum_b200::DevBuf<unsigned> scan_tmp1, scan_tmp2;
+    psum_b200::DevBuf<int> far_flag;          // per species: a particle moved more than one cell on an axis
     int sort_interval = 1;
     long long steps = 0;
     bool timing = false;
