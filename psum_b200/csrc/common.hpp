@@ -22,7 +22,12 @@ void set_last_error(const std::string& msg);
 const std::string& last_error();
 
 // Process-wide count of kernels launched by this library (psum_kernel_launches).
+// Kernels enqueued while a stream is being captured into a CUDA graph are
+// taken back out (uncount_launches) and counted per graph launch instead.
 void count_launch();
+void add_launches(unsigned long long n);
+void uncount_launches(unsigned long long n);
+unsigned long long thread_launches();   // launches counted by the calling thread
 
 inline void cuda_check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw Error(PSUM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));

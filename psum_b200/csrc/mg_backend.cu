@@ -125,9 +125,22 @@ struct SolverBase {
     int max_coarse = 8192;
     std::array<int, 3> periodic{0, 0, 0};   // wrap-around transfers per axis (option periodic_I/J/K)
     double tol = 0.0;
+    int use_graph = 1;                      // option `graph 0|1`: replay the solve as one CUDA graph
     unsigned long long n_row = 0;
     bool ready = false;
     cudaStream_t own_stream = nullptr;
+    // The solve's launch sequence depends only on the options, the operator,
+    // the sources and the (b, x) pointers: it is captured once into a CUDA
+    // graph and replayed while none of them changes (`version` counts the
+    // changes of the first three).
+    unsigned long long version = 0;
+    struct {
+        cudaGraphExec_t exec = nullptr;
+        const double* b = nullptr;
+        const double* x = nullptr;
+        unsigned long long version = 0;
+        unsigned long long kernels = 0;
+    } graph;
     // sources (host copies kept, device copies uploaded at set time)
     std::vector<unsigned long long> rep_idx, add_idx;
     std::vector<double> rep_val, add_val;
@@ -143,7 +156,12 @@ struct SolverBase {
     unsigned long long coarse_rows = 0;
 
     virtual ~SolverBase() {
+        drop_graph();
         if (own_stream) cudaStreamDestroy(own_stream);
+    }
+    void drop_graph() {
+        if (graph.exec) cudaGraphExecDestroy(graph.exec);
+        graph.exec = nullptr;
     }
     virtual void build_device(cudaStream_t s) = 0;
     virtual void enqueue_solve(double* b, double* x, cudaStream_t s) = 0;
@@ -345,6 +363,7 @@ void solver_set_options(SolverBase* s, const char* options) {
         else if (key == "periodic_I") s->periodic[0] = parse_int(iss, key) != 0;
         else if (key == "periodic_J") s->periodic[1] = parse_int(iss, key) != 0;
         else if (key == "periodic_K") s->periodic[2] = parse_int(iss, key) != 0;
+        else if (key == "graph") s->use_graph = parse_int(iss, key) != 0;
         else if (key == "correction_interval") {
             int v = 0;
             if (!(iss >> v) || v < 1) throw std::invalid_argument("correction_interval must be positive");
@@ -361,6 +380,7 @@ void solver_set_options(SolverBase* s, const char* options) {
     if (!k_provided) s->K = 1;
     if (s->pre_relax < 0 || s->post_relax < 0 || s->max_cycles < 0 || s->depth < 1)
         throw std::invalid_argument("set_options: negative relax/cycle counts or depth < 1");
+    s->version++;
 }
 
 void solver_set_matrix(SolverBase* s, unsigned long long n_row, unsigned long long n_col, unsigned long long nnz,
@@ -370,6 +390,8 @@ void solver_set_matrix(SolverBase* s, unsigned long long n_row, unsigned long lo
     s->host = build_hierarchy(A, s->I, s->J, s->K, s->depth, s->max_coarse, s->periodic);
     s->n_row = n_row;
     ensure_stream(s);
+    s->version++;
+    s->drop_graph();
     s->build_device(s->own_stream);
     s->ready = true;
 }
@@ -381,6 +403,42 @@ static void upload_sources(SolverBase* s) {
     s->d_add_idx.upload(s->add_idx.data(), s->add_idx.size(), s->own_stream);
     s->d_add_val.upload(s->add_val.data(), s->add_val.size(), s->own_stream);
     cuda_check(cudaStreamSynchronize(s->own_stream), "upload sources");
+    s->version++;
+}
+
+// Graph capture needs a stream that is not the legacy/per-thread default
+// stream and is not already being captured by the caller (then the caller's
+// capture records the launches directly).
+static bool capturable(cudaStream_t st) {
+    if (st == nullptr || st == cudaStreamLegacy || st == cudaStreamPerThread) return false;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cuda_check(cudaStreamIsCapturing(st, &cs), "cudaStreamIsCapturing");
+    return cs == cudaStreamCaptureStatusNone;
+}
+
+static void capture_solve(SolverBase* s, double* b, double* x, cudaStream_t st) {
+    s->drop_graph();
+    const unsigned long long k0 = thread_launches();
+    cuda_check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    cudaGraph_t g = nullptr;
+    try {
+        s->enqueue_solve(b, x, st);
+    } catch (...) {
+        cudaStreamEndCapture(st, &g);
+        if (g) cudaGraphDestroy(g);
+        uncount_launches(thread_launches() - k0);
+        throw;
+    }
+    cuda_check(cudaStreamEndCapture(st, &g), "cudaStreamEndCapture");
+    const unsigned long long kernels = thread_launches() - k0;
+    uncount_launches(kernels);   // counted again at every replay
+    const cudaError_t e = cudaGraphInstantiate(&s->graph.exec, g, 0);
+    cudaGraphDestroy(g);
+    cuda_check(e, "cudaGraphInstantiate");
+    s->graph.b = b;
+    s->graph.x = x;
+    s->graph.version = s->version;
+    s->graph.kernels = kernels;
 }
 
 void solver_set_source(SolverBase* s, bool replace, unsigned long long n, const unsigned long long* idx,
@@ -406,7 +464,15 @@ void solver_solve_async(SolverBase* s, double* b, double* x, cudaStream_t stream
         if (i >= s->n_row) throw std::invalid_argument("set_source_replace: index out of range");
     for (auto i : s->add_idx)
         if (i >= s->n_row) throw std::invalid_argument("set_source_addback: index out of range");
-    s->enqueue_solve(b, x, stream ? stream : s->own_stream);
+    cudaStream_t st = stream ? stream : s->own_stream;
+    if (s->use_graph && capturable(st)) {
+        if (!(s->graph.exec && s->graph.b == b && s->graph.x == x && s->graph.version == s->version))
+            capture_solve(s, b, x, st);
+        cuda_check(cudaGraphLaunch(s->graph.exec, st), "cudaGraphLaunch");
+        add_launches(s->graph.kernels);
+        return;
+    }
+    s->enqueue_solve(b, x, st);
 }
 
 MGState solver_read_state(SolverBase* s, cudaStream_t stream) {

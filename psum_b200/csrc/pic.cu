@@ -85,14 +85,21 @@ struct PushArgs {
     float Bt[3];        // B * q/m * dt / 2 (Boris t vector)
     float dr[3];
     unsigned long long* acc;
-    float scale;        // 2^dep_shift
+    int dep_lsh;        // accumulator units per 2^-26 weight unit: 2^dep_lsh
     unsigned long long* losses;
     unsigned* err;
 };
 
+// Field data of one cell for the CIC gather of the edge differences: the
+// components that interpolate G_a over the cell (G_a lives on the edges along
+// axis a, so it varies with the other axes' offsets only).
 template <int D>
-__device__ __forceinline__ void gather_grad(const PushArgs& a, int c0, int c1, int c2, float f0, float f1, float f2,
-                                            float G[3]) {
+struct CellField {
+    float e[D == 2 ? 4 : 12];
+};
+
+template <int D>
+__device__ __forceinline__ void load_cell_field(const PushArgs& a, int c0, int c1, int c2, CellField<D>& F) {
     const GridView& g = a.g;
     if (D == 2) {
         const float2* E = reinterpret_cast<const float2*>(a.edges);
@@ -100,9 +107,10 @@ __device__ __forceinline__ void gather_grad(const PushArgs& a, int c0, int c1, i
         const float2 e00 = __ldg(E + node_index(g, c0, c1, 0));
         const float2 e01 = __ldg(E + node_index(g, c0, n1p, 0));
         const float2 e10 = __ldg(E + node_index(g, n0p, c1, 0));
-        G[0] = __fadd_rn(__fmul_rn(e00.x, __fsub_rn(1.f, f1)), __fmul_rn(e01.x, f1));
-        G[1] = __fadd_rn(__fmul_rn(e00.y, __fsub_rn(1.f, f0)), __fmul_rn(e10.y, f0));
-        G[2] = 0.f;
+        F.e[0] = e00.x;
+        F.e[1] = e01.x;
+        F.e[2] = e00.y;
+        F.e[3] = e10.y;
     } else {
         const float4* E = reinterpret_cast<const float4*>(a.edges);
         const int n0p = next_node(g, 0, c0), n1p = next_node(g, 1, c1), n2p = next_node(g, 2, c2);
@@ -113,26 +121,37 @@ __device__ __forceinline__ void gather_grad(const PushArgs& a, int c0, int c1, i
         const float4 e100 = __ldg(E + node_index(g, n0p, c1, c2));
         const float4 e101 = __ldg(E + node_index(g, n0p, c1, n2p));
         const float4 e110 = __ldg(E + node_index(g, n0p, n1p, c2));
-        const float g1 = __fsub_rn(1.f, f1), g2 = __fsub_rn(1.f, f2), g0 = __fsub_rn(1.f, f0);
-#define PSUM_LERP(a_, wa_, b_, wb_) __fadd_rn(__fmul_rn((a_), (wa_)), __fmul_rn((b_), (wb_)))
-        G[0] = PSUM_LERP(PSUM_LERP(e000.x, g2, e001.x, f2), g1, PSUM_LERP(e010.x, g2, e011.x, f2), f1);
-        G[1] = PSUM_LERP(PSUM_LERP(e000.y, g2, e001.y, f2), g0, PSUM_LERP(e100.y, g2, e101.y, f2), f0);
-        G[2] = PSUM_LERP(PSUM_LERP(e000.z, g1, e010.z, f1), g0, PSUM_LERP(e100.z, g1, e110.z, f1), f0);
-#undef PSUM_LERP
+        F.e[0] = e000.x; F.e[1] = e001.x; F.e[2] = e010.x; F.e[3] = e011.x;
+        F.e[4] = e000.y; F.e[5] = e001.y; F.e[6] = e100.y; F.e[7] = e101.y;
+        F.e[8] = e000.z; F.e[9] = e010.z; F.e[10] = e100.z; F.e[11] = e110.z;
     }
 }
 
-// One particle: gather, push, boundary.  c[] holds the cell on entry and the
-// new cell on exit.  Returns the loss code (axis*2+side), -1 when the
-// particle stays, or -2 when its state became non-finite.
+template <int D>
+__device__ __forceinline__ void interp_grad(const CellField<D>& F, const float f[3], float G[3]) {
+#define PSUM_LERP(a_, wa_, b_, wb_) __fadd_rn(__fmul_rn((a_), (wa_)), __fmul_rn((b_), (wb_)))
+    if (D == 2) {
+        G[0] = PSUM_LERP(F.e[0], __fsub_rn(1.f, f[1]), F.e[1], f[1]);
+        G[1] = PSUM_LERP(F.e[2], __fsub_rn(1.f, f[0]), F.e[3], f[0]);
+        G[2] = 0.f;
+    } else {
+        const float g0 = __fsub_rn(1.f, f[0]), g1 = __fsub_rn(1.f, f[1]), g2 = __fsub_rn(1.f, f[2]);
+        G[0] = PSUM_LERP(PSUM_LERP(F.e[0], g2, F.e[1], f[2]), g1, PSUM_LERP(F.e[2], g2, F.e[3], f[2]), f[1]);
+        G[1] = PSUM_LERP(PSUM_LERP(F.e[4], g2, F.e[5], f[2]), g0, PSUM_LERP(F.e[6], g2, F.e[7], f[2]), f[0]);
+        G[2] = PSUM_LERP(PSUM_LERP(F.e[8], g1, F.e[9], f[1]), g0, PSUM_LERP(F.e[10], g1, F.e[11], f[1]), f[0]);
+    }
+#undef PSUM_LERP
+}
+
+// Velocity update from the gathered edge differences G, then the move in
+// cell units.  f holds the new in-cell offsets and dc the cell steps per axis
+// on exit (offset carry rule: an offset that rounds to 1.0f moves to the next
+// cell with offset 0).  Every operation is an explicit round-to-nearest
+// intrinsic (no contraction), so every kernel that calls this function moves
+// the same particle bit-identically.  False when the state became
+// non-finite (the error word is flagged).
 template <int D, int PUSHER>
-__device__ __forceinline__ int push_one(const PushArgs& a, int c[3], float f[3], float v[3]) {
-    const GridView& g = a.g;
-    float G[3];
-    gather_grad<D>(a, c[0], c[1], c[2], f[0], f[1], f[2], G);
-    // Every operation is an explicit round-to-nearest intrinsic (no
-    // contraction), so the same particle is moved bit-identically by every
-    // kernel that calls this function.
+__device__ __forceinline__ bool kick_move(const PushArgs& a, const float G[3], float f[3], float v[3], int dc[3]) {
     if (PUSHER == PSUM_PIC_LEAPFROG) {
 #pragma unroll
         for (int d = 0; d < D; ++d) v[d] = __fsub_rn(v[d], __fmul_rn(a.kE[d], G[d]));   // v += (q/m) E dt, E = -dr G
@@ -158,28 +177,34 @@ __device__ __forceinline__ int push_one(const PushArgs& a, int c[3], float f[3],
 #pragma unroll
         for (int q = 0; q < 3; ++q) v[q] = __fadd_rn(vp[q], __fmul_rn(E[q], a.qmdt_half));
     }
-    // position in cell units; offset carry rule: an offset that rounds to
-    // 1.0f moves to the next cell with offset 0.
 #pragma unroll
     for (int d = 0; d < D; ++d) {
         const float sd = __fadd_rn(f[d], __fmul_rn(v[d], a.dtdr[d]));
         if (!(fabsf(sd) < 1.0e9f)) {
             atomicOr(a.err, kErrNonFinite);
-            return -2;
+            return false;
         }
         const float fl = floorf(sd);
         float nf = __fsub_rn(sd, fl);
-        int dc = (int)fl;
+        int step = (int)fl;
         if (nf >= 1.0f) {
             nf = 0.0f;
-            dc += 1;
+            step += 1;
         }
         f[d] = nf;
-        c[d] += dc;
+        dc[d] = step;
     }
+    return true;
+}
+
+// Wrap periodic axes and test absorbing ones after c += dc.  Returns the loss
+// code (axis*2+side) of the first absorbing axis left, or -1.
+template <int D>
+__device__ __forceinline__ int apply_step(const GridView& g, int c[3], const int dc[3]) {
     int lost = -1;
 #pragma unroll
     for (int d = 0; d < D; ++d) {
+        c[d] += dc[d];
         if (g.periodic[d]) {
             if (c[d] < 0 || c[d] >= g.M[d]) {
                 c[d] %= g.M[d];
@@ -193,25 +218,67 @@ __device__ __forceinline__ int push_one(const PushArgs& a, int c[3], float f[3],
     return lost;
 }
 
-// CIC corner k of a particle in cell c with offsets f: node index and
-// fixed-point weight.  Corner bits: bit 0 -> last axis (PSuM's support
-// order, simple_grid.hpp:330-343).
+// One particle: gather, push, boundary.  c[] holds the cell on entry and the
+// new cell on exit.  Returns the loss code (axis*2+side), -1 when the
+// particle stays, or -2 when its state became non-finite.
+template <int D, int PUSHER>
+__device__ __forceinline__ int push_one(const PushArgs& a, int c[3], float f[3], float v[3]) {
+    CellField<D> F;
+    load_cell_field<D>(a, c[0], c[1], c[2], F);
+    float G[3];
+    interp_grad<D>(F, f, G);
+    int dc[3] = {0, 0, 0};
+    if (!kick_move<D, PUSHER>(a, G, f, v, dc)) return -2;
+    return apply_step<D>(a.g, c, dc);
+}
+
+// ------------------------------------------------ quantised CIC weights --
+// Every mixed-precision deposit uses integer CIC weights on a 2^-26 grid,
+// built from quantised moments of the in-cell offsets, indexed by axis set m
+// (bit a = axis a):
+//   Q_0 = 2^26,  Q_m = rint(2^26 * prod_{a in m} f_a)  (FP32 products, left to right).
+// The corner whose upper axes form the set B gets the inclusion-exclusion sum
+//   w_B = sum_{T superset of B} (-1)^{|T|-|B|} Q_T,
+// the exact expansion of prod_{a in B} f_a * prod_{a not in B} (1 - f_a) with
+// every product replaced by its quantised moment.  A particle's weights sum
+// to exactly 2^26 and each lies within 2^(D-2) * 2^-26 of the CIC weight of
+// its FP32 offsets.  The map from moments to weights is linear, so a group of
+// particles sums its moments (exact integers) and forms the corner sums
+// once: the deposit is exact and independent of grouping and order.
+constexpr int kCicBits = 26;
+constexpr float kCicScale = 67108864.0f;   // 2^26
+
 template <int D>
-__device__ __forceinline__ long long corner(const PushArgs& a, int k, const int c[3], const float f[3],
-                                            long long& val) {
-    const GridView& g = a.g;
-    const int b0 = (D == 2) ? (k >> 1) & 1 : (k >> 2) & 1;
-    const int b1 = (D == 2) ? k & 1 : (k >> 1) & 1;
-    const int b2 = (D == 2) ? 0 : k & 1;
-    const float w0 = b0 ? f[0] : 1.f - f[0];
-    const float w1 = b1 ? f[1] : 1.f - f[1];
-    float w = w0 * w1;
-    if (D == 3) w *= b2 ? f[2] : 1.f - f[2];
-    val = __float2ll_rn(w * a.scale);
-    const int i = b0 ? next_node(g, 0, c[0]) : c[0];
-    const int j = b1 ? next_node(g, 1, c[1]) : c[1];
-    const int kk = (D == 3) ? (b2 ? next_node(g, 2, c[2]) : c[2]) : 0;
-    return node_index(g, i, j, kk);
+__device__ __forceinline__ void cic_moments(const float f[3], unsigned q[8]) {
+    q[0] = 1u << kCicBits;
+    q[1] = __float2uint_rn(__fmul_rn(f[0], kCicScale));
+    q[2] = __float2uint_rn(__fmul_rn(f[1], kCicScale));
+    const float f01 = __fmul_rn(f[0], f[1]);
+    q[3] = __float2uint_rn(__fmul_rn(f01, kCicScale));
+    if (D == 3) {
+        q[4] = __float2uint_rn(__fmul_rn(f[2], kCicScale));
+        q[5] = __float2uint_rn(__fmul_rn(__fmul_rn(f[0], f[2]), kCicScale));
+        q[6] = __float2uint_rn(__fmul_rn(__fmul_rn(f[1], f[2]), kCicScale));
+        q[7] = __float2uint_rn(__fmul_rn(__fmul_rn(f01, f[2]), kCicScale));
+    }
+}
+
+// Corner weight of upper-axis set B from (group sums of) the moments S[m].
+template <int D>
+__device__ __forceinline__ long long cic_corner(const long long S[8], int B) {
+    long long w = 0;
+#pragma unroll
+    for (int T = 0; T < (1 << D); ++T)
+        if ((T & B) == B) w += (__popc(T ^ B) & 1) ? -S[T] : S[T];
+    return w;
+}
+
+// Node of corner B of cell c (wrapping on periodic axes).
+template <int D>
+__device__ __forceinline__ void corner_node(const GridView& g, int B, const int c[3], int n[3]) {
+    n[0] = (B & 1) ? next_node(g, 0, c[0]) : c[0];
+    n[1] = (B & 2) ? next_node(g, 1, c[1]) : c[1];
+    n[2] = (D == 3) ? ((B & 4) ? next_node(g, 2, c[2]) : c[2]) : 0;
 }
 
 // 4 particles per thread, 128-bit loads/stores of every SoA array.  The
@@ -277,14 +344,22 @@ __global__ void __launch_bounds__(kPicThreads) k_push_mixed(PushArgs a) {
             }
         }
         if (a.acc) {
+            unsigned q[4][8];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) cic_moments<D>(f[j], q[j]);
 #pragma unroll
             for (int k = 0; k < (1 << D); ++k) {
                 long long node0 = -1, sum = 0;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     if (key[j] < 0) continue;
-                    long long val;
-                    const long long node = corner<D>(a, k, cell[j], f[j], val);
+                    long long S[8];
+#pragma unroll
+                    for (int m = 0; m < (1 << D); ++m) S[m] = q[j][m];
+                    const long long val = (long long)((unsigned long long)cic_corner<D>(S, k) << a.dep_lsh);
+                    int nd[3];
+                    corner_node<D>(a.g, k, cell[j], nd);
+                    const long long node = node_index(a.g, nd[0], nd[1], nd[2]);
                     if (node0 < 0) {
                         node0 = node;
                         sum = val;
@@ -335,93 +410,68 @@ __global__ void __launch_bounds__(kPicThreads) k_push_mixed(PushArgs a) {
 //
 // With the state sorted by cell, a particle can only move to one of the 3^D
 // neighbour cells (or further, or out).  Pass 1 pushes every particle without
-// writing it, counts particles per (old cell, move class), and deposits the
-// new positions.  The new cell counts follow from the class counts of the
-// 3^D source cells; their exclusive scan gives the new cell starts.  Pass 2
-// pushes again (bit-identical: every operation of push_one is an explicit
-// rounding intrinsic) and writes each particle to
-//   new_start[new cell] + (particles of earlier classes landing in that cell)
-//                       + (rank within its own (old cell, class) group)
-// in the other state buffer.  Within a new cell, particles are ordered by
-// move class, then by old position: a deterministic order.  A block owns a
-// particle-balanced run of whole cells and gives each cell to one warp, so
-// ranks and counts need no cross-warp synchronisation.
-constexpr int kClsBlockParticles = 2048;
+// writing it, counts particles per (old cell, move class) and deposits the
+// new positions.  The offsets kernel turns the class counts into, per new
+// cell, its particle count and the offset of every (source cell, class)
+// group inside it; groups are ordered by source cell index, which is the
+// order of the old positions.  After the exclusive scan of the new counts,
+// pass 2 pushes again (bit-identical: every operation is an explicit rounding
+// intrinsic) and writes particle i of a group to
+//   new_start[new cell] + group offset + (rank of i within its group)
+// in the other state buffer.  The result is exactly the stable sort by new
+// cell of the pushed state, with absorbed particles removed: what the general
+// path (push in place, stable radix sort) produces.
+//
+// A block owns the cells whose first particle index lies in
+// [b*T, (b+1)*T) (table from k_cls_blocks) and gives each cell to one warp,
+// so ranks and counts need no cross-warp synchronisation.  The pass-1
+// deposit sums the quantised CIC moments of the particles of one (cell,
+// class) group with warp reductions, forms the 2^D corner sums once per group
+// and cell, and adds them to a block node tile in shared memory that is
+// flushed with one integer atomic per touched node.
 constexpr int kClsWarps = kPicThreads / 32;
-constexpr int kClsTileMax = 5120;   // int64 node accumulators in shared memory (40 KB)
+constexpr int kClsTileMax = 3072;   // int64 node accumulators in shared memory (24 KB)
+constexpr int kClsRounds = 4;       // rounds of 32 particles per warp iteration (all loads issued first)
+
+// Particles per block: 2D blocks cover a few tens of cells of one row; 3D
+// blocks stay short enough that their node box usually fits the tile.
+__host__ __device__ constexpr int cls_block_particles(int dim) { return dim == 2 ? 8192 : 2048; }
 
 template <int D>
 struct MoveClasses {
     static constexpr int N = D == 2 ? 9 : 27;
+    static constexpr int STAY = (N - 1) / 2;   // class of the particles that keep their cell
 };
 
 struct ClsArgs {
     PushArgs p;                   // current state, fields, deposit, losses, error word
     const unsigned* starts;       // n_cells + 1 cell offsets of the current state
-    unsigned* cls;                // n_cells * classes counts (pass 1 writes, pass 2 reads)
+    const unsigned* block_first;  // first cell of each block (k_cls_blocks)
+    unsigned* cls;                // n_cells * classes: counts (pass 1), then group offsets (pass 2)
     const unsigned* new_starts;   // n_cells + 1 offsets of the new state (pass 2)
     int* far;                     // pass 1: 1 when a particle moved more than one cell on an axis
-    int* key_out;
-    float* off_out[3];
+    float* off_out[3];            // new state (its keys follow from new_starts)
     float* vel_out[3];
     long long n_cells;
 };
 
-__device__ __forceinline__ long long lower_bound_u32(const unsigned* __restrict__ a, long long n,
-                                                     unsigned long long v) {
-    long long lo = 0, hi = n;
-    while (lo < hi) {
-        const long long mid = (lo + hi) >> 1;
-        if ((unsigned long long)__ldg(a + mid) < v) lo = mid + 1;
-        else hi = mid;
-    }
-    return lo;
-}
-
-// Cells owned by this block: those whose first particle index lies in
-// [b*T, (b+1)*T) (empty cells belong to the block of the next particle).
-__device__ __forceinline__ void cls_block_cells(const ClsArgs& a, long long& ca, long long& cb) {
-    const unsigned long long v0 = (unsigned long long)blockIdx.x * kClsBlockParticles;
-    ca = lower_bound_u32(a.starts, a.n_cells + 1, v0);
-    cb = lower_bound_u32(a.starts, a.n_cells + 1, v0 + kClsBlockParticles);
-    if (ca > a.n_cells) ca = a.n_cells;
-    if (cb > a.n_cells) cb = a.n_cells;
-}
-
-// Move class of a step from cell co to cell cn: digits (delta_a + 1) in base 3,
-// axis 0 most significant; -1 when some axis moved by more than one cell.
+// Per-axis step of move class d: digits (step_a + 1) in base 3, axis 0 most
+// significant.
 template <int D>
-__device__ __forceinline__ int move_class(const GridView& g, const int co[3], const int cn[3]) {
-    int d = 0;
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-        int dl = cn[a] - co[a];
-        if (g.periodic[a] && g.M[a] > 2) {
-            if (dl == g.M[a] - 1) dl = -1;
-            else if (dl == 1 - g.M[a]) dl = 1;
-        }
-        if (dl < -1 || dl > 1) return -1;
-        d = d * 3 + dl + 1;
-    }
-    return d;
+__device__ __forceinline__ int class_delta(int d, int a) {
+    if (D == 2) return a == 0 ? d / 3 - 1 : d % 3 - 1;
+    return a == 0 ? d / 9 - 1 : (a == 1 ? (d / 3) % 3 - 1 : d % 3 - 1);
 }
 
-__device__ __forceinline__ int class_delta(int d, int a, int D) {
-    int p = 1;
-    for (int q = a + 1; q < D; ++q) p *= 3;
-    return (d / p) % 3 - 1;
-}
-
-// Cell reached from cell c by class d (sign +1) or the source cell of class d
-// arriving in c (sign -1); false when it leaves an absorbing axis.
+// Cell reached from cell c by class d; false when it leaves an absorbing axis.
 template <int D>
-__device__ __forceinline__ bool class_step(const GridView& g, const int c[3], int d, int sign, int out[3]) {
+__device__ __forceinline__ bool class_target(const GridView& g, const int c[3], int d, int out[3]) {
     out[0] = c[0];
     out[1] = c[1];
     out[2] = c[2];
 #pragma unroll
     for (int a = 0; a < D; ++a) {
-        int x = c[a] + sign * class_delta(d, a, D);
+        int x = c[a] + class_delta<D>(d, a);
         if (x < 0 || x >= g.M[a]) {
             if (!g.periodic[a]) return false;
             x = x < 0 ? x + g.M[a] : x - g.M[a];
@@ -431,10 +481,23 @@ __device__ __forceinline__ bool class_step(const GridView& g, const int c[3], in
     return true;
 }
 
+// Block -> first owned cell: first[b] = lower bound of b*T in starts,
+// clamped to n_cells; entries 0..nb.
+__global__ void k_cls_blocks(const unsigned* __restrict__ starts, long long n_cells, long long nb, long long T,
+                             unsigned* __restrict__ first) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t <= n_cells) {
+        const long long hi = (long long)starts[t] / T;
+        for (long long b = t == 0 ? 0 : (long long)starts[t - 1] / T + 1; b <= hi && b <= nb; ++b)
+            first[b] = (unsigned)t;
+    }
+    if (t <= nb && t * T > (long long)starts[n_cells]) first[t] = (unsigned)n_cells;
+}
+
 struct NodeTile {
     int lo[3], ext[3];
     int on;
-    long long vol;
+    int vol;
 };
 
 // Node box touched by particles of the block's cells after one move (cells
@@ -462,7 +525,7 @@ __device__ void node_tile_box(const GridView& g, long long ca, long long cb, Nod
             hi[2] = b[2];
         }
     }
-    t.vol = 1;
+    long long vol = 1;
     for (int q = 0; q < 3; ++q) {
         if (q < D) {
             t.lo[q] = max(lo[q] - 1, 0);
@@ -472,96 +535,205 @@ __device__ void node_tile_box(const GridView& g, long long ca, long long cb, Nod
             t.lo[q] = 0;
             t.ext[q] = 1;
         }
-        t.vol *= t.ext[q];
+        vol *= t.ext[q];
     }
-    t.on = t.vol <= kClsTileMax;
+    t.on = vol <= kClsTileMax;
+    t.vol = t.on ? (int)vol : 0;
+}
+
+// Push of one particle of cell co with the warp's cell field: move class
+// (>= 0), -1 far (more than one cell on some axis), -3 absorbed or
+// non-finite (loss counted).  cn is the new cell for far particles.
+template <int D, int PUSHER>
+__device__ __forceinline__ int push_classify(const PushArgs& a, const CellField<D>& F, const int co[3], float f[3],
+                                             float v[3], int cn[3], unsigned lost_cnt[2 * D]) {
+    float G[3];
+    interp_grad<D>(F, f, G);
+    int dc[3] = {0, 0, 0};
+    if (!kick_move<D, PUSHER>(a, G, f, v, dc)) return -3;
+    cn[0] = co[0];
+    cn[1] = co[1];
+    cn[2] = co[2];
+    const int lost = apply_step<D>(a.g, cn, dc);
+    if (lost >= 0) {
+#pragma unroll
+        for (int q = 0; q < 2 * D; ++q) lost_cnt[q] += (lost == q);
+        return -3;
+    }
+    int cls = 0;
+    bool far = false;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        far |= dc[d] < -1 || dc[d] > 1;
+        cls = cls * 3 + dc[d] + 1;
+    }
+    return far ? -1 : cls;
+}
+
+// Exact warp sum of per-lane values below 2^32 (two reductions of 26-bit
+// and 6-bit parts).
+__device__ __forceinline__ unsigned long long warp_sum_u32(unsigned v) {
+    const unsigned lo = __reduce_add_sync(0xffffffffu, v & ((1u << kCicBits) - 1u));
+    const unsigned hi = __reduce_add_sync(0xffffffffu, v >> kCicBits);
+    return (unsigned long long)lo + ((unsigned long long)hi << kCicBits);
+}
+
+// 64-bit shared-memory accumulators kept as 32-bit low/high words: native
+// 32-bit atomics, the carry out of the low word goes to the high word, so the
+// pair holds the exact sum modulo 2^64 once all adds are done.
+__device__ __forceinline__ void smem_add64(unsigned* lo, unsigned* hi, unsigned long long v) {
+    const unsigned vl = (unsigned)v, vh = (unsigned)(v >> 32);
+    const unsigned old = atomicAdd(lo, vl);
+    const unsigned up = vh + (old + vl < old ? 1u : 0u);
+    if (up) atomicAdd(hi, up);
+}
+
+__device__ __forceinline__ unsigned long long pair64(unsigned lo, unsigned hi) {
+    return (unsigned long long)lo | ((unsigned long long)hi << 32);
 }
 
 template <int D, int PUSHER>
 __global__ void __launch_bounds__(kPicThreads) k_cls_pass1(ClsArgs a) {
     constexpr int NC = MoveClasses<D>::N;
-    __shared__ unsigned cnt_w[kClsWarps][NC];
-    __shared__ unsigned long long tile[kClsTileMax];
+    constexpr int STAY = MoveClasses<D>::STAY;
+    constexpr int NM = 1 << D;
+    // per (warp, moment, class): count (moment 0, low word only) and moment
+    // sums of the current cell; block node tile in units of 2^-26
+    __shared__ unsigned mom_lo[kClsWarps][NM][NC], mom_hi[kClsWarps][NM][NC];
+    __shared__ unsigned tile_lo[kClsTileMax], tile_hi[kClsTileMax];
     __shared__ NodeTile box;
+    const long long ca = a.block_first[blockIdx.x], cb = a.block_first[blockIdx.x + 1];
+    if (ca >= cb) return;
     const GridView& g = a.p.g;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned full = 0xffffffffu;
-    long long ca, cb;
-    cls_block_cells(a, ca, cb);
     if (threadIdx.x == 0) node_tile_box<D>(g, ca, cb, box);
+    for (int q = threadIdx.x; q < kClsWarps * NM * NC; q += blockDim.x) {
+        (&mom_lo[0][0][0])[q] = 0u;
+        (&mom_hi[0][0][0])[q] = 0u;
+    }
     __syncthreads();
-    if (box.on)
-        for (long long q = threadIdx.x; q < box.vol; q += blockDim.x) tile[q] = 0ull;
+    for (int q = threadIdx.x; q < box.vol; q += blockDim.x) {
+        tile_lo[q] = 0u;
+        tile_hi[q] = 0u;
+    }
     __syncthreads();
     unsigned lost_cnt[2 * D];
 #pragma unroll
     for (int q = 0; q < 2 * D; ++q) lost_cnt[q] = 0u;
     for (long long c = ca + warp; c < cb; c += kClsWarps) {
-        if (lane < NC) cnt_w[warp][lane] = 0u;
-        __syncwarp();
         const long long p0 = a.starts[c], p1 = a.starts[c + 1];
         int co[3];
         key_to_cell(g, (int)c, co[0], co[1], co[2]);
-        for (long long base = p0; base < p1; base += 32) {
-            const long long i = base + lane;
-            int cls = -2;       // -2 no particle, -3 absorbed or non-finite, -1 far, >= 0 move class
-            int newkey = -1;
-            int cn[3] = {co[0], co[1], co[2]};
-            float f[3] = {0.f, 0.f, 0.f}, v[3] = {0.f, 0.f, 0.f};
-            if (i < p1) {
+        if (p1 > p0) {
+            CellField<D> F;
+            load_cell_field<D>(a.p, co[0], co[1], co[2], F);
+            // particles that keep their cell: per-lane count and moment sums
+            // (at most 2^31 over 32 rounds), reduced over the warp every 32 rounds
+            unsigned sacc[NM];
 #pragma unroll
-                for (int d = 0; d < D; ++d) f[d] = a.p.off[d][i];
+            for (int m = 0; m < NM; ++m) sacc[m] = 0u;
+            int pending = 0;
+            for (long long base = p0; base < p1; base += 32 * kClsRounds) {
+                // all rounds' loads in flight before the first push
+                float f[kClsRounds][3], v[kClsRounds][3];
+                bool live[kClsRounds];
 #pragma unroll
-                for (int q = 0; q < 3; ++q) v[q] = a.p.vel[q][i];
-                const int lost = push_one<D, PUSHER>(a.p, cn, f, v);
-                if (lost == -1) {
-                    cls = move_class<D>(g, co, cn);
-                    newkey = cell_to_key(g, cn[0], cn[1], cn[2]);
-                    if (cls < 0) atomicOr(a.far, 1);
-                } else {
-                    cls = -3;
-                    if (lost >= 0) {
+                for (int r = 0; r < kClsRounds; ++r) {
+                    const long long i = base + 32 * r + lane;
+                    live[r] = i < p1;
+                    f[r][0] = f[r][1] = f[r][2] = 0.f;
+                    v[r][0] = v[r][1] = v[r][2] = 0.f;
+                    if (live[r]) {
 #pragma unroll
-                        for (int q = 0; q < 2 * D; ++q) lost_cnt[q] += (lost == q);
+                        for (int d = 0; d < D; ++d) f[r][d] = a.p.off[d][i];
+#pragma unroll
+                        for (int q = 0; q < 3; ++q) v[r][q] = a.p.vel[q][i];
                     }
                 }
-            }
-            const unsigned cpeers = __match_any_sync(full, cls);
-            if (cls >= 0 && lane == __ffs(cpeers) - 1) cnt_w[warp][cls] += __popc(cpeers);
-            // deposit: lanes sharing the new cell share the CIC nodes; exact
-            // group sums of the int64 weights via three 22-bit-chunk reductions
-            const unsigned gpeers = __match_any_sync(full, newkey);
-            const bool leader = newkey >= 0 && lane == __ffs(gpeers) - 1;
 #pragma unroll
-            for (int k = 0; k < (1 << D); ++k) {
-                long long val = 0;
-                long long node = -1;
-                if (newkey >= 0) node = corner<D>(a.p, k, cn, f, val);
-                const unsigned long long u = (unsigned long long)val;
-                const unsigned lo = __reduce_add_sync(gpeers, (unsigned)(u & 0x3fffffull));
-                const unsigned mid = __reduce_add_sync(gpeers, (unsigned)((u >> 22) & 0x3fffffull));
-                const unsigned hi = __reduce_add_sync(gpeers, (unsigned)(u >> 44));
-                if (leader) {
-                    const unsigned long long sum =
-                        (unsigned long long)lo + ((unsigned long long)mid << 22) + ((unsigned long long)hi << 44);
-                    if (sum == 0ull) continue;
-                    const int b0 = (D == 2) ? (k >> 1) & 1 : (k >> 2) & 1;
-                    const int b1 = (D == 2) ? k & 1 : (k >> 1) & 1;
-                    const int b2 = (D == 2) ? 0 : k & 1;
-                    const int ni = b0 ? next_node(g, 0, cn[0]) : cn[0];
-                    const int nj = b1 ? next_node(g, 1, cn[1]) : cn[1];
-                    const int nk = (D == 3) ? (b2 ? next_node(g, 2, cn[2]) : cn[2]) : 0;
-                    const int ti = ni - box.lo[0], tj = nj - box.lo[1], tk = nk - box.lo[2];
-                    if (box.on && ti >= 0 && ti < box.ext[0] && tj >= 0 && tj < box.ext[1] && tk >= 0 &&
-                        tk < box.ext[2])
-                        atomicAdd(&tile[((long long)ti * box.ext[1] + tj) * box.ext[2] + tk], sum);
-                    else
-                        atomicAdd(a.p.acc + node, sum);
+                for (int r = 0; r < kClsRounds; ++r) {
+                    int cn[3];
+                    const int cls = live[r] ? push_classify<D, PUSHER>(a.p, F, co, f[r], v[r], cn, lost_cnt) : -2;
+                    unsigned q[8];
+                    cic_moments<D>(f[r], q);
+                    if (cls == STAY) {
+                        sacc[0] += 1u;
+#pragma unroll
+                        for (int m = 1; m < NM; ++m) sacc[m] += q[m];
+                    } else if (cls >= 0) {
+                        // mover: a few per round, distinct classes mostly
+                        atomicAdd(&mom_lo[warp][0][cls], 1u);
+#pragma unroll
+                        for (int m = 1; m < NM; ++m) smem_add64(&mom_lo[warp][m][cls], &mom_hi[warp][m][cls], q[m]);
+                    } else if (cls == -1) {
+                        // far mover: own corners, direct atomics; the caller redoes the move
+                        atomicOr(a.far, 1);
+                        long long W[8];
+#pragma unroll
+                        for (int m = 0; m < NM; ++m) W[m] = q[m];
+#pragma unroll
+                        for (int B = 0; B < NM; ++B) {
+                            const long long w = cic_corner<D>(W, B);
+                            if (w == 0) continue;
+                            int nd[3];
+                            corner_node<D>(g, B, cn, nd);
+                            atomicAdd(a.p.acc + node_index(g, nd[0], nd[1], nd[2]),
+                                      (unsigned long long)w << a.p.dep_lsh);
+                        }
+                    }
+                }
+                if (++pending == 32 / kClsRounds || base + 32 * kClsRounds >= p1) {
+                    pending = 0;
+#pragma unroll
+                    for (int m = 0; m < NM; ++m) {
+                        const unsigned long long t = warp_sum_u32(sacc[m]);
+                        sacc[m] = 0u;
+                        if (lane == 0) {
+                            const unsigned long long v64 = pair64(mom_lo[warp][m][STAY], mom_hi[warp][m][STAY]) + t;
+                            mom_lo[warp][m][STAY] = (unsigned)v64;
+                            mom_hi[warp][m][STAY] = (unsigned)(v64 >> 32);
+                        }
+                    }
                 }
             }
         }
         __syncwarp();
-        if (lane < NC) a.cls[c * NC + lane] = cnt_w[warp][lane];
+        // class lanes: count out, corner sums of the class into the node tile
+        // (for a fixed corner the classes reach distinct nodes: no conflicts)
+        if (lane < NC) {
+            const unsigned n = mom_lo[warp][0][lane];
+            a.cls[c * NC + lane] = n;
+            if (n) {
+                long long W[8];
+                W[0] = (long long)n << kCicBits;
+                mom_lo[warp][0][lane] = 0u;
+                mom_hi[warp][0][lane] = 0u;
+#pragma unroll
+                for (int m = 1; m < NM; ++m) {
+                    W[m] = (long long)pair64(mom_lo[warp][m][lane], mom_hi[warp][m][lane]);
+                    mom_lo[warp][m][lane] = 0u;
+                    mom_hi[warp][m][lane] = 0u;
+                }
+                int cn[3];
+                class_target<D>(g, co, lane, cn);   // inside: the class holds no absorbed particle
+#pragma unroll
+                for (int B = 0; B < NM; ++B) {
+                    const long long w = cic_corner<D>(W, B);
+                    if (w == 0) continue;
+                    int nd[3];
+                    corner_node<D>(g, B, cn, nd);
+                    const int ti = nd[0] - box.lo[0], tj = nd[1] - box.lo[1], tk = nd[2] - box.lo[2];
+                    if (box.on && (unsigned)ti < (unsigned)box.ext[0] && (unsigned)tj < (unsigned)box.ext[1] &&
+                        (unsigned)tk < (unsigned)box.ext[2]) {
+                        const int t = (ti * box.ext[1] + tj) * box.ext[2] + tk;
+                        smem_add64(&tile_lo[t], &tile_hi[t], (unsigned long long)w);
+                    } else {
+                        atomicAdd(a.p.acc + node_index(g, nd[0], nd[1], nd[2]), (unsigned long long)w << a.p.dep_lsh);
+                    }
+                }
+            }
+        }
         __syncwarp();
     }
 #pragma unroll
@@ -572,22 +744,25 @@ __global__ void __launch_bounds__(kPicThreads) k_cls_pass1(ClsArgs a) {
         if (lane == 0 && t) atomicAdd(a.p.losses + q, (unsigned long long)t);
     }
     __syncthreads();
-    if (box.on) {
-        for (long long q = threadIdx.x; q < box.vol; q += blockDim.x) {
-            const unsigned long long val = tile[q];
-            if (val == 0ull) continue;
-            const int tk = (int)(q % box.ext[2]);
-            const int tj = (int)((q / box.ext[2]) % box.ext[1]);
-            const int ti = (int)(q / ((long long)box.ext[1] * box.ext[2]));
-            atomicAdd(a.p.acc + node_index(g, ti + box.lo[0], tj + box.lo[1], tk + box.lo[2]), val);
-        }
+    const int e2 = box.ext[2], e12 = box.ext[1] * box.ext[2];
+    for (int q = threadIdx.x; q < box.vol; q += blockDim.x) {
+        const unsigned long long val = pair64(tile_lo[q], tile_hi[q]);
+        if (val == 0ull) continue;
+        const int ti = q / e12, r = q - ti * e12;
+        const int tj = r / e2, tk = r - tj * e2;
+        atomicAdd(a.p.acc + node_index(g, ti + box.lo[0], tj + box.lo[1], tk + box.lo[2]), val << a.p.dep_lsh);
     }
 }
 
-// new cell counts from the class counts of the 3^D source cells
+// Per new cell: its particle count, and the offset inside it of every
+// (source cell, class) group landing there, written over that group's count.
+// Groups are visited by increasing source cell index (per axis: the source
+// below, the cell itself, the source above, rotated at periodic seams), so
+// the new cell keeps the particles in their old order.  Periodic axes need
+// at least 3 cells for the sources to be distinct.
 template <int D>
-__global__ void k_cls_newcount(GridView g, const unsigned* __restrict__ cls, unsigned* __restrict__ newcount,
-                               long long n_cells) {
+__global__ void k_cls_offsets(GridView g, unsigned* __restrict__ cls, unsigned* __restrict__ newcount,
+                              long long n_cells) {
     constexpr int NC = MoveClasses<D>::N;
     const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c > n_cells) return;
@@ -597,11 +772,45 @@ __global__ void k_cls_newcount(GridView g, const unsigned* __restrict__ cls, uns
     }
     int cc[3];
     key_to_cell(g, (int)c, cc[0], cc[1], cc[2]);
+    // steps of the arriving moves in order of increasing source coordinate
+    int ord[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const bool seam_lo = g.periodic[a] && cc[a] == 0;
+        const bool seam_hi = g.periodic[a] && cc[a] == g.M[a] - 1;
+        ord[a][0] = seam_lo ? 0 : (seam_hi ? -1 : 1);
+        ord[a][1] = seam_lo ? -1 : (seam_hi ? 1 : 0);
+        ord[a][2] = seam_lo ? 1 : (seam_hi ? 0 : -1);
+    }
     unsigned total = 0;
-    for (int d = 0; d < NC; ++d) {
-        int src[3];
-        if (!class_step<D>(g, cc, d, -1, src)) continue;
-        total += __ldg(cls + (long long)cell_to_key(g, src[0], src[1], src[2]) * NC + d);
+    constexpr int n1 = D == 3 ? 3 : 1;
+#pragma unroll
+    for (int o0 = 0; o0 < 3; ++o0) {
+#pragma unroll
+        for (int o1 = 0; o1 < 3; ++o1) {
+#pragma unroll
+            for (int o2 = 0; o2 < n1; ++o2) {
+                const int st[3] = {ord[0][o0], ord[1][o1], D == 3 ? ord[2][o2] : 0};
+                int src[3] = {cc[0], cc[1], cc[2]};
+                bool ok = true;
+                int d = 0;
+#pragma unroll
+                for (int a = 0; a < D; ++a) {
+                    int x = cc[a] - st[a];
+                    if (x < 0 || x >= g.M[a]) {
+                        if (!g.periodic[a]) ok = false;
+                        x = x < 0 ? x + g.M[a] : x - g.M[a];
+                    }
+                    src[a] = x;
+                    d = d * 3 + st[a] + 1;
+                }
+                if (!ok) continue;
+                const long long idx = (long long)cell_to_key(g, src[0], src[1], src[2]) * NC + d;
+                const unsigned t = cls[idx];
+                cls[idx] = total;
+                total += t;
+            }
+        }
     }
     newcount[c] = total;
 }
@@ -609,59 +818,69 @@ __global__ void k_cls_newcount(GridView g, const unsigned* __restrict__ cls, uns
 template <int D, int PUSHER>
 __global__ void __launch_bounds__(kPicThreads) k_cls_pass2(ClsArgs a) {
     constexpr int NC = MoveClasses<D>::N;
+    constexpr int STAY = MoveClasses<D>::STAY;
     __shared__ unsigned base_w[kClsWarps][NC];
-    __shared__ unsigned run_w[kClsWarps][NC];
     if (*a.far) return;   // some particle moved too far: the caller takes the general path
+    const long long ca = a.block_first[blockIdx.x], cb = a.block_first[blockIdx.x + 1];
     const GridView& g = a.p.g;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned full = 0xffffffffu;
-    long long ca, cb;
-    cls_block_cells(a, ca, cb);
+    const unsigned lt = (1u << lane) - 1u;
+    unsigned lost_dummy[2 * D] = {};   // losses were counted by pass 1
     for (long long c = ca + warp; c < cb; c += kClsWarps) {
+        const long long p0 = a.starts[c], p1 = a.starts[c + 1];
+        if (p1 == p0) continue;
         int co[3];
         key_to_cell(g, (int)c, co[0], co[1], co[2]);
         if (lane < NC) {
-            run_w[warp][lane] = 0u;
-            if (__ldg(a.cls + c * NC + lane) != 0u) {
-                // group base: start of the new cell + earlier classes landing there
-                int cn[3], src[3];
-                class_step<D>(g, co, lane, +1, cn);
-                const long long kn = cell_to_key(g, cn[0], cn[1], cn[2]);
-                unsigned b = __ldg(a.new_starts + kn);
-                for (int d2 = 0; d2 < lane; ++d2)
-                    if (class_step<D>(g, cn, d2, -1, src))
-                        b += __ldg(a.cls + (long long)cell_to_key(g, src[0], src[1], src[2]) * NC + d2);
-                base_w[warp][lane] = b;
-            }
+            int cn[3];
+            if (class_target<D>(g, co, lane, cn))
+                base_w[warp][lane] = __ldg(a.new_starts + cell_to_key(g, cn[0], cn[1], cn[2])) +
+                                     __ldg(a.cls + c * NC + lane);
         }
+        CellField<D> F;
+        load_cell_field<D>(a.p, co[0], co[1], co[2], F);
         __syncwarp();
-        const long long p0 = a.starts[c], p1 = a.starts[c + 1];
-        for (long long base = p0; base < p1; base += 32) {
-            const long long i = base + lane;
-            int cls = -2;
-            int cn[3] = {co[0], co[1], co[2]};
-            float f[3] = {0.f, 0.f, 0.f}, v[3] = {0.f, 0.f, 0.f};
-            if (i < p1) {
+        unsigned stay_next = base_w[warp][STAY];   // next slot of the class that keeps its cell
+        for (long long base = p0; base < p1; base += 32 * kClsRounds) {
+            float f[kClsRounds][3], v[kClsRounds][3];
+            bool live[kClsRounds];
 #pragma unroll
-                for (int d = 0; d < D; ++d) f[d] = a.p.off[d][i];
+            for (int r = 0; r < kClsRounds; ++r) {
+                const long long i = base + 32 * r + lane;
+                live[r] = i < p1;
+                f[r][0] = f[r][1] = f[r][2] = 0.f;
+                v[r][0] = v[r][1] = v[r][2] = 0.f;
+                if (live[r]) {
 #pragma unroll
-                for (int q = 0; q < 3; ++q) v[q] = a.p.vel[q][i];
-                const int lost = push_one<D, PUSHER>(a.p, cn, f, v);
-                cls = lost == -1 ? move_class<D>(g, co, cn) : -3;
+                    for (int d = 0; d < D; ++d) f[r][d] = a.p.off[d][i];
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) v[r][q] = a.p.vel[q][i];
+                }
             }
-            const unsigned peers = __match_any_sync(full, cls);
-            if (cls >= 0) {
-                const unsigned dest =
-                    base_w[warp][cls] + run_w[warp][cls] + (unsigned)__popc(peers & ((1u << lane) - 1u));
-                a.key_out[dest] = cell_to_key(g, cn[0], cn[1], cn[2]);
 #pragma unroll
-                for (int d = 0; d < D; ++d) a.off_out[d][dest] = f[d];
+            for (int r = 0; r < kClsRounds; ++r) {
+                int cn[3];
+                const int cls = live[r] ? push_classify<D, PUSHER>(a.p, F, co, f[r], v[r], cn, lost_dummy) : -2;
+                const unsigned stay = __ballot_sync(full, cls == STAY);
+                const bool mover = cls >= 0 && cls != STAY;
+                unsigned dest = stay_next + (unsigned)__popc(stay & lt);
+                unsigned peers = 0u;
+                if (__any_sync(full, mover)) {
+                    peers = __match_any_sync(full, cls);
+                    if (mover) dest = base_w[warp][cls] + (unsigned)__popc(peers & lt);
+                }
+                if (cls >= 0) {
 #pragma unroll
-                for (int q = 0; q < 3; ++q) a.vel_out[q][dest] = v[q];
+                    for (int d = 0; d < D; ++d) a.off_out[d][dest] = f[r][d];
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) a.vel_out[q][dest] = v[r][q];
+                }
+                stay_next += (unsigned)__popc(stay);
+                __syncwarp();
+                if (mover && lane == __ffs(peers) - 1) base_w[warp][cls] += __popc(peers);
+                __syncwarp();
             }
-            __syncwarp();
-            if (cls >= 0 && lane == __ffs(peers) - 1) run_w[warp][cls] += __popc(peers);
-            __syncwarp();
         }
     }
 }
@@ -678,6 +897,14 @@ __global__ void k_cell_starts(const int* __restrict__ key, const long long* __re
 }
 
 __global__ void k_count_from(long long* __restrict__ count, const unsigned* __restrict__ src) { *count = *src; }
+
+// keys of a sorted state from its cell offsets: one warp per cell
+__global__ void k_fill_keys(const unsigned* __restrict__ starts, long long n_cells, int* __restrict__ key) {
+    const long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (c >= n_cells) return;
+    const unsigned e = starts[c + 1];
+    for (unsigned i = starts[c] + (threadIdx.x & 31); i < e; i += 32) key[i] = (int)c;
+}
 
 // ------------------------------------------------------- load / export --
 __global__ void k_load_mixed(GridView g, long long n, const double* __restrict__ pos, const double* __restrict__ vel,
@@ -1165,7 +1392,17 @@ static void radix_sort(psum_pic_ctx* c, long long n, unsigned max_key, unsigned*
     *idx_out = vin;
 }
 
+// The fused sorted step leaves the keys implied by the cell offsets; every
+// reader of the keys calls this first.
+static void ensure_keys(psum_pic_ctx* c, Species& sp) {
+    if (!sp.keys_stale) return;
+    const long long nc = c->g.n_cells;
+    { k_fill_keys<<<blocks_for(nc * 32, 256), 256, 0, c->stream>>>(sp.starts[sp.starts_cur].p, nc, sp.key[sp.cur].p); count_launch(); }
+    sp.keys_stale = false;
+}
+
 static void sort_species(psum_pic_ctx* c, Species& sp, int sidx) {
+    ensure_keys(c, sp);
     const long long n = sp.n;
     if (n <= 0) return;
     cudaStream_t s = c->stream;
@@ -1233,7 +1470,7 @@ static PushArgs make_push_args(psum_pic_ctx* c, Species& sp, int sidx, double dt
     }
     a.qmdt_half = (float)(qm * dt * 0.5);
     a.acc = sp.acc.p;
-    a.scale = std::ldexp(1.0f, sp.dep_shift);
+    a.dep_lsh = sp.dep_shift - kCicBits;
     a.losses = c->losses.p + (size_t)sidx * 6;
     a.err = c->err.p;
     (void)pusher;
@@ -1267,6 +1504,7 @@ static void deposit_all(psum_pic_ctx* c) {
         Species& sp = *c->sp[s];
         if (sp.n <= 0) continue;
         if (c->precision == PSUM_PIC_MIXED) {
+            ensure_keys(c, sp);
             PushArgs a = make_push_args(c, sp, s, 0.0, 0, nullptr);
             launch_mixed(a, c->g.dim, 0, true, sp.n, c->stream);
         } else {
@@ -1297,6 +1535,7 @@ static void push_all(psum_pic_ctx* c, const double* phi, double dt, int pusher, 
         if (sp.n <= 0) continue;
         sp.sorted = false;   // moved in place
         if (c->precision == PSUM_PIC_MIXED) {
+            ensure_keys(c, sp);
             PushArgs a = make_push_args(c, sp, si, dt, pusher, B);
             launch_mixed(a, c->g.dim, pusher, false, sp.n, s);
         } else {
@@ -1332,8 +1571,10 @@ static void sort_all(psum_pic_ctx* c) {
 // k_cls_pass1 / k_cls_pass2.  Species in which some particle moved more
 // than one cell along an axis take the general path (in-place push, radix
 // sort) for this step; their deposit from pass 1 stands.
+static long long cls_blocks(long long n, int dim) { return n / cls_block_particles(dim) + 1; }
+
 static void launch_pass(psum_pic_ctx* c, const ClsArgs& a, int dim, int pusher, int pass, long long n) {
-    const unsigned blocks = (unsigned)(n / kClsBlockParticles + 1);
+    const unsigned blocks = (unsigned)cls_blocks(n, dim);
     cudaStream_t s = c->stream;
 #define PSUM_PASS(D_, P_) \
     do { \
@@ -1353,11 +1594,22 @@ static void launch_pass(psum_pic_ctx* c, const ClsArgs& a, int dim, int pusher, 
 static void ensure_cls_buffers(psum_pic_ctx* c) {
     const long long nc = c->g.n_cells;
     const int ncls = c->g.dim == 2 ? 9 : 27;
+    long long nmax = 0;
+    for (auto& sp : c->sp) nmax = std::max(nmax, sp->n);
     c->cls_count.alloc((size_t)nc * ncls);
+    c->cls_first.alloc((size_t)cls_blocks(nmax, c->g.dim) + 1);
     c->newcount.alloc((size_t)nc + 1);
     c->scan_tmp1.alloc((size_t)(nc + 1 + kScanBlock - 1) / kScanBlock + 1);
     c->scan_tmp2.alloc(16);
     c->far_flag.alloc(8);
+}
+
+// The fused step needs distinct source cells for the classes arriving in a
+// cell: at least 3 internal cells on every periodic axis.
+static bool cls_step_applies(const psum_pic_ctx* c) {
+    for (int a = 0; a < c->g.dim; ++a)
+        if (c->g.periodic[a] && c->g.M[a] < 3) return false;
+    return true;
 }
 
 static void cls_step(psum_pic_ctx* c, const double* phi, double dt, int pusher, const double* B) {
@@ -1368,26 +1620,29 @@ static void cls_step(psum_pic_ctx* c, const double* phi, double dt, int pusher, 
     else { k_edges<3><<<blocks_for(c->g.n_nodes, 256), 256, 0, s>>>(c->g, phi, c->edges.p); count_launch(); }
     cuda_check(cudaMemsetAsync(c->far_flag.p, 0, sizeof(int) * 8, s), "memset");
     const int ns = (int)c->sp.size();
+    const long long nc = c->g.n_cells;
     for (int si = 0; si < ns; ++si) {
         Species& sp = *c->sp[si];
         if (sp.n <= 0) continue;
         ClsArgs a{};
         a.p = make_push_args(c, sp, si, dt, pusher, B);
         a.starts = sp.starts[sp.starts_cur].p;
+        a.block_first = c->cls_first.p;
         a.cls = c->cls_count.p;
         a.new_starts = sp.starts[1 - sp.starts_cur].p;
         a.far = c->far_flag.p + si;
         const int nxt = 1 - sp.cur;
-        a.key_out = sp.key[nxt].p;
         for (int d = 0; d < 3; ++d) {
             a.off_out[d] = d < c->g.dim ? sp.off[d][nxt].p : nullptr;
             a.vel_out[d] = sp.vel[d][nxt].p;
         }
-        a.n_cells = c->g.n_cells;
+        a.n_cells = nc;
+        const long long nb = cls_blocks(sp.n, c->g.dim);
+        { k_cls_blocks<<<blocks_for(std::max(nc, nb) + 1, 256), 256, 0, s>>>(a.starts, nc, nb, cls_block_particles(c->g.dim),
+                                                                             c->cls_first.p); count_launch(); }
         launch_pass(c, a, c->g.dim, pusher, 1, sp.n);
-        const long long nc = c->g.n_cells;
-        if (c->g.dim == 2) { k_cls_newcount<2><<<blocks_for(nc + 1, 256), 256, 0, s>>>(c->g, c->cls_count.p, c->newcount.p, nc); count_launch(); }
-        else { k_cls_newcount<3><<<blocks_for(nc + 1, 256), 256, 0, s>>>(c->g, c->cls_count.p, c->newcount.p, nc); count_launch(); }
+        if (c->g.dim == 2) { k_cls_offsets<2><<<blocks_for(nc + 1, 256), 256, 0, s>>>(c->g, c->cls_count.p, c->newcount.p, nc); count_launch(); }
+        else { k_cls_offsets<3><<<blocks_for(nc + 1, 256), 256, 0, s>>>(c->g, c->cls_count.p, c->newcount.p, nc); count_launch(); }
         exclusive_scan_u32(c->newcount.p, sp.starts[1 - sp.starts_cur].p, nc + 1, c->scan_tmp1.p, c->scan_tmp2.p, s);
         launch_pass(c, a, c->g.dim, pusher, 2, sp.n);
     }
@@ -1401,9 +1656,11 @@ static void cls_step(psum_pic_ctx* c, const double* phi, double dt, int pusher, 
             { k_count_from<<<1, 1, 0, s>>>(c->count.p + si, sp.starts[1 - sp.starts_cur].p + c->g.n_cells); count_launch(); }
             sp.cur = 1 - sp.cur;
             sp.starts_cur = 1 - sp.starts_cur;
+            sp.keys_stale = true;
             continue;
         }
         // general path: move in place (no second deposit), then radix sort
+        ensure_keys(c, sp);
         PushArgs pa = make_push_args(c, sp, si, dt, pusher, B);
         pa.acc = nullptr;
         pa.losses = c->losses.p + 6 * 8;   // discard slot: pass 1 already counted this step's losses
@@ -1543,6 +1800,8 @@ EXPORT int psum_pic_add_species(psum_pic_ctx* ctx, const psum_pic_species_desc* 
         sp->cap = (long long)((capacity + 3) & ~3ULL);
         // fixed point: every node sum stays below 2^62 even if all particles share one node
         sp->dep_shift = 62 - bits_for((unsigned long long)sp->cap);
+        if (ctx->precision == PSUM_PIC_MIXED && sp->dep_shift < kCicBits)
+            throw Error(PSUM_ERR_INVALID_ARGUMENT, "add_species: capacity above 2^36 particles");
         alloc_species_state(ctx, *sp);
         ctx->sp.push_back(std::move(sp));
         *id = (int)ctx->sp.size() - 1;
@@ -1573,6 +1832,7 @@ static void load_common(psum_pic_ctx* ctx, int species, unsigned long long n, co
     { k_set_count<<<1, 1, 0, s>>>(ctx->count.p + species, (long long)n); count_launch(); }
     sp.n = (long long)n;
     sp.sorted = false;
+    sp.keys_stale = false;
     if (ctx->precision == PSUM_PIC_FP64 && n > 0) {
         double* p3[3] = {sp.pos64[0][0].p, ctx->g.dim > 1 ? sp.pos64[1][0].p : nullptr,
                          ctx->g.dim > 2 ? sp.pos64[2][0].p : nullptr};
@@ -1619,6 +1879,7 @@ EXPORT int psum_pic_count(psum_pic_ctx* ctx, int species, unsigned long long* n_
         sp.n = dc;
         if (n_stored) *n_stored = (unsigned long long)dc;
         if (n_valid) {
+            ensure_keys(ctx, sp);
             std::vector<int> keys(dc);
             if (dc > 0)
                 cuda_check(cudaMemcpy(keys.data(), sp.key[sp.cur].p, sizeof(int) * dc, cudaMemcpyDeviceToHost),
@@ -1647,6 +1908,7 @@ EXPORT int psum_pic_get_state(psum_pic_ctx* ctx, int species, double* pos_host, 
         dv.alloc((size_t)n * 3);
         const int cur = sp.cur;
         if (ctx->precision == PSUM_PIC_MIXED) {
+            ensure_keys(ctx, sp);
             { k_export_mixed<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(
                 ctx->g, n, sp.key[cur].p, sp.off[0][cur].p, D > 1 ? sp.off[1][cur].p : nullptr,
                 D > 2 ? sp.off[2][cur].p : nullptr, sp.vel[0][cur].p, sp.vel[1][cur].p, sp.vel[2][cur].p, dp.p, dv.p); count_launch(); }
@@ -1671,6 +1933,7 @@ EXPORT int psum_pic_get_keys(psum_pic_ctx* ctx, int species, int* keys_dev) {
         ctx_check(ctx);
         Species& sp = species_at(ctx, species);
         if (!keys_dev) throw std::invalid_argument("get_keys: null output");
+        ensure_keys(ctx, sp);
         if (sp.n > 0)
             cuda_check(cudaMemcpyAsync(keys_dev, sp.key[sp.cur].p, sizeof(int) * sp.n, cudaMemcpyDeviceToDevice,
                                        ctx->stream),
@@ -1705,6 +1968,7 @@ EXPORT int psum_pic_bin(psum_pic_ctx* ctx, int species, long long* keys_dev, uns
         const int cur = sp.cur;
         if (n > 0) {
             if (ctx->precision == PSUM_PIC_MIXED) {
+                ensure_keys(ctx, sp);
                 { k_bin_keys_mixed<<<blocks_for(n, 256), 256, 0, s>>>(g, sp.key[cur].p, sp.off[0][cur].p, n, keys_dev,
                                                                      ctx->sort.keyA.p, ctx->sort.idxA.p, sentinel); count_launch(); }
             } else {
@@ -1830,7 +2094,7 @@ EXPORT int psum_pic_step(psum_pic_ctx* ctx, psum_field_solver_handle solver, dou
             solver_solve_async(sv, rho_dev, phi_dev, ctx->stream);
             t.stop();
         }
-        bool fused = ctx->precision == PSUM_PIC_MIXED && ctx->sort_interval == 1;
+        bool fused = ctx->precision == PSUM_PIC_MIXED && ctx->sort_interval == 1 && cls_step_applies(ctx);
         for (auto& sp : ctx->sp) fused = fused && (sp->sorted || sp->n == 0);
         if (pusher != PSUM_PIC_LEAPFROG && pusher != PSUM_PIC_BORIS) throw std::invalid_argument("step: unknown pusher");
         if (fused) {
@@ -1891,6 +2155,7 @@ EXPORT int psum_pic_diagnostics(psum_pic_ctx* ctx, const double* phi_dev, double
         for (int si = 0; si < ns; ++si) {
             Species& sp = *ctx->sp[si];
             const int cur = sp.cur;
+            if (ctx->precision == PSUM_PIC_MIXED) ensure_keys(ctx, *ctx->sp[si]);
             if (ctx->precision == PSUM_PIC_MIXED)
                 { k_kinetic_mixed<<<kDiagBlocks, 256, 0, s>>>(sp.key[cur].p, sp.vel[0][cur].p, sp.vel[1][cur].p,
                                                           sp.vel[2][cur].p, ctx->count.p + si, sp.m * sp.w,

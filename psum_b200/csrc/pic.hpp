@@ -31,6 +31,7 @@ struct Species {
     DevBuf<unsigned> starts[2];
     int starts_cur = 0;
     bool sorted = false;              // state sorted by cell and starts valid
+    bool keys_stale = false;          // sorted mixed state whose keys follow from starts but are not written
 };
 
 struct SortScratch {
@@ -56,7 +57,8 @@ struct psum_pic_ctx {
     psum_b200::DevBuf<double> partials;
     psum_b200::DevBuf<long long> ipartials;
     psum_b200::SortScratch sort;
-    psum_b200::DevBuf<unsigned> cls_count;    // per (cell, move class) counts of the fused sorted step
+    psum_b200::DevBuf<unsigned> cls_count;    // per (cell, move class) counts, then group offsets, of the fused sorted step
+    psum_b200::DevBuf<unsigned> cls_first;    // first cell owned by each block of the fused sorted step
     psum_b200::DevBuf<unsigned> newcount;     // per new cell counts (n_cells + 1)
     psum_b200::DevBuf<unsigned> scan_tmp1, scan_tmp2;
     psum_b200::DevBuf<int> far_flag;          // per species: a particle moved more than one cell on an axis

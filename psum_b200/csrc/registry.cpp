@@ -25,9 +25,16 @@ std::mutex& registry_mutex() {
 }
 thread_local std::string g_last_error;
 std::atomic<unsigned long long> g_launches{0};
+thread_local unsigned long long g_thread_launches = 0;
 }  // namespace
 
-void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void count_launch() {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    ++g_thread_launches;
+}
+void add_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+void uncount_launches(unsigned long long n) { g_launches.fetch_sub(n, std::memory_order_relaxed); }
+unsigned long long thread_launches() { return g_thread_launches; }
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 const std::string& last_error() { return g_last_error; }

@@ -372,13 +372,18 @@ def test_load_device_buffers_reusable_immediately():
     assert np.abs(got_vel - vel.astype(np.float32)).max() == 0.0
 
 
-def _fused_vs_general(kind, pusher, dt, seed, vscale=1.0, species=2):
+def _fused_vs_general(kind, pusher, dt, seed, vscale=1.0, species=2, sort_general=False, cluster=None):
     """Runs one step on the same sorted state with the fused sorted step
-    (sort_interval 1) and with the general path (push in place, then stable
-    radix sort); returns both results."""
+    (sort_interval 1) and with the general path (push in place; with
+    sort_general, followed by the stable radix sort); returns both results.
+    cluster = (centre, sigma) draws the positions from a Gaussian blob."""
     out = []
     for interval in (1, 0):
         ctx, g, pos, vel, phi = make_case(kind, P.MIXED, seed=seed, n=40000)
+        if cluster is not None:
+            rng_c = np.random.default_rng(seed + 7)
+            centre, sigma = cluster
+            pos = np.stack([rng_c.normal(centre[a], sigma, pos.shape[1]) for a in range(g.dim)])
         pos = wrap_into(pos, g)
         ctx.set_options(f"sort_interval {interval}")
         sps = []
@@ -400,6 +405,8 @@ def _fused_vs_general(kind, pusher, dt, seed, vscale=1.0, species=2):
         phi_t = dev(phi)
         ctx.deposit()
         ctx.step(solver, 0.0, rho, phi_t, dt, pusher, (0.2, -0.1, 0.4))
+        if sort_general and interval == 0:
+            ctx.sort()
         torch.cuda.synchronize()
         res = []
         for sp in sps:
@@ -445,4 +452,37 @@ def test_fused_step_far_movers_fall_back():
         ok = ~np.isnan(pg[0])
         a2, b2 = _canon(pg[:, ok], vg[:, ok])
         assert (a1.view(np.int64) == a2.view(np.int64)).all()
+        assert (df.view(np.int64) == dg.view(np.int64)).all()
+
+
+@pytest.mark.parametrize("kind", ["2d_absorb", "2d_periodic", "2d_mixed_bc", "3d_periodic"])
+@pytest.mark.parametrize("pusher", [P.LEAPFROG, P.BORIS])
+def test_fused_step_equals_general_step_then_stable_sort(kind, pusher):
+    # the fused step orders each new cell by old position: exactly the stable
+    # sort of the pushed state, so arrays agree element by element
+    # dt small enough that no particle crosses more than one cell (no fallback)
+    (fused, loss_f, cnt_f), (gen, loss_g, cnt_g) = _fused_vs_general(kind, pusher, 0.12, seed=33,
+                                                                      sort_general=True)
+    assert (loss_f == loss_g).all()
+    assert cnt_f == cnt_g
+    for (pf, vf, kf, df), (pg, vg, kg, dg) in zip(fused, gen):
+        assert (kf == kg).all()
+        assert (pf.view(np.int64) == pg.view(np.int64)).all()
+        assert (vf.view(np.int64) == vg.view(np.int64)).all()
+        assert (df.view(np.int64) == dg.view(np.int64)).all()
+
+
+@pytest.mark.parametrize("kind", ["2d_periodic", "3d_periodic"])
+def test_fused_step_clustered_cells(kind):
+    # a dense blob: cells far above one block's particle budget, many empty
+    # blocks and cells, long per-warp runs
+    centre = (32.0, 32.0) if kind == "2d_periodic" else (8.0, 8.0, 8.0)
+    (fused, loss_f, cnt_f), (gen, loss_g, cnt_g) = _fused_vs_general(kind, P.LEAPFROG, 0.12, seed=34,
+                                                                      sort_general=True, cluster=(centre, 0.6))
+    assert cnt_f == cnt_g
+    for (pf, vf, kf, df), (pg, vg, kg, dg) in zip(fused, gen):
+        assert np.bincount(kf).max() > 4096
+        assert (kf == kg).all()
+        assert (pf.view(np.int64) == pg.view(np.int64)).all()
+        assert (vf.view(np.int64) == vg.view(np.int64)).all()
         assert (df.view(np.int64) == dg.view(np.int64)).all()
