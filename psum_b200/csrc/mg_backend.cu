@@ -57,15 +57,19 @@ struct DevStencil {
         exc_val.upload(v.data(), v.size(), s);
         cuda_check(cudaStreamSynchronize(s), "upload stencil");
         exceptions = (long long)op.exc_rows.size();
+        if (op.n >= (1LL << 31)) throw std::invalid_argument("multigrid: more than 2^31 - 1 rows per level");
         view.n0 = op.dims[0];
         view.n1 = op.dims[1];
         view.n2 = op.dims[2];
         view.n = op.n;
         view.ns = op.ns;
+        view.div12 = make_fastdiv((unsigned)(op.dims[1] * op.dims[2]));
+        view.div2 = make_fastdiv((unsigned)op.dims[2]);
         for (int t = 0; t < op.ns && t < kMaxTaps; ++t) {
             view.di[t] = (signed char)op.delta[t][0];
             view.dj[t] = (signed char)op.delta[t][1];
             view.dk[t] = (signed char)op.delta[t][2];
+            view.off[t] = (op.delta[t][0] * op.dims[1] + op.delta[t][1]) * op.dims[2] + op.delta[t][2];
             view.c[t] = T(op.coef[t]);
         }
         view.mask = mask.p;
@@ -100,6 +104,32 @@ struct DevAxis {
         view.r_w = r_w.p;
     }
 };
+
+// Launches of the stencil kernels with the operator's tap count as a
+// compile-time constant where it is one of the common ones.
+template <class T, int Mode>
+void launch_level_op(const StencilDev<T>& A, const T* x, const T* b, T* out, T omega, const MGState* st,
+                     cudaStream_t s) {
+    const unsigned g = grid_for(A.n);
+    if (Mode == kSmoothFromZero) k_level_op<T, Mode, 0><<<g, kThreads, 0, s>>>(A, x, b, out, omega, st);
+    else if (A.ns == 5) k_level_op<T, Mode, 5><<<g, kThreads, 0, s>>>(A, x, b, out, omega, st);
+    else if (A.ns == 7) k_level_op<T, Mode, 7><<<g, kThreads, 0, s>>>(A, x, b, out, omega, st);
+    else if (A.ns == 9) k_level_op<T, Mode, 9><<<g, kThreads, 0, s>>>(A, x, b, out, omega, st);
+    else if (A.ns == 27) k_level_op<T, Mode, 27><<<g, kThreads, 0, s>>>(A, x, b, out, omega, st);
+    else k_level_op<T, Mode, 0><<<g, kThreads, 0, s>>>(A, x, b, out, omega, st);
+    count_launch();
+}
+
+template <class TOut>
+void launch_residual64(const StencilDev<double>& A, const double* x, const double* b, const double* dinv, TOut* bhat,
+                       double* partials, const MGState* st, int gated, cudaStream_t s) {
+    if (A.ns == 5) k_residual64<TOut, 5><<<kNormBlocks, kThreads, 0, s>>>(A, x, b, dinv, bhat, partials, st, gated);
+    else if (A.ns == 7) k_residual64<TOut, 7><<<kNormBlocks, kThreads, 0, s>>>(A, x, b, dinv, bhat, partials, st, gated);
+    else if (A.ns == 9) k_residual64<TOut, 9><<<kNormBlocks, kThreads, 0, s>>>(A, x, b, dinv, bhat, partials, st, gated);
+    else if (A.ns == 27) k_residual64<TOut, 27><<<kNormBlocks, kThreads, 0, s>>>(A, x, b, dinv, bhat, partials, st, gated);
+    else k_residual64<TOut, 0><<<kNormBlocks, kThreads, 0, s>>>(A, x, b, dinv, bhat, partials, st, gated);
+    count_launch();
+}
 
 template <class T>
 struct Level {
@@ -174,7 +204,6 @@ struct Solver : SolverBase {
     std::vector<std::unique_ptr<Level<T>>> lv;
     DevBuf<T> coarse_inv;
     DevBuf<double> x64;   // FP64 level-0 iterate for the FP64 backend
-
     void build_device(cudaStream_t s) override {
         a0.upload(host.a0, s);
         dinv0.upload(host.dinv[0].data(), host.dinv[0].size(), s);
@@ -190,8 +219,14 @@ struct Solver : SolverBase {
             L->bufA.alloc(L->n);
             L->bufB.alloc(L->n);
             L->b.alloc(L->n);
-            if (l < host.L)
+            if (l < host.L) {
                 for (int a = 0; a < 3; ++a) L->axes[a].upload(host.xfer[l][a], s, L->xfer.ax[a]);
+                const AxisDev<T>* ax = L->xfer.ax;
+                L->xfer.divc12 = make_fastdiv((unsigned)(ax[1].nc * ax[2].nc));
+                L->xfer.divc2 = make_fastdiv((unsigned)ax[2].nc);
+                L->xfer.divf12 = make_fastdiv((unsigned)(ax[1].nf * ax[2].nf));
+                L->xfer.divf2 = make_fastdiv((unsigned)ax[2].nf);
+            }
             lv.push_back(std::move(L));
         }
         std::vector<T> ci(host.coarse_inv.begin(), host.coarse_inv.end());
@@ -222,12 +257,11 @@ struct Solver : SolverBase {
         zero[0] = x_is_zero;
         auto smooth = [&](int l) {
             Level<T>& V = *lv[l];
-            const unsigned g = grid_for(V.n);
             if (zero[l]) {
-                { k_level_op<T, kSmoothFromZero><<<g, kThreads, 0, s>>>(V.op.view, xcur[l], bl[l], xoth[l], omega, st); count_launch(); }
+                launch_level_op<T, kSmoothFromZero>(V.op.view, xcur[l], bl[l], xoth[l], omega, st, s);
                 zero[l] = false;
             } else {
-                { k_level_op<T, kSmooth><<<g, kThreads, 0, s>>>(V.op.view, xcur[l], bl[l], xoth[l], omega, st); count_launch(); }
+                launch_level_op<T, kSmooth>(V.op.view, xcur[l], bl[l], xoth[l], omega, st, s);
             }
             std::swap(xcur[l], xoth[l]);
         };
@@ -240,8 +274,7 @@ struct Solver : SolverBase {
                     { k_restrict<T><<<grid_for(lv[l + 1]->n), kThreads, 0, s>>>(V.xfer, bl[l], bl[l + 1], xcur[l + 1],
                                                                              lv[l + 1]->dinv.p, st); count_launch(); }
                 } else {
-                    { k_level_op<T, kResidual><<<grid_for(V.n), kThreads, 0, s>>>(V.op.view, xcur[l], bl[l], xoth[l],
-                                                                                omega, st); count_launch(); }
+                    launch_level_op<T, kResidual>(V.op.view, xcur[l], bl[l], xoth[l], omega, st, s);
                     { k_restrict<T><<<grid_for(lv[l + 1]->n), kThreads, 0, s>>>(V.xfer, xoth[l], bl[l + 1],
                                                                              xcur[l + 1], lv[l + 1]->dinv.p, st); count_launch(); }
                 }
@@ -285,7 +318,7 @@ struct Solver : SolverBase {
             // FP64 refinement around FP32 V-cycles (sycl_multigrid32f_gpu.cpp:137-157)
             while (cycles_done < max_cycles) {
                 const int batch = std::min(correction_interval, max_cycles - cycles_done);
-                { k_residual64<T><<<kNormBlocks, kThreads, 0, s>>>(a0.view, x, b, dinv0.p, F.b.p, partials.p, st, 1); count_launch(); }
+                launch_residual64<T>(a0.view, x, b, dinv0.p, F.b.p, partials.p, st, 1, s);
                 { k_check<<<1, 32, 0, s>>>(partials.p, kNormBlocks, st, 1, tol, cycles_done, refinements); count_launch(); }
                 T* e = enqueue_vcycles(F.bufA.p, F.bufB.p, F.b.p, batch, /*x_is_zero=*/true, s);
                 { k_correct<T><<<grid_for(n), kThreads, 0, s>>>(x, e, n, st); count_launch(); }
@@ -300,8 +333,7 @@ struct Solver : SolverBase {
             while (cycles_done < max_cycles) {
                 const int batch = tol > 0 ? std::min(correction_interval, max_cycles - cycles_done) : max_cycles;
                 if (tol > 0) {
-                    { k_residual64<double><<<kNormBlocks, kThreads, 0, s>>>(a0.view, xc, b, nullptr, (double*)nullptr,
-                                                                          partials.p, st, 1); count_launch(); }
+                    launch_residual64<double>(a0.view, xc, b, nullptr, (double*)nullptr, partials.p, st, 1, s);
                     { k_check<<<1, 32, 0, s>>>(partials.p, kNormBlocks, st, 1, tol, cycles_done, refinements); count_launch(); }
                 }
                 T* r = enqueue_vcycles(reinterpret_cast<T*>(xc), reinterpret_cast<T*>(xo), F.b.p, batch, false, s);
@@ -310,7 +342,7 @@ struct Solver : SolverBase {
             }
             cuda_check(cudaMemcpyAsync(x, xc, sizeof(double) * n, cudaMemcpyDeviceToDevice, s), "copy x");
         }
-        { k_residual64<double><<<kNormBlocks, kThreads, 0, s>>>(a0.view, x, b, nullptr, (double*)nullptr, partials.p, st, 0); count_launch(); }
+        launch_residual64<double>(a0.view, x, b, nullptr, (double*)nullptr, partials.p, st, 0, s);
         { k_check<<<1, 32, 0, s>>>(partials.p, kNormBlocks, st, 2, tol, cycles_done, refinements); count_launch(); }
         cuda_check(cudaGetLastError(), "solve launch");
     }

@@ -2,17 +2,21 @@
 //
 // Every level operator is a constant stencil (<= 27 taps with periodic wrap
 // on the level's node box) plus an exception CSR for the rows that differ
-// (mg_host.hpp).  All kernels are HBM-bound streaming kernels: one row per
-// thread, coalesced along the last (fastest) dimension; neighbour rows are
-// re-read through L1/L2.  Kernels in the V-cycle return immediately once the
-// solve's device-side `done` flag is set, so a fixed launch schedule can stop
-// early without a host round trip.
+// (mg_host.hpp).  All kernels are streaming kernels: one row per thread,
+// coalesced along the last (fastest) dimension; neighbour rows are re-read
+// through L1/L2.  The tap loop is unrolled for the common tap counts (5, 7,
+// 9, 27) so every load of a row is in flight at once, interior rows use
+// precomputed linear offsets, and the exception-row test runs beside the
+// stencil loads instead of before them.  Kernels in the V-cycle return
+// immediately once the solve's device-side `done` flag is set, so a fixed
+// launch schedule can stop early without a host round trip.
 #pragma once
 
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "../../include/psum_field_solver.h"
+#include "fastdiv.cuh"
 
 namespace psum_b200 {
 
@@ -32,10 +36,12 @@ struct MGState {
 template <class T>
 struct StencilDev {
     int n0, n1, n2;
-    long long n;
+    long long n;            // rows (below 2^31)
     int ns;
     signed char di[kMaxTaps], dj[kMaxTaps], dk[kMaxTaps];
+    int off[kMaxTaps];      // linear offset of each tap on interior rows
     T c[kMaxTaps];
+    FastDiv div12, div2;    // by n1 * n2 and by n2
     const uint32_t* mask;
     const uint32_t* mask_prefix;
     const int* exc_ptr;
@@ -57,33 +63,55 @@ struct AxisDev {
 template <class T>
 struct XferDev {
     AxisDev<T> ax[3];
+    FastDiv divc12, divc2;   // coarse box: by nc1 * nc2 and by nc2
+    FastDiv divf12, divf2;   // fine box: by nf1 * nf2 and by nf2
 };
 
 __device__ __forceinline__ int wrap_idx(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
 // (A x)_r for one row of a stencil operator; Acc is the accumulation type.
-template <class T, class Acc>
-__device__ __forceinline__ Acc stencil_row(const StencilDev<T>& A, const T* __restrict__ x, long long r) {
+// NS > 0: the operator has exactly NS taps; NS == 0: any count up to 27.
+// Taps are summed in order, so every NS gives the same rounding.
+// Load of data that is read-only while the kernel runs (RO = true, through
+// the read-only path) or that the running kernel may have written (RO = false).
+template <bool RO, class T>
+__device__ __forceinline__ T ldv(const T* p) {
+    if constexpr (RO) return __ldg(p);
+    else return *p;
+}
+
+template <class T, class Acc, int NS, bool RO = true>
+__device__ __forceinline__ Acc stencil_row(const StencilDev<T>& A, const T* __restrict__ x, int r) {
     const uint32_t word = __ldg(A.mask + (r >> 5));
-    const uint32_t bit = 1u << (r & 31);
+    const int i = (int)fastdiv((unsigned)r, A.div12);
+    const int rem = r - i * (int)A.div12.d;
+    const int j = (int)fastdiv((unsigned)rem, A.div2);
+    const int k = rem - j * A.n2;
+    const bool interior = (A.n0 == 1 || (i > 0 && i < A.n0 - 1)) && (A.n1 == 1 || (j > 0 && j < A.n1 - 1)) &&
+                          (A.n2 == 1 || (k > 0 && k < A.n2 - 1));
+    constexpr int NT = NS > 0 ? NS : kMaxTaps;
     Acc s = Acc(0);
+    if (interior) {
+#pragma unroll
+        for (int t = 0; t < NT; ++t)
+            if (NS > 0 || t < A.ns) s += Acc(A.c[t]) * Acc(ldv<RO>(x + r + A.off[t]));
+    } else {
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+            if (NS > 0 || t < A.ns) {
+                const int ii = wrap_idx(i + A.di[t], A.n0);
+                const int jj = wrap_idx(j + A.dj[t], A.n1);
+                const int kk = wrap_idx(k + A.dk[t], A.n2);
+                s += Acc(A.c[t]) * Acc(ldv<RO>(x + (ii * A.n1 + jj) * A.n2 + kk));
+            }
+        }
+    }
+    const uint32_t bit = 1u << (r & 31);
     if (word & bit) {
         const int q = (int)__ldg(A.mask_prefix + (r >> 5)) + __popc(word & (bit - 1u));
         const int b = __ldg(A.exc_ptr + q), e = __ldg(A.exc_ptr + q + 1);
-        for (int k = b; k < e; ++k) s += Acc(__ldg(A.exc_val + k)) * Acc(__ldg(x + __ldg(A.exc_col + k)));
-        return s;
-    }
-    const long long n12 = (long long)A.n1 * A.n2;
-    const int i = (int)(r / n12);
-    const long long rem = r - (long long)i * n12;
-    const int j = (int)(rem / A.n2);
-    const int k = (int)(rem - (long long)j * A.n2);
-#pragma unroll 1
-    for (int t = 0; t < A.ns; ++t) {
-        const int ii = wrap_idx(i + A.di[t], A.n0);
-        const int jj = wrap_idx(j + A.dj[t], A.n1);
-        const int kk = wrap_idx(k + A.dk[t], A.n2);
-        s += Acc(A.c[t]) * Acc(__ldg(x + ((long long)ii * A.n1 + jj) * A.n2 + kk));
+        s = Acc(0);
+        for (int t = b; t < e; ++t) s += Acc(__ldg(A.exc_val + t)) * Acc(ldv<RO>(x + __ldg(A.exc_col + t)));
     }
     return s;
 }
@@ -93,37 +121,38 @@ enum SmoothMode { kSmooth = 0, kSmoothFromZero = 1, kResidual = 2 };
 // kSmooth:          out = x + w (b - A x)      (damped Jacobi on the scaled system)
 // kSmoothFromZero:  out = w b                  (first sweep from x = 0)
 // kResidual:        out = b - A x
-template <class T, int Mode>
+template <class T, int Mode, int NS, bool RO>
+__device__ __forceinline__ void level_row(const StencilDev<T>& A, const T* __restrict__ x, const T* __restrict__ b,
+                                          T* __restrict__ out, T omega, int r) {
+    if (Mode == kSmoothFromZero) {
+        out[r] = omega * ldv<RO>(b + r);
+        return;
+    }
+    const T ax = stencil_row<T, T, NS, RO>(A, x, r);
+    if (Mode == kSmooth) out[r] = ldv<RO>(x + r) + omega * (ldv<RO>(b + r) - ax);
+    else out[r] = ldv<RO>(b + r) - ax;
+}
+
+template <class T, int Mode, int NS>
 __global__ void __launch_bounds__(kThreads) k_level_op(StencilDev<T> A, const T* __restrict__ x,
                                                        const T* __restrict__ b, T* __restrict__ out, T omega,
                                                        const MGState* __restrict__ st) {
     if (st->done) return;
-    const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= A.n) return;
-    if (Mode == kSmoothFromZero) {
-        out[r] = omega * b[r];
-        return;
-    }
-    const T ax = stencil_row<T, T>(A, x, r);
-    if (Mode == kSmooth) out[r] = x[r] + omega * (b[r] - ax);
-    else out[r] = b[r] - ax;
+    level_row<T, Mode, NS, true>(A, x, b, out, omega, r);
 }
 
-// b_c = dinv_c * (R r_f), x_c = 0
-template <class T>
-__global__ void __launch_bounds__(kThreads) k_restrict(XferDev<T> X, const T* __restrict__ rf, T* __restrict__ bc,
-                                                       T* __restrict__ xc, const T* __restrict__ dinv_c,
-                                                       const MGState* __restrict__ st) {
-    if (st->done) return;
-    const int nc0 = X.ax[0].nc, nc1 = X.ax[1].nc, nc2 = X.ax[2].nc;
+// b_c = dinv_c * (R r_f), x_c = 0 at coarse row c
+template <class T, bool RO>
+__device__ __forceinline__ void restrict_row(const XferDev<T>& X, const T* __restrict__ rf, T* __restrict__ bc,
+                                             T* __restrict__ xc, const T* __restrict__ dinv_c, int c) {
+    const int nc1 = X.ax[1].nc, nc2 = X.ax[2].nc;
     const int nf1 = X.ax[1].nf, nf2 = X.ax[2].nf;
-    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long ncount = (long long)nc0 * nc1 * nc2;
-    if (c >= ncount) return;
-    const int ci = (int)(c / ((long long)nc1 * nc2));
-    const long long rem = c - (long long)ci * nc1 * nc2;
-    const int cj = (int)(rem / nc2);
-    const int ck = (int)(rem - (long long)cj * nc2);
+    const int ci = (int)fastdiv((unsigned)c, X.divc12);
+    const int rem = c - ci * nc1 * nc2;
+    const int cj = (int)fastdiv((unsigned)rem, X.divc2);
+    const int ck = rem - cj * nc2;
     T s = T(0);
 #pragma unroll
     for (int qa = 0; qa < 3; ++qa) {
@@ -135,33 +164,38 @@ __global__ void __launch_bounds__(kThreads) k_restrict(XferDev<T> X, const T* __
             const int fj = __ldg(X.ax[1].r_f + 3 * cj + qb);
             if (fj < 0) continue;
             const T wij = wi * __ldg(X.ax[1].r_w + 3 * cj + qb);
-            const T* row = rf + ((long long)fi * nf1 + fj) * nf2;
+            const T* row = rf + (fi * nf1 + fj) * nf2;
 #pragma unroll
             for (int qc = 0; qc < 3; ++qc) {
                 const int fk = __ldg(X.ax[2].r_f + 3 * ck + qc);
                 if (fk < 0) continue;
-                s += (wij * __ldg(X.ax[2].r_w + 3 * ck + qc)) * __ldg(row + fk);
+                s += (wij * __ldg(X.ax[2].r_w + 3 * ck + qc)) * ldv<RO>(row + fk);
             }
         }
     }
-    bc[c] = s * dinv_c[c];
+    bc[c] = s * __ldg(dinv_c + c);
     xc[c] = T(0);
 }
 
-// x_f += P x_c
 template <class T>
-__global__ void __launch_bounds__(kThreads) k_prolong_add(XferDev<T> X, const T* __restrict__ xc, T* __restrict__ xf,
-                                                          const MGState* __restrict__ st) {
+__global__ void __launch_bounds__(kThreads) k_restrict(XferDev<T> X, const T* __restrict__ rf, T* __restrict__ bc,
+                                                       T* __restrict__ xc, const T* __restrict__ dinv_c,
+                                                       const MGState* __restrict__ st) {
     if (st->done) return;
-    const int nf0 = X.ax[0].nf, nf1 = X.ax[1].nf, nf2 = X.ax[2].nf;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= X.ax[0].nc * X.ax[1].nc * X.ax[2].nc) return;
+    restrict_row<T, true>(X, rf, bc, xc, dinv_c, c);
+}
+
+// x_f += P x_c at fine row f
+template <class T, bool RO>
+__device__ __forceinline__ void prolong_row(const XferDev<T>& X, const T* __restrict__ xc, T* __restrict__ xf, int f) {
+    const int nf1 = X.ax[1].nf, nf2 = X.ax[2].nf;
     const int nc1 = X.ax[1].nc, nc2 = X.ax[2].nc;
-    const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long nfc = (long long)nf0 * nf1 * nf2;
-    if (f >= nfc) return;
-    const int fi = (int)(f / ((long long)nf1 * nf2));
-    const long long rem = f - (long long)fi * nf1 * nf2;
-    const int fj = (int)(rem / nf2);
-    const int fk = (int)(rem - (long long)fj * nf2);
+    const int fi = (int)fastdiv((unsigned)f, X.divf12);
+    const int rem = f - fi * nf1 * nf2;
+    const int fj = (int)fastdiv((unsigned)rem, X.divf2);
+    const int fk = rem - fj * nf2;
     const int ci[2] = {__ldg(X.ax[0].p_c0 + fi), __ldg(X.ax[0].p_c1 + fi)};
     const int cj[2] = {__ldg(X.ax[1].p_c0 + fj), __ldg(X.ax[1].p_c1 + fj)};
     const int ck[2] = {__ldg(X.ax[2].p_c0 + fk), __ldg(X.ax[2].p_c1 + fk)};
@@ -178,14 +212,33 @@ __global__ void __launch_bounds__(kThreads) k_prolong_add(XferDev<T> X, const T*
 #pragma unroll
             for (int c2 = 0; c2 < 2; ++c2) {
                 if (ck[c2] < 0) continue;
-                s += (wi[a] * wj[b2] * wk[c2]) * __ldg(xc + ((long long)ci[a] * nc1 + cj[b2]) * nc2 + ck[c2]);
+                s += (wi[a] * wj[b2] * wk[c2]) * ldv<RO>(xc + (ci[a] * nc1 + cj[b2]) * nc2 + ck[c2]);
             }
         }
     }
     xf[f] = s + xf[f];
 }
 
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_prolong_add(XferDev<T> X, const T* __restrict__ xc, T* __restrict__ xf,
+                                                          const MGState* __restrict__ st) {
+    if (st->done) return;
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= X.ax[0].nf * X.ax[1].nf * X.ax[2].nf) return;
+    prolong_row<T, true>(X, xc, xf, f);
+}
+
 // x = Ainv b (dense, row-major), one warp per row, fixed shuffle tree.
+template <class T, bool RO>
+__device__ __forceinline__ T dense_row(const T* __restrict__ Ainv, const T* __restrict__ b, int n, int row, int lane) {
+    const T* a = Ainv + (long long)row * n;
+    T s = T(0);
+    for (int c = lane; c < n; c += 32) s += __ldg(a + c) * ldv<RO>(b + c);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    return s;
+}
+
 template <class T>
 __global__ void __launch_bounds__(kThreads) k_dense_mv(const T* __restrict__ Ainv, const T* __restrict__ b,
                                                        T* __restrict__ x, int n, const MGState* __restrict__ st) {
@@ -193,11 +246,7 @@ __global__ void __launch_bounds__(kThreads) k_dense_mv(const T* __restrict__ Ain
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= n) return;
-    const T* row = Ainv + (long long)warp * n;
-    T s = T(0);
-    for (int c = lane; c < n; c += 32) s += __ldg(row + c) * __ldg(b + c);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    const T s = dense_row<T, true>(Ainv, b, n, warp, lane);
     if (lane == 0) x[warp] = s;
 }
 
@@ -219,16 +268,15 @@ __device__ __forceinline__ double block_sum(double v) {
 // FP64 residual of the unscaled fine operator: r = b - A x; optional output
 // bhat = TOut(dinv * r) (the FP32 defect of the refinement); per-block
 // partial sums of r^2 (grid-stride, fixed grid -> deterministic).
-template <class TOut>
+template <class TOut, int NS>
 __global__ void __launch_bounds__(kThreads) k_residual64(StencilDev<double> A, const double* __restrict__ x,
                                                          const double* __restrict__ b, const double* __restrict__ dinv,
                                                          TOut* __restrict__ bhat, double* __restrict__ partials,
                                                          const MGState* __restrict__ st, int gated) {
     if (gated && st->done) return;
     double acc = 0.0;
-    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < A.n;
-         r += (long long)gridDim.x * blockDim.x) {
-        const double ax = stencil_row<double, double>(A, x, r);
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < A.n; r += gridDim.x * blockDim.x) {
+        const double ax = stencil_row<double, double, NS>(A, x, r);
         const double res = b[r] - ax;
         acc += res * res;
         if (bhat) bhat[r] = TOut(dinv[r] * res);

@@ -815,11 +815,26 @@ __global__ void k_cls_offsets(GridView g, unsigned* __restrict__ cls, unsigned* 
     newcount[c] = total;
 }
 
+// Mover slots per class in the pass-2 staging buffer of a warp.
+template <int D>
+struct MoverStage {
+    static constexpr int MS = D == 2 ? 8 : 4;
+    static constexpr int SLOTS = (MoveClasses<D>::N - 1) * MS;
+};
+
 template <int D, int PUSHER>
 __global__ void __launch_bounds__(kPicThreads) k_cls_pass2(ClsArgs a) {
     constexpr int NC = MoveClasses<D>::N;
     constexpr int STAY = MoveClasses<D>::STAY;
+    constexpr int MS = MoverStage<D>::MS;
+    constexpr int SLOTS = MoverStage<D>::SLOTS;
+    constexpr int NF = D + 3;   // offsets, then velocities
+    // per (warp, class): global slot of the first staged (or next) particle,
+    // and the number staged; movers are staged per class so that each
+    // class's run is written with consecutive lanes
     __shared__ unsigned base_w[kClsWarps][NC];
+    __shared__ unsigned fill_w[kClsWarps][NC];
+    __shared__ float stage[kClsWarps][NF][SLOTS];
     if (*a.far) return;   // some particle moved too far: the caller takes the general path
     const long long ca = a.block_first[blockIdx.x], cb = a.block_first[blockIdx.x + 1];
     const GridView& g = a.p.g;
@@ -827,6 +842,30 @@ __global__ void __launch_bounds__(kPicThreads) k_cls_pass2(ClsArgs a) {
     const unsigned full = 0xffffffffu;
     const unsigned lt = (1u << lane) - 1u;
     unsigned lost_dummy[2 * D] = {};   // losses were counted by pass 1
+    auto out_field = [&](int fld) -> float* { return fld < D ? a.off_out[fld] : a.vel_out[fld - D]; };
+    // write every staged mover, class by class, and advance the class bases
+    auto flush = [&]() {
+        __syncwarp();
+#pragma unroll
+        for (int s0 = 0; s0 < SLOTS; s0 += 32) {
+            const int s = s0 + lane;
+            if (s < SLOTS) {
+                const int k = s / MS, pos = s - k * MS;
+                const int cls = k < STAY ? k : k + 1;
+                if (pos < (int)fill_w[warp][cls]) {
+                    const unsigned dest = base_w[warp][cls] + pos;
+#pragma unroll
+                    for (int fld = 0; fld < NF; ++fld) out_field(fld)[dest] = stage[warp][fld][s];
+                }
+            }
+        }
+        __syncwarp();
+        if (lane < NC && lane != STAY) {
+            base_w[warp][lane] += fill_w[warp][lane];
+            fill_w[warp][lane] = 0u;
+        }
+        __syncwarp();
+    };
     for (long long c = ca + warp; c < cb; c += kClsWarps) {
         const long long p0 = a.starts[c], p1 = a.starts[c + 1];
         if (p1 == p0) continue;
@@ -834,6 +873,7 @@ __global__ void __launch_bounds__(kPicThreads) k_cls_pass2(ClsArgs a) {
         key_to_cell(g, (int)c, co[0], co[1], co[2]);
         if (lane < NC) {
             int cn[3];
+            fill_w[warp][lane] = 0u;
             if (class_target<D>(g, co, lane, cn))
                 base_w[warp][lane] = __ldg(a.new_starts + cell_to_key(g, cn[0], cn[1], cn[2])) +
                                      __ldg(a.cls + c * NC + lane);
@@ -863,25 +903,49 @@ __global__ void __launch_bounds__(kPicThreads) k_cls_pass2(ClsArgs a) {
                 int cn[3];
                 const int cls = live[r] ? push_classify<D, PUSHER>(a.p, F, co, f[r], v[r], cn, lost_dummy) : -2;
                 const unsigned stay = __ballot_sync(full, cls == STAY);
-                const bool mover = cls >= 0 && cls != STAY;
-                unsigned dest = stay_next + (unsigned)__popc(stay & lt);
-                unsigned peers = 0u;
-                if (__any_sync(full, mover)) {
-                    peers = __match_any_sync(full, cls);
-                    if (mover) dest = base_w[warp][cls] + (unsigned)__popc(peers & lt);
-                }
-                if (cls >= 0) {
+                if (cls == STAY) {
+                    const unsigned dest = stay_next + (unsigned)__popc(stay & lt);
 #pragma unroll
                     for (int d = 0; d < D; ++d) a.off_out[d][dest] = f[r][d];
 #pragma unroll
                     for (int q = 0; q < 3; ++q) a.vel_out[q][dest] = v[r][q];
                 }
                 stay_next += (unsigned)__popc(stay);
-                __syncwarp();
-                if (mover && lane == __ffs(peers) - 1) base_w[warp][cls] += __popc(peers);
-                __syncwarp();
+                const bool mover = cls >= 0 && cls != STAY;
+                if (__any_sync(full, mover)) {
+                    const unsigned peers = __match_any_sync(full, cls);
+                    const unsigned gsize = (unsigned)__popc(peers), rank = (unsigned)__popc(peers & lt);
+                    // a group larger than the class's slots is written directly, after
+                    // whatever of its class is staged; otherwise flush when it would not fit
+                    const bool direct = gsize > (unsigned)MS;
+                    if (__any_sync(full, mover && (direct ? fill_w[warp][cls] > 0u
+                                                          : fill_w[warp][cls] + gsize > (unsigned)MS)))
+                        flush();
+                    if (mover) {
+                        if (direct) {
+                            const unsigned dest = base_w[warp][cls] + rank;   // nothing of the class staged
+#pragma unroll
+                            for (int d = 0; d < D; ++d) a.off_out[d][dest] = f[r][d];
+#pragma unroll
+                            for (int q = 0; q < 3; ++q) a.vel_out[q][dest] = v[r][q];
+                        } else {
+                            const int slot = (cls < STAY ? cls : cls - 1) * MS + (int)(fill_w[warp][cls] + rank);
+#pragma unroll
+                            for (int d = 0; d < D; ++d) stage[warp][d][slot] = f[r][d];
+#pragma unroll
+                            for (int q = 0; q < 3; ++q) stage[warp][D + q][slot] = v[r][q];
+                        }
+                    }
+                    __syncwarp();
+                    if (mover && lane == __ffs(peers) - 1) {
+                        if (direct) base_w[warp][cls] += gsize;
+                        else fill_w[warp][cls] += gsize;
+                    }
+                    __syncwarp();
+                }
             }
         }
+        flush();
     }
 }
 

@@ -14,6 +14,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "fastdiv.cuh"
+
 namespace psum_b200 {
 
 void count_launch();   // registry.cpp: process-wide kernel launch counter
@@ -30,26 +32,6 @@ constexpr unsigned kErrKeyRange = 1u << 8;    // internal key out of range
 // using multiplication", PLDI 1994, Fig. 4.1): for l = ceil(log2 d) and
 // m = floor(2^32 (2^l - d) / d) + 1, q = (t + ((n - t) >> 1)) >> (l - 1)
 // with t = mulhi(m, n), exact for every 32-bit n.
-struct FastDiv {
-    unsigned d, m;
-    int l;
-};
-
-inline FastDiv make_fastdiv(unsigned d) {
-    FastDiv f{d, 0u, 0};
-    int l = 0;
-    while ((1ull << l) < d) ++l;
-    f.l = l;
-    f.m = d <= 1 ? 0u : (unsigned)((((1ull << l) - d) << 32) / d + 1);
-    return f;
-}
-
-__device__ __forceinline__ unsigned fastdiv(unsigned n, const FastDiv& f) {
-    if (f.d == 1) return n;
-    const unsigned t = __umulhi(f.m, n);
-    return (t + ((n - t) >> 1)) >> (f.l - 1);
-}
-
 struct GridView {
     int dim;
     int cells[3];     // PSuM cell counts (axis >= dim: 1)

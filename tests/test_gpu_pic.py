@@ -372,11 +372,12 @@ def test_load_device_buffers_reusable_immediately():
     assert np.abs(got_vel - vel.astype(np.float32)).max() == 0.0
 
 
-def _fused_vs_general(kind, pusher, dt, seed, vscale=1.0, species=2, sort_general=False, cluster=None):
+def _fused_vs_general(kind, pusher, dt, seed, vscale=1.0, species=2, sort_general=False, cluster=None, drift=None):
     """Runs one step on the same sorted state with the fused sorted step
     (sort_interval 1) and with the general path (push in place; with
     sort_general, followed by the stable radix sort); returns both results.
-    cluster = (centre, sigma) draws the positions from a Gaussian blob."""
+    cluster = (centre, sigma) draws the positions from a Gaussian blob; drift
+    (per-axis) is added to every velocity."""
     out = []
     for interval in (1, 0):
         ctx, g, pos, vel, phi = make_case(kind, P.MIXED, seed=seed, n=40000)
@@ -385,6 +386,10 @@ def _fused_vs_general(kind, pusher, dt, seed, vscale=1.0, species=2, sort_genera
             centre, sigma = cluster
             pos = np.stack([rng_c.normal(centre[a], sigma, pos.shape[1]) for a in range(g.dim)])
         pos = wrap_into(pos, g)
+        if drift is not None:
+            vel = vel.copy()
+            for a_, d_ in enumerate(drift):
+                vel[a_] += d_
         ctx.set_options(f"sort_interval {interval}")
         sps = []
         rng = np.random.default_rng(seed + 1)
@@ -482,6 +487,23 @@ def test_fused_step_clustered_cells(kind):
     assert cnt_f == cnt_g
     for (pf, vf, kf, df), (pg, vg, kg, dg) in zip(fused, gen):
         assert np.bincount(kf).max() > 4096
+        assert (kf == kg).all()
+        assert (pf.view(np.int64) == pg.view(np.int64)).all()
+        assert (vf.view(np.int64) == vg.view(np.int64)).all()
+        assert (df.view(np.int64) == dg.view(np.int64)).all()
+
+
+@pytest.mark.parametrize("kind", ["2d_periodic", "3d_periodic", "2d_absorb"])
+def test_fused_step_drifting_beam(kind):
+    # a drifting beam: about half of the particles cross one cell along x in
+    # the same direction, so many movers of one class share a round (large
+    # groups, staging overflow, direct writes)
+    drift = (4.0, 0.0) if kind.startswith("2d") else (4.0, 0.0, 0.0)
+    (fused, loss_f, cnt_f), (gen, loss_g, cnt_g) = _fused_vs_general(kind, P.LEAPFROG, 0.12, seed=35, vscale=0.3,
+                                                                      sort_general=True, drift=drift)
+    assert (loss_f == loss_g).all()
+    assert cnt_f == cnt_g
+    for (pf, vf, kf, df), (pg, vg, kg, dg) in zip(fused, gen):
         assert (kf == kg).all()
         assert (pf.view(np.int64) == pg.view(np.int64)).all()
         assert (vf.view(np.int64) == vg.view(np.int64)).all()

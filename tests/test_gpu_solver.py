@@ -239,3 +239,4 @@ def test_graph_replay_matches_direct_launches(kind):
     for a, bb in zip(outs[1], outs[0]):
         assert (a.view(np.int64) == bb.view(np.int64)).all()
     assert launches[1] == launches[0]
+
