@@ -28,6 +28,10 @@ void count_launch();
 void add_launches(unsigned long long n);
 void uncount_launches(unsigned long long n);
 unsigned long long thread_launches();   // launches counted by the calling thread
+// Pinned, device-mapped counter that kernels add to when they start work
+// whose launch count the host cannot know in advance (the iterations of a
+// conditional graph loop); psum_kernel_launches includes it.
+unsigned long long* device_launch_counter();
 
 inline void cuda_check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw Error(PSUM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));

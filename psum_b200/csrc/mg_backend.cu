@@ -187,12 +187,15 @@ struct SolverBase {
 
     virtual ~SolverBase() {
         drop_graph();
+        if (aux_stream) cudaStreamDestroy(aux_stream);
         if (own_stream) cudaStreamDestroy(own_stream);
     }
     void drop_graph() {
         if (graph.exec) cudaGraphExecDestroy(graph.exec);
         graph.exec = nullptr;
     }
+    cudaStream_t aux_stream = nullptr;      // captures the body of a conditional loop
+    unsigned long long loop_kernels = 0;    // kernels captured into loop bodies (counted on the device)
     virtual void build_device(cudaStream_t s) = 0;
     virtual void enqueue_solve(double* b, double* x, cudaStream_t s) = 0;
 };
@@ -300,6 +303,60 @@ struct Solver : SolverBase {
         return xcur[0];
     }
 
+    // [residual, check] then WHILE(check says continue) { V-cycles, correct,
+    // residual, check } (sycl_multigrid32f_gpu.cpp:137-157 with the loop kept
+    // on the device).  The body's check adds the body's kernel count to the
+    // mapped launch counter each time the body runs.
+    void enqueue_refinement_loop(double* b, double* x, cudaStream_t s) {
+        MGState* st = state.p;
+        Level<T>& F = *lv[0];
+        const long long n = (long long)n_row;
+        const int ci = correction_interval;
+        if (!aux_stream) throw Error(PSUM_ERR_INTERNAL, "multigrid: loop stream missing");
+        unsigned long long* counter = device_launch_counter();   // created by set_matrix
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t g = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        cuda_check(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd), "cudaStreamGetCaptureInfo");
+        cudaGraphConditionalHandle h;
+        cuda_check(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault), "conditional handle");
+        launch_residual64<T>(a0.view, x, b, dinv0.p, F.b.p, partials.p, st, 1, s);
+        { k_check_loop<<<1, 32, 0, s>>>(partials.p, kNormBlocks, st, 0, max_cycles, tol, h, 0ull, counter); count_launch(); }
+        cuda_check(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd), "cudaStreamGetCaptureInfo");
+        cudaGraphNodeParams np{};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t loop;
+        cuda_check(cudaGraphAddNode(&loop, g, deps, nd, &np), "add conditional node");
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        cuda_check(cudaStreamUpdateCaptureDependencies(s, &loop, 1, cudaStreamSetCaptureDependencies),
+                   "update capture dependencies");
+        cuda_check(cudaStreamBeginCaptureToGraph(aux_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal),
+                   "capture loop body");
+        const unsigned long long k0 = thread_launches();
+        unsigned long long body_kernels = 0;
+        try {
+            T* e = enqueue_vcycles(F.bufA.p, F.bufB.p, F.b.p, ci, /*x_is_zero=*/true, aux_stream);
+            { k_correct<T><<<grid_for(n), kThreads, 0, aux_stream>>>(x, e, n, st); count_launch(); }
+            launch_residual64<T>(a0.view, x, b, dinv0.p, F.b.p, partials.p, st, 1, aux_stream);
+            body_kernels = thread_launches() - k0 + 1;
+            { k_check_loop<<<1, 32, 0, aux_stream>>>(partials.p, kNormBlocks, st, ci, max_cycles, tol, h,
+                                                     body_kernels, counter); count_launch(); }
+            cuda_check(cudaGetLastError(), "loop body launch");
+        } catch (...) {
+            cudaGraph_t tmp = nullptr;
+            cudaStreamEndCapture(aux_stream, &tmp);
+            uncount_launches(thread_launches() - k0);
+            throw;
+        }
+        cuda_check(cudaStreamEndCapture(aux_stream, &body), "end loop body capture");
+        uncount_launches(body_kernels);   // counted by the body's check, once per iteration run
+        loop_kernels += body_kernels;
+    }
+
     void enqueue_sources(double* b, cudaStream_t s) {
         const long long na = (long long)add_idx.size(), nr = (long long)rep_idx.size();
         if (na > 0) { k_addback<<<grid_for(na), kThreads, 0, s>>>(b, d_add_idx.p, d_add_val.p, na); count_launch(); }
@@ -314,7 +371,17 @@ struct Solver : SolverBase {
         { k_check<<<1, 32, 0, s>>>(partials.p, kNormBlocks, st, 0, tol, 0, 0); count_launch(); }
         Level<T>& F = *lv[0];
         int cycles_done = 0, refinements = 0;
-        if (precision == 32) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cuda_check(cudaStreamIsCapturing(s, &cs), "cudaStreamIsCapturing");
+        if (precision == 32 && cs == cudaStreamCaptureStatusActive && tol > 0 && max_cycles > 0 &&
+            max_cycles % correction_interval == 0) {
+            // captured into a graph: the refinements run as a conditional loop
+            // that ends on the device once the residual test passes, so no
+            // kernel of the cycles after convergence is launched
+            enqueue_refinement_loop(b, x, s);
+            cycles_done = max_cycles;
+            refinements = max_cycles / correction_interval;
+        } else if (precision == 32) {
             // FP64 refinement around FP32 V-cycles (sycl_multigrid32f_gpu.cpp:137-157)
             while (cycles_done < max_cycles) {
                 const int batch = std::min(correction_interval, max_cycles - cycles_done);
@@ -422,6 +489,10 @@ void solver_set_matrix(SolverBase* s, unsigned long long n_row, unsigned long lo
     s->host = build_hierarchy(A, s->I, s->J, s->K, s->depth, s->max_coarse, s->periodic);
     s->n_row = n_row;
     ensure_stream(s);
+    // created here, outside any stream capture: the stream that captures the
+    // body of the conditional refinement loop, and the mapped launch counter
+    if (!s->aux_stream) cuda_check(cudaStreamCreateWithFlags(&s->aux_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    device_launch_counter();
     s->version++;
     s->drop_graph();
     s->build_device(s->own_stream);
@@ -451,6 +522,7 @@ static bool capturable(cudaStream_t st) {
 static void capture_solve(SolverBase* s, double* b, double* x, cudaStream_t st) {
     s->drop_graph();
     const unsigned long long k0 = thread_launches();
+    s->loop_kernels = 0;
     cuda_check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
     cudaGraph_t g = nullptr;
     try {
@@ -458,11 +530,11 @@ static void capture_solve(SolverBase* s, double* b, double* x, cudaStream_t st) 
     } catch (...) {
         cudaStreamEndCapture(st, &g);
         if (g) cudaGraphDestroy(g);
-        uncount_launches(thread_launches() - k0);
+        uncount_launches(thread_launches() - k0 - s->loop_kernels);
         throw;
     }
     cuda_check(cudaStreamEndCapture(st, &g), "cudaStreamEndCapture");
-    const unsigned long long kernels = thread_launches() - k0;
+    const unsigned long long kernels = thread_launches() - k0 - s->loop_kernels;   // outside loop bodies
     uncount_launches(kernels);   // counted again at every replay
     const cudaError_t e = cudaGraphInstantiate(&s->graph.exec, g, 0);
     cudaGraphDestroy(g);

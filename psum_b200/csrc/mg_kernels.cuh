@@ -31,6 +31,8 @@ struct MGState {
     int cycles;             // V-cycles run before `done` was raised / in total
     int refinements;        // refinement steps run
     int status;             // psum_status of the solve
+    int cycles_run;         // device-side counts of a solve looping in a graph
+    int refinements_run;
 };
 
 template <class T>
@@ -323,6 +325,56 @@ __global__ void k_replace(double* __restrict__ b, const unsigned long long* __re
     if (i < n) b[idx[i]] = v[i];
 }
 
+// Convergence test on ||r||^2 = s between refinements.
+__device__ __forceinline__ void check_update(MGState* st, double s, double tol, int cycles, int refinements) {
+    if (st->done) return;
+    if (st->rnorm2_first < 0) st->rnorm2_first = s;
+    st->rnorm2_last = s;
+    st->cycles = cycles;
+    st->refinements = refinements;
+    const double bn = st->bnorm2 > 0 ? st->bnorm2 : 1.0;
+    if (!(s == s) || s > 1e300 || (st->rnorm2_first > 0 && s > 1e12 * st->rnorm2_first)) {
+        st->status = PSUM_ERR_DIVERGED;
+        st->done = 1;
+    } else if (tol > 0 && s <= tol * tol * bn) {
+        st->done = 1;
+    }
+}
+
+// Fixed-order two-level sum of the per-block partials (valid in thread 0).
+__device__ __forceinline__ double sum_partials(const double* __restrict__ partials, int nparts) {
+    __shared__ double sh[32];
+    double v = 0.0;
+    if (threadIdx.x < 32) {
+        for (int q = threadIdx.x; q < nparts; q += 32) v += partials[q];
+        sh[threadIdx.x] = v;
+    }
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 32; ++q) s += sh[q];
+    return s;
+}
+
+// Check of a solve that loops in a CUDA graph: counts the `batch` cycles just
+// run, applies the convergence test, and sets the loop condition (continue
+// while not done and below max_cycles).  Each continuation adds the loop
+// body's kernel count to the mapped launch counter.
+__global__ void k_check_loop(const double* __restrict__ partials, int nparts, MGState* st, int batch,
+                             int max_cycles, double tol, cudaGraphConditionalHandle loop,
+                             unsigned long long body_kernels, unsigned long long* launch_counter) {
+    const double s = sum_partials(partials, nparts);
+    if (threadIdx.x != 0) return;
+    if (batch > 0) {
+        st->cycles_run += batch;
+        st->refinements_run += 1;
+    }
+    check_update(st, s, tol, st->cycles_run, st->refinements_run);
+    const bool more = !st->done && st->cycles_run < max_cycles;
+    if (more) atomicAdd_system(launch_counter, body_kernels);
+    cudaGraphSetConditional(loop, more ? 1u : 0u);
+}
+
 // Single-block state update. phase 0: start of solve (partials hold ||b||^2);
 // phase 1: convergence check (partials hold ||r||^2); phase 2: final residual.
 __global__ void k_check(const double* __restrict__ partials, int nparts, MGState* st, int phase, double tol,
@@ -346,21 +398,12 @@ __global__ void k_check(const double* __restrict__ partials, int nparts, MGState
         st->cycles = 0;
         st->refinements = 0;
         st->status = 0;
+        st->cycles_run = 0;
+        st->refinements_run = 0;
         return;
     }
     if (phase == 1) {
-        if (st->done) return;
-        if (st->rnorm2_first < 0) st->rnorm2_first = s;
-        st->rnorm2_last = s;
-        st->cycles = cycles;
-        st->refinements = refinements;
-        const double bn = st->bnorm2 > 0 ? st->bnorm2 : 1.0;
-        if (!(s == s) || s > 1e300 || (st->rnorm2_first > 0 && s > 1e12 * st->rnorm2_first)) {
-            st->status = PSUM_ERR_DIVERGED;
-            st->done = 1;
-        } else if (tol > 0 && s <= tol * tol * bn) {
-            st->done = 1;
-        }
+        check_update(st, s, tol, cycles, refinements);
         return;
     }
     // phase 2: final

@@ -26,7 +26,20 @@ std::mutex& registry_mutex() {
 thread_local std::string g_last_error;
 std::atomic<unsigned long long> g_launches{0};
 thread_local unsigned long long g_thread_launches = 0;
+std::once_flag g_mapped_once;
+unsigned long long* g_mapped = nullptr;   // pinned host word, device-mapped
 }  // namespace
+
+unsigned long long* device_launch_counter() {
+    std::call_once(g_mapped_once, [] {
+        void* p = nullptr;
+        cuda_check(cudaHostAlloc(&p, sizeof(unsigned long long), cudaHostAllocMapped | cudaHostAllocPortable),
+                   "cudaHostAlloc launch counter");
+        *static_cast<volatile unsigned long long*>(p) = 0ull;
+        g_mapped = static_cast<unsigned long long*>(p);
+    });
+    return g_mapped;
+}
 
 void count_launch() {
     g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -62,6 +75,9 @@ EXPORT struct func_table get_solver_funcs(const char* name) {
 
 EXPORT const char* psum_last_error(void) { return psum_b200::last_error().c_str(); }
 
-EXPORT unsigned long long psum_kernel_launches(void) { return psum_b200::g_launches.load(); }
+EXPORT unsigned long long psum_kernel_launches(void) {
+    const volatile unsigned long long* m = psum_b200::g_mapped;
+    return psum_b200::g_launches.load() + (m ? *m : 0ull);
+}
 
 }

@@ -209,34 +209,40 @@ def test_repeat_solves_bitwise_identical():
 
 @pytest.mark.parametrize("kind", ["cuda_multigrid32f_gpu", "cuda_multigrid64_gpu"])
 def test_graph_replay_matches_direct_launches(kind):
-    # the solve is captured once into a CUDA graph and replayed; results and
-    # kernel counts equal the directly launched solve, and a changed option,
-    # source or buffer is picked up
+    # the solve is captured once into a CUDA graph and replayed (the mixed
+    # backend's refinements as a device-side conditional loop); iterates and
+    # statistics equal the directly launched solve, a changed option, source
+    # or buffer is picked up, and the graph never launches more kernels
     g, fixed, r, c, v, n, b = dirichlet_case(64, seed=3)
     opts = "I 65 J 65 depth 4 pre_relax 2 post_relax 2 max_cycles 12 correction_interval 2 tol 1e-9"
-    solvers = []
+    outs, launches, stats, codes = {0: [], 1: []}, {0: [], 1: []}, {0: [], 1: []}, {0: [], 1: []}
     for graph in (1, 0):
         s = P.solver_backend(kind)
         s.set_options(opts + f" graph {graph}")
         s.set_matrix(n, n, r.size, r, c, v)
-        solvers.append(s)
-    outs = {0: [], 1: []}
-    launches = {0: [], 1: []}
-    for graph, s in zip((1, 0), solvers):
         bd, xd = dev(b), dev(np.zeros(n))
-        for step in range(4):
+        for step in range(6):
             if step == 2:
                 s.set_options(opts.replace("tol 1e-9", "tol 1e-7") + f" graph {graph}")
                 s.set_source_addback(np.array([5], np.uint64), np.array([0.25]))
+            if step == 4:   # cannot converge: loop ends on max_cycles
+                s.set_options(opts.replace("max_cycles 12", "max_cycles 2").replace("tol 1e-9", "tol 1e-14")
+                              + f" graph {graph}")
             bd.copy_(dev(b + 0.01 * step))
             k0 = P.lib().psum_kernel_launches()
-            s.solve(bd, xd)
+            codes[graph].append(s.solve(bd, xd))
             launches[graph].append(P.lib().psum_kernel_launches() - k0)
+            stats[graph].append(s.last_stats())
             outs[graph].append(xd.cpu().numpy().copy())
         xd2 = dev(np.zeros(n))   # new output buffer: recaptured
         s.solve(bd, xd2)
         outs[graph].append(xd2.cpu().numpy().copy())
     for a, bb in zip(outs[1], outs[0]):
         assert (a.view(np.int64) == bb.view(np.int64)).all()
-    assert launches[1] == launches[0]
-
+    assert stats[1] == stats[0]
+    assert codes[1] == codes[0] and codes[0][4] == 4 and codes[0][0] == 0
+    assert all(l1 <= l0 for l1, l0 in zip(launches[1], launches[0]))
+    if kind == "cuda_multigrid64_gpu":
+        assert launches[1] == launches[0]
+    else:
+        assert sum(launches[1]) < sum(launches[0])   # converged cycles are not launched
