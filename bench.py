@@ -40,6 +40,8 @@ SEED = 20261203 + 2
 MG_OPTIONS = (f"I {CELLS + 1} J {CELLS + 1} K 1 depth 5 pre_relax 2 post_relax 2 max_cycles 16 "
               f"correction_interval 2 tol 1e-8")
 BYTES_PER_PARTICLE = 24          # int32 cell + 2 FP32 offsets + 3 FP32 velocities (2D3V mixed)
+COMPARE_STEPS = 3                # steps from the common initial state before the mixed/FP64 field comparison
+FP64_SORT_INTERVAL = 10
 
 
 def parse():
@@ -53,7 +55,10 @@ def parse():
     ap.add_argument("--sort-interval", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 GPU run and the field comparison")
     ap.add_argument("--cpu-sample", type=int, default=1 << 21, help="particles in the CPU baseline sample")
+    ap.add_argument("--mg-extra", default="", help="extra multigrid options (e.g. 'graph 0' to launch the solve's "
+                    "kernels one by one, which profilers need)")
     return ap.parse_args()
 
 
@@ -123,35 +128,81 @@ def make_species_device(torch, gen, n, cells, vth, device):
     return pos, vel
 
 
-def mg_options(cells):
-    return MG_OPTIONS.replace(f"I {CELLS + 1} J {CELLS + 1}", f"I {cells + 1} J {cells + 1}")
+def mg_options(cells, extra=""):
+    opts = MG_OPTIONS.replace(f"I {CELLS + 1} J {CELLS + 1}", f"I {cells + 1} J {cells + 1}")
+    return f"{opts} {extra}".strip()
 
 
-def build_problem(torch, P, cells, ppc, seed, device, sort_interval):
-    """Context + solver for the bounded two-species plasma; particles are
-    returned (device FP64 SoA) but not loaded."""
+def build_problem(torch, P, cells, ppc, seed, device, sort_interval, mg_extra="", precision=None,
+                  backend="cuda_multigrid32f_gpu"):
+    """Context + solver for the bounded two-species plasma (particles are
+    loaded by the caller)."""
     n = cells * cells * ppc
     w = 1.0 / ppc
-    ctx = P.ParticleContext((cells, cells), (0.0, 0.0), (float(cells), float(cells)), (0, 0), P.MIXED)
+    ctx = P.ParticleContext((cells, cells), (0.0, 0.0), (float(cells), float(cells)), (0, 0),
+                            P.MIXED if precision is None else precision)
     ctx.set_options(f"sort_interval {sort_interval}")
     e = ctx.add_species(-1.0, 1.0, w, n)
     i = ctx.add_species(1.0, MASS_RATIO, w, n)
     grid = P.simple_grid((0.0, 0.0), (float(cells), float(cells)), (cells, cells))
     ps = P.Poisson_solver_2d()
-    opts = mg_options(cells)
+    opts = mg_options(cells, mg_extra)
     ps.set_options(opts)
-    ps.init("cuda_multigrid32f_gpu", grid, P.Poisson_solver_2d.Cartesian,
+    ps.init(backend, grid, P.Poisson_solver_2d.Cartesian,
             [P.Dirichlet_line(grid, d, 0.0) for d in "NSEW"], 1.0)
     ps.make_righthand_item()
     return ctx, (e, i), ps, n, w
 
 
 def roofline_block(push_ms_per_step, n_total, peak, peak_kind, traffic):
+    """Roofline of the dominant work: the fused sorted step of both species
+    (gather + push + boundary + deposit + stable re-sort), whose algorithmic
+    bytes are one read and one write of every particle's state (2 x 24 B)."""
     algo = n_total * 2 * BYTES_PER_PARTICLE
     achieved = algo / (push_ms_per_step * 1e-3) / 1e9
-    return {"bound": "hbm", "kernel": "k_push_mixed (gather+push+boundary+deposit, both species)",
+    return {"bound": "hbm",
+            "kernel": "fused sorted step: k_cls_pass1 + k_cls_offsets + scan + k_cls_pass2, both species",
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-            "peak_kind": peak_kind, "algorithmic_bytes_per_step": algo, "traffic": traffic}
+            "peak_kind": peak_kind, "algorithmic_bytes_per_step": algo,
+            "traffic": None if traffic is None else int(traffic * n_total)}
+
+
+def step_algorithmic_bytes(n_total, cells, cycles, refinements, pre=2, post=2):
+    """B_step = N_p * 2 S_p + B_grid with B_grid = N_nodes (b_phi + b_rho)
+    + n_VC c_d N_nodes (pre + post + 3) 3 b_f + n_ref N_nodes (2*8 + 4):
+    compulsory traffic of the particle state, the FP64 fields, the FP32
+    V-cycles (c_d = 4/3, the 2-D level sum) and the FP64 refinements."""
+    nodes = (cells + 1) ** 2
+    grid = nodes * 16 + cycles * (4.0 / 3.0) * nodes * (pre + post + 3) * 3 * 4 + refinements * nodes * 20
+    return n_total * 2 * BYTES_PER_PARTICLE + int(grid)
+
+
+def measured_traffic_per_particle():
+    """DRAM bytes (read + write) per particle of the fused sorted step from
+    the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "fused_step_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        for line in f:
+            if line.startswith("bytes_per_particle:"):
+                return float(line.split(":", 1)[1])
+    return None
+
+
+def step_roofline(n_total, cells, stats, ms_per_step, peak):
+    b = step_algorithmic_bytes(n_total, cells, stats["cycles"], stats["refinements"])
+    achieved = b / (ms_per_step * 1e-3) / 1e9
+    return {"algorithmic_bytes": b, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4)}
+
+
+def workload_config(args, world=1):
+    return {"workload": "2D bounded two-species plasma, mixed precision",
+            "grid_cells": [args.cells, args.cells], "particles": 2 * args.cells * args.cells * args.ppc,
+            "ppc_per_species": args.ppc, "mass_ratio": MASS_RATIO, "dt": DT, "mg": mg_options(args.cells, args.mg_extra),
+            "sort_interval": args.sort_interval, "parallelism": "replicas" if world > 1 else "single GPU",
+            "l2_policy": "inputs larger than L2 (state 12.9 GB)"}
 
 
 # ------------------------------------------------------------ CPU baseline --
@@ -212,24 +263,30 @@ def run_ours(args, rank, world, dist):
     gen = torch.Generator(device=dev)
     gen.manual_seed(SEED + 1000 * rank)
 
-    ctx, (e, i), ps, n, w = build_problem(torch, P, cells, ppc, SEED + rank, dev, args.sort_interval)
+    ctx, (e, i), ps, n, w = build_problem(torch, P, cells, ppc, SEED + rank, dev, args.sort_interval, args.mg_extra)
     ctx.set_stream(stream)
     nn = (cells + 1) ** 2
     rho = torch.zeros(nn, dtype=torch.float64, device=dev)
     phi = torch.zeros(nn, dtype=torch.float64, device=dev)
     vth_i = 1.0 / np.sqrt(MASS_RATIO)
+    init = []   # the FP64 initial state, kept for the FP64 run
     for sp, vth in ((e, 1.0), (i, vth_i)):
         pos, vel = make_species_device(torch, gen, n, cells, vth, dev)
         ctx.load(sp, pos, vel)
-        del pos, vel
+        init.append((pos, vel))
     torch.cuda.synchronize()
-    torch.cuda.empty_cache()
     ctx.sort()
     ctx.deposit()
 
     def step():
         ctx.step(ps.backend, 0.0, rho, phi, DT)
 
+    # the first COMPARE_STEPS steps (untimed) give the fields compared with
+    # the FP64 run from the same initial state
+    for _ in range(COMPARE_STEPS):
+        step()
+    torch.cuda.synchronize()
+    rho_mixed, phi_mixed = rho.clone(), phi.clone()
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -264,6 +321,14 @@ def run_ours(args, rank, world, dist):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_max = float(t.item())
 
+    fp64 = None
+    if not args.no_fp64:
+        del ctx, ps
+        torch.cuda.empty_cache()
+        fp64 = run_fp64(args, torch, P, dev, init, rho_mixed, phi_mixed)
+    del init
+    torch.cuda.empty_cache()
+
     e2e = None
     if not args.no_e2e:
         e2e = run_e2e(args, torch, P, dev, rank, dist)
@@ -274,27 +339,21 @@ def run_ours(args, rank, world, dist):
     value = n_total * world * args.steps / (ms_max * 1e-3)
     peak, peak_kind = measured_peaks()
     push_ms = phases["push"][0] / max(phases["push"][1], 1)
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "push_traffic.json")
-    if os.path.exists(tpath):
-        with open(tpath) as f:
-            traffic = json.load(f).get("bytes_per_step")
+    traffic = measured_traffic_per_particle()
     line = {
         "metric": "particle-steps/s incl. Poisson MG, mixed-prec vs FP64 on GPU at stated error",
         "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 push / f32-in-f64 MG", "data": "synthetic",
-        "config": {"workload": "2D bounded two-species plasma, mixed precision",
-                   "grid_cells": [cells, cells], "particles": n_total, "ppc_per_species": ppc,
-                   "mass_ratio": MASS_RATIO, "dt": DT, "mg": mg_options(cells), "sort_interval": args.sort_interval,
-                   "parallelism": "replicas" if world > 1 else "single GPU",
-                   "l2_policy": "inputs larger than L2 (state 12.9 GB)"},
+        "config": workload_config(args, world),
         "roofline": roofline_block(push_ms, n_total, peak, peak_kind, traffic),
         "phase_ms_per_step": {k: round(v[0] / max(v[1], 1), 4) for k, v in phases.items()},
-        "step_roofline_frac": round((n_total * 2 * BYTES_PER_PARTICLE) / (ms_max / args.steps * 1e-3) / 1e9 / peak, 4),
+        "step_roofline": step_roofline(n_total, cells, stats, ms_max / args.steps, peak),
         "mg_last_solve": stats, "valid_particles_end": n_valid, "charge_end": diag["charge"],
         "gpu_launches": int(launches), "clocks": clocks,
     }
+    if fp64 is not None:
+        line["fp64_gpu"] = fp64
     if e2e is not None:
         line["e2e"] = e2e
     if not args.no_cpu_baseline:
@@ -302,6 +361,52 @@ def run_ours(args, rank, world, dist):
         cb.pop("t_step_full_s", None)
         line["cpu_baseline"] = cb
     return line
+
+
+def run_fp64(args, torch, P, dev, init, rho_mixed, phi_mixed):
+    """The same workload in FP64 on the GPU (FP64 particle state, FP64
+    multigrid V-cycles): throughput over K timed steps, and the relative field
+    error of the mixed run against it after COMPARE_STEPS steps from the same
+    initial state."""
+    cells, ppc = args.cells, args.ppc
+    ctx, (e, i), ps, n, w = build_problem(torch, P, cells, ppc, SEED, dev, FP64_SORT_INTERVAL, args.mg_extra,
+                                          precision=P.FP64, backend="cuda_multigrid64_gpu")
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream)
+    nn = (cells + 1) ** 2
+    rho = torch.zeros(nn, dtype=torch.float64, device=dev)
+    phi = torch.zeros(nn, dtype=torch.float64, device=dev)
+    for sp, (pos, vel) in zip((e, i), init):
+        ctx.load(sp, pos, vel)
+    torch.cuda.synchronize()
+    ctx.sort()
+    ctx.deposit()
+    for _ in range(COMPARE_STEPS):
+        ctx.step(ps.backend, 0.0, rho, phi, DT)
+    torch.cuda.synchronize()
+
+    def rel(a, b):
+        return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+
+    err = {"after_steps": COMPARE_STEPS, "phi_rel_l2": rel(phi_mixed, phi), "rho_rel_l2": rel(rho_mixed, rho),
+           "phi_rel_max": float((phi_mixed - phi).abs().max() / phi.abs().max())}
+    for _ in range(args.warmup):
+        ctx.step(ps.backend, 0.0, rho, phi, DT)
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        start.record(stream)
+        for _ in range(args.steps):
+            ctx.step(ps.backend, 0.0, rho, phi, DT)
+        stop.record(stream)
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(stop) / args.steps
+    del ctx, ps
+    torch.cuda.empty_cache()
+    return {"value": 2 * n * args.steps / (ms * args.steps * 1e-3), "unit": "particle-steps/s", "ms_per_step": ms,
+            "definition": f"FP64 particle state and FP64 V-cycles (cuda_multigrid64_gpu, same options), "
+                          f"in-place push with deposit, stable sort every {FP64_SORT_INTERVAL} steps",
+            "field_error_of_mixed": err}
 
 
 def run_e2e(args, torch, P, dev, rank, dist):
@@ -333,7 +438,7 @@ def run_e2e(args, torch, P, dev, rank, dist):
         del pos, vel
         host.append((hp, hv))
     torch.cuda.synchronize()
-    ctx, (e, i), ps, n, w = build_problem(torch, P, cells, ppc, SEED + rank, dev, args.sort_interval)
+    ctx, (e, i), ps, n, w = build_problem(torch, P, cells, ppc, SEED + rank, dev, args.sort_interval, args.mg_extra)
     nn = (cells + 1) ** 2
     rho = torch.zeros(nn, dtype=torch.float64, device=dev)
     phi = torch.zeros(nn, dtype=torch.float64, device=dev)
@@ -371,19 +476,20 @@ def run_reference(args, rank):
     if rank != 0:
         return None
     steps = max(args.steps, 1)
+    for _ in range(args.warmup):   # untimed samples
+        cpu_baseline(args.cells, args.ppc, args.cpu_sample)
     vals = []
     cb = None
-    for _ in range(min(steps, 3)):
+    for _ in range(steps):
         cb = cpu_baseline(args.cells, args.ppc, args.cpu_sample)
         vals.append(cb["value"])
     value = statistics.median(vals)
     return {"impl": "reference",
             "metric": "particle-steps/s incl. Poisson MG, mixed-prec vs FP64 on GPU at stated error",
-            "value": value, "unit": "particle-steps/s", "n_gpus": 1, "steps": len(vals), "warmup": 0,
+            "value": value, "unit": "particle-steps/s", "n_gpus": 1, "steps": len(vals), "warmup": args.warmup,
             "ms_per_step": 1e3 * (2 * args.cells * args.cells * args.ppc) / value, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "2D bounded two-species plasma, mixed precision",
-                       "grid_cells": [args.cells, args.cells], "particles": 2 * args.cells * args.cells * args.ppc},
+            "config": workload_config(args),
             "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cb["cores"], "kind": "port",
                              "sample": cb["sample"]},
             "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
