@@ -122,6 +122,28 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
+# ------------------------------------------------------------- replicas --
+def replica_seed(rank):
+    """Seed of one replica: replicas are independent runs of the workload."""
+    return SEED + 1000 * rank
+
+
+def max_over_ranks(value, dist, device):
+    """The largest of the ranks' values (all ranks take this collective)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(particles_per_rank, world, steps, ms_max):
+    """Whole-job particle-steps/s: all ranks' particle-steps over the slowest
+    rank's time."""
+    return particles_per_rank * world * steps / (ms_max * 1e-3)
+
+
 def make_species_device(torch, gen, n, cells, vth, device):
     pos = torch.rand((2, n), generator=gen, device=device, dtype=torch.float64) * cells
     vel = torch.randn((3, n), generator=gen, device=device, dtype=torch.float64) * vth
@@ -261,7 +283,7 @@ def run_ours(args, rank, world, dist):
     stream = torch.cuda.Stream()
     cells, ppc = args.cells, args.ppc
     gen = torch.Generator(device=dev)
-    gen.manual_seed(SEED + 1000 * rank)
+    gen.manual_seed(replica_seed(rank))
 
     ctx, (e, i), ps, n, w = build_problem(torch, P, cells, ppc, SEED + rank, dev, args.sort_interval, args.mg_extra)
     ctx.set_stream(stream)
@@ -315,11 +337,7 @@ def run_ours(args, rank, world, dist):
     diag = ctx.diagnostics(phi, 1.0)
     clocks = clk.summary()
 
-    ms_max = ms
-    if dist is not None:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, dist, dev)
 
     fp64 = None
     if not args.no_fp64:
@@ -336,7 +354,7 @@ def run_ours(args, rank, world, dist):
     if rank != 0:
         return None
     n_total = 2 * n
-    value = n_total * world * args.steps / (ms_max * 1e-3)
+    value = replica_value(n_total, world, args.steps, ms_max)
     peak, peak_kind = measured_peaks()
     push_ms = phases["push"][0] / max(phases["push"][1], 1)
     traffic = measured_traffic_per_particle()
@@ -457,16 +475,12 @@ def run_e2e(args, torch, P, dev, rank, dist):
         losses_total += int(ctx.losses(reset=True).sum())
     phi_host.copy_(phi)
     torch.cuda.synchronize()
-    sec = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([sec], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        sec = float(t.item())
+    sec = max_over_ranks(time.perf_counter() - t0, dist, dev)
     world = dist.get_world_size() if dist is not None else 1
     h2d = 2 * n * 5 * 8
     d2h = args.steps * 2 * 2 * 2 * 8 + nn * 8
     del ctx, ps, host
-    return {"value": 2 * n * world * args.steps / sec, "unit": "particle-steps/s",
+    return {"value": replica_value(2 * n, world, args.steps, sec * 1e3), "unit": "particle-steps/s",
             "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps,
             "wall_s": sec, "definition": "whole job: H2D of the FP64 particle state, then K steps with a D2H "
                                          "of the loss counters after each, then D2H of phi"}
@@ -509,7 +523,7 @@ def main():
         import torch.distributed as tdist
         if args.impl == "ours":
             torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", rank)))
-            tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
             dist = tdist
     if args.impl == "reference":
         line = run_reference(args, rank)
