@@ -39,7 +39,7 @@ def _rank_main(rank, world, port, out):
 
 def test_replicas_time_is_slowest_rank_and_value_counts_all_ranks():
     world = 2
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_rank_main, args=(world, _free_port(), out), nprocs=world, join=True)
         res = dict(out)
