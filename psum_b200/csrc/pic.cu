@@ -129,7 +129,7 @@ __device__ __forceinline__ void load_cell_field(const PushArgs& a, int c0, int c
 
 template <int D>
 __device__ __forceinline__ void interp_grad(const CellField<D>& F, const float f[3], float G[3]) {
-#define PSUM_LERP(a_, wa_, b_, wb_) __fadd_rn(__fmul_rn((a_), (wa_)), __fmul_rn((b_), (wb_)))
+#define PSUM_LERP(a_, wa_, b_, wb_) __fmaf_rn((b_), (wb_), __fmul_rn((a_), (wa_)))
     if (D == 2) {
         G[0] = PSUM_LERP(F.e[0], __fsub_rn(1.f, f[1]), F.e[1], f[1]);
         G[1] = PSUM_LERP(F.e[2], __fsub_rn(1.f, f[0]), F.e[3], f[0]);
@@ -147,14 +147,14 @@ __device__ __forceinline__ void interp_grad(const CellField<D>& F, const float f
 // cell units.  f holds the new in-cell offsets and dc the cell steps per axis
 // on exit (offset carry rule: an offset that rounds to 1.0f moves to the next
 // cell with offset 0).  Every operation is an explicit round-to-nearest
-// intrinsic (no contraction), so every kernel that calls this function moves
-// the same particle bit-identically.  False when the state became
-// non-finite (the error word is flagged).
+// intrinsic (fused multiply-adds where written), so every kernel that calls
+// this function moves the same particle bit-identically.  False when the
+// state became non-finite (the error word is flagged).
 template <int D, int PUSHER>
 __device__ __forceinline__ bool kick_move(const PushArgs& a, const float G[3], float f[3], float v[3], int dc[3]) {
     if (PUSHER == PSUM_PIC_LEAPFROG) {
 #pragma unroll
-        for (int d = 0; d < D; ++d) v[d] = __fsub_rn(v[d], __fmul_rn(a.kE[d], G[d]));   // v += (q/m) E dt, E = -dr G
+        for (int d = 0; d < D; ++d) v[d] = __fmaf_rn(-a.kE[d], G[d], v[d]);   // v += (q/m) E dt, E = -dr G
     } else {
         float E[3] = {0.f, 0.f, 0.f};
 #pragma unroll
@@ -177,13 +177,11 @@ __device__ __forceinline__ bool kick_move(const PushArgs& a, const float G[3], f
 #pragma unroll
         for (int q = 0; q < 3; ++q) v[q] = __fadd_rn(vp[q], __fmul_rn(E[q], a.qmdt_half));
     }
+    bool ok = true;
 #pragma unroll
     for (int d = 0; d < D; ++d) {
-        const float sd = __fadd_rn(f[d], __fmul_rn(v[d], a.dtdr[d]));
-        if (!(fabsf(sd) < 1.0e9f)) {
-            atomicOr(a.err, kErrNonFinite);
-            return false;
-        }
+        const float sd = __fmaf_rn(v[d], a.dtdr[d], f[d]);
+        ok = ok && fabsf(sd) < 1.0e9f;   // false for NaN and infinities too
         const float fl = floorf(sd);
         float nf = __fsub_rn(sd, fl);
         int step = (int)fl;
@@ -194,7 +192,8 @@ __device__ __forceinline__ bool kick_move(const PushArgs& a, const float G[3], f
         f[d] = nf;
         dc[d] = step;
     }
-    return true;
+    if (!ok) atomicOr(a.err, kErrNonFinite);
+    return ok;
 }
 
 // Wrap periodic axes and test absorbing ones after c += dc.  Returns the loss
