@@ -243,8 +243,8 @@ struct Solver : SolverBase {
     // Enqueue `cycles` V(pre,post) cycles on level-0 (x0 in/out, b0 = scaled rhs).
     // `x_is_zero`: the level-0 iterate starts at zero (first sweep simplified).
     // Returns the buffer holding the final level-0 iterate.
-    T* enqueue_vcycles(T* x0, T* other0, T* b0, int cycles, bool x_is_zero, cudaStream_t s) {
-        const MGState* st = state.p;
+    T* enqueue_vcycles(T* x0, T* other0, T* b0, int cycles, bool x_is_zero, cudaStream_t s, bool gated = true) {
+        const MGState* st = gated ? state.p : nullptr;
         const T omega = T(2.0 / 3);
         const int L = host.L;
         std::vector<T*> xcur(L + 1), xoth(L + 1), bl(L + 1);
@@ -339,9 +339,10 @@ struct Solver : SolverBase {
         const unsigned long long k0 = thread_launches();
         unsigned long long body_kernels = 0;
         try {
-            T* e = enqueue_vcycles(F.bufA.p, F.bufB.p, F.b.p, ci, /*x_is_zero=*/true, aux_stream);
-            { k_correct<T><<<grid_for(n), kThreads, 0, aux_stream>>>(x, e, n, st); count_launch(); }
-            launch_residual64<T>(a0.view, x, b, dinv0.p, F.b.p, partials.p, st, 1, aux_stream);
+            // inside the loop the solve is never done: the kernels skip the flag
+            T* e = enqueue_vcycles(F.bufA.p, F.bufB.p, F.b.p, ci, /*x_is_zero=*/true, aux_stream, /*gated=*/false);
+            { k_correct<T><<<grid_for(n), kThreads, 0, aux_stream>>>(x, e, n, nullptr); count_launch(); }
+            launch_residual64<T>(a0.view, x, b, dinv0.p, F.b.p, partials.p, nullptr, 0, aux_stream);
             body_kernels = thread_launches() - k0 + 1;
             { k_check_loop<<<1, 32, 0, aux_stream>>>(partials.p, kNormBlocks, st, ci, max_cycles, tol, h,
                                                      body_kernels, counter); count_launch(); }

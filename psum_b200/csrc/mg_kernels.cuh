@@ -9,7 +9,8 @@
 // precomputed linear offsets, and the exception-row test runs beside the
 // stencil loads instead of before them.  Kernels in the V-cycle return
 // immediately once the solve's device-side `done` flag is set, so a fixed
-// launch schedule can stop early without a host round trip.
+// launch schedule can stop early without a host round trip; kernels in the
+// body of the device-side refinement loop get no flag and skip that load.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -139,7 +140,7 @@ template <class T, int Mode, int NS>
 __global__ void __launch_bounds__(kThreads) k_level_op(StencilDev<T> A, const T* __restrict__ x,
                                                        const T* __restrict__ b, T* __restrict__ out, T omega,
                                                        const MGState* __restrict__ st) {
-    if (st->done) return;
+    if (st && st->done) return;   // st == nullptr: ungated (inside the device-side loop)
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= A.n) return;
     level_row<T, Mode, NS, true>(A, x, b, out, omega, r);
@@ -183,7 +184,7 @@ template <class T>
 __global__ void __launch_bounds__(kThreads) k_restrict(XferDev<T> X, const T* __restrict__ rf, T* __restrict__ bc,
                                                        T* __restrict__ xc, const T* __restrict__ dinv_c,
                                                        const MGState* __restrict__ st) {
-    if (st->done) return;
+    if (st && st->done) return;   // st == nullptr: ungated (inside the device-side loop)
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= X.ax[0].nc * X.ax[1].nc * X.ax[2].nc) return;
     restrict_row<T, true>(X, rf, bc, xc, dinv_c, c);
@@ -224,7 +225,7 @@ __device__ __forceinline__ void prolong_row(const XferDev<T>& X, const T* __rest
 template <class T>
 __global__ void __launch_bounds__(kThreads) k_prolong_add(XferDev<T> X, const T* __restrict__ xc, T* __restrict__ xf,
                                                           const MGState* __restrict__ st) {
-    if (st->done) return;
+    if (st && st->done) return;   // st == nullptr: ungated (inside the device-side loop)
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= X.ax[0].nf * X.ax[1].nf * X.ax[2].nf) return;
     prolong_row<T, true>(X, xc, xf, f);
@@ -244,7 +245,7 @@ __device__ __forceinline__ T dense_row(const T* __restrict__ Ainv, const T* __re
 template <class T>
 __global__ void __launch_bounds__(kThreads) k_dense_mv(const T* __restrict__ Ainv, const T* __restrict__ b,
                                                        T* __restrict__ x, int n, const MGState* __restrict__ st) {
-    if (st->done) return;
+    if (st && st->done) return;   // st == nullptr: ungated (inside the device-side loop)
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= n) return;
@@ -275,7 +276,7 @@ __global__ void __launch_bounds__(kThreads) k_residual64(StencilDev<double> A, c
                                                          const double* __restrict__ b, const double* __restrict__ dinv,
                                                          TOut* __restrict__ bhat, double* __restrict__ partials,
                                                          const MGState* __restrict__ st, int gated) {
-    if (gated && st->done) return;
+    if (gated && st && st->done) return;
     double acc = 0.0;
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < A.n; r += gridDim.x * blockDim.x) {
         const double ax = stencil_row<double, double, NS>(A, x, r);
@@ -308,7 +309,7 @@ __global__ void __launch_bounds__(kThreads) k_scale(const double* __restrict__ b
 template <class T>
 __global__ void __launch_bounds__(kThreads) k_correct(double* __restrict__ x, const T* __restrict__ e, long long n,
                                                       const MGState* __restrict__ st) {
-    if (st->done) return;
+    if (st && st->done) return;   // st == nullptr: ungated (inside the device-side loop)
     const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (r < n) x[r] += (double)e[r];
 }
@@ -327,7 +328,7 @@ __global__ void k_replace(double* __restrict__ b, const unsigned long long* __re
 
 // Convergence test on ||r||^2 = s between refinements.
 __device__ __forceinline__ void check_update(MGState* st, double s, double tol, int cycles, int refinements) {
-    if (st->done) return;
+    if (st && st->done) return;   // st == nullptr: ungated (inside the device-side loop)
     if (st->rnorm2_first < 0) st->rnorm2_first = s;
     st->rnorm2_last = s;
     st->cycles = cycles;
