@@ -156,6 +156,32 @@ EXPORT int psum_pic_diagnostics(psum_pic_ctx* ctx, const double* phi_dev, double
  * psum_status code: non-finite state, overflow, key out of range); resets it. */
 EXPORT int psum_pic_device_errors(psum_pic_ctx* ctx, unsigned int* flags);
 
+/* ---- Differentiable runs (no counterpart in the reference: PSuM has no
+ * adjoint).  Device snapshots of a species' state for checkpoints, and the
+ * discrete adjoint of one leapfrog step on the current state.  Positions are
+ * in cell units (cell index + offset per axis), so lam_x is dL/ds. */
+
+/* Size of a snapshot of `species` (stored count + state arrays at capacity). */
+EXPORT int psum_pic_state_bytes(psum_pic_ctx* ctx, int species, unsigned long long* bytes);
+/* Copy the species' current state into / out of a device buffer of
+ * psum_pic_state_bytes bytes (stream-ordered device copies). */
+EXPORT int psum_pic_save_state(psum_pic_ctx* ctx, int species, void* dst_dev);
+EXPORT int psum_pic_restore_state(psum_pic_ctx* ctx, int species, const void* src_dev);
+
+/* Adjoint of the leapfrog kick and move of `species` at its current state
+ * (the state before the step), with the potential phi_dev the step gathered
+ * from.  lam_x_dev ([dim][n]) and lam_v_dev ([3][n]) hold the adjoints of the
+ * new positions and velocities on entry and of the old ones on exit (FP32
+ * for PSUM_PIC_MIXED contexts, FP64 otherwise; n = the loaded count); the
+ * deposit term is added by psum_pic_adjoint_deposit.  The adjoint of phi
+ * (the scatter of the force adjoint to the nodes) is added to mu_dev
+ * (FP64, one value per node) in exact fixed point. */
+EXPORT int psum_pic_adjoint_push(psum_pic_ctx* ctx, int species, const double* phi_dev, double dt, void* lam_x_dev,
+                                 void* lam_v_dev, double* mu_dev);
+/* lam_x += (dL/drho)^T d rho/ds for `species` at its current state, given
+ * nu_dev = dL/drho (FP64 per node): the gather of nu's CIC gradient. */
+EXPORT int psum_pic_adjoint_deposit(psum_pic_ctx* ctx, int species, const double* nu_dev, void* lam_x_dev);
+
 /* Allocation-free binning of caller-owned FP64 SoA device positions
  * (pos_dev[d*n+i]) on a grid: the same keys, per-cell counts, offsets,
  * stable permutation and in-grid count as psum_pic_bin, without a context

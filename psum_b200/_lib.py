@@ -82,6 +82,11 @@ PROTOTYPES = {
     "psum_pic_get_timing": (I, [P, P, P, I]),
     "psum_pic_diagnostics": (I, [P, P, D, P]),
     "psum_pic_device_errors": (I, [P, C.POINTER(C.c_uint)]),
+    "psum_pic_state_bytes": (I, [P, I, C.POINTER(ULL)]),
+    "psum_pic_save_state": (I, [P, I, P]),
+    "psum_pic_restore_state": (I, [P, I, P]),
+    "psum_pic_adjoint_push": (I, [P, I, P, D, P, P, P]),
+    "psum_pic_adjoint_deposit": (I, [P, I, P, P]),
     "psum_bin_positions_noalloc": (I, [C.POINTER(GridDesc), ULL, P, P, P, P, P, C.POINTER(ULL), P]),
 }
 

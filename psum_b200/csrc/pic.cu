@@ -1401,12 +1401,12 @@ constexpr int kDiagBlocks = 296;
 
 // ============================================================ host side ===
 
-static psum_pic_ctx* ctx_check(psum_pic_ctx* c) {
+psum_pic_ctx* ctx_check(psum_pic_ctx* c) {
     if (!c || c->magic != kPicMagic) throw Error(PSUM_ERR_INVALID_ARGUMENT, "not a particle context of this library");
     return c;
 }
 
-static Species& species_at(psum_pic_ctx* c, int s) {
+Species& species_at(psum_pic_ctx* c, int s) {
     if (s < 0 || s >= (int)c->sp.size()) throw Error(PSUM_ERR_INVALID_ARGUMENT, "species index out of range");
     return *c->sp[s];
 }
@@ -1457,7 +1457,7 @@ static void radix_sort(psum_pic_ctx* c, long long n, unsigned max_key, unsigned*
 
 // The fused sorted step leaves the keys implied by the cell offsets; every
 // reader of the keys calls this first.
-static void ensure_keys(psum_pic_ctx* c, Species& sp) {
+void ensure_keys(psum_pic_ctx* c, Species& sp) {
     if (!sp.keys_stale) return;
     const long long nc = c->g.n_cells;
     { k_fill_keys<<<blocks_for(nc * 32, 256), 256, 0, c->stream>>>(sp.starts[sp.starts_cur].p, nc, sp.key[sp.cur].p); count_launch(); }
@@ -1988,6 +1988,68 @@ EXPORT int psum_pic_get_state(psum_pic_ctx* ctx, int species, double* pos_host, 
         cuda_check(cudaMemcpyAsync(pos_host, dp.p, sizeof(double) * n * D, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
         cuda_check(cudaMemcpyAsync(vel_host, dv.p, sizeof(double) * n * 3, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
         cuda_check(cudaStreamSynchronize(ctx->stream), "get_state sync");
+    });
+}
+
+// Device snapshot of a species' state (checkpoints of differentiable runs):
+// stored count, then the arrays of the current buffer over the capacity.
+static size_t state_bytes(const psum_pic_ctx* c, const Species& sp) {
+    const size_t n = (size_t)sp.cap, D = (size_t)c->g.dim;
+    if (c->precision == PSUM_PIC_MIXED) return 8 + n * (4 + 4 * D + 4 * 3);
+    return 8 + n * (8 * D + 8 * 3 + 4);
+}
+
+static void state_copy(psum_pic_ctx* c, int species, char* base, bool save) {
+    Species& sp = species_at(c, species);
+    cudaStream_t s = c->stream;
+    const size_t n = (size_t)sp.cap;
+    const int D = c->g.dim, cur = sp.cur;
+    size_t off = 0;
+    auto move = [&](void* dev, size_t bytes) {
+        if (save) cuda_check(cudaMemcpyAsync(base + off, dev, bytes, cudaMemcpyDeviceToDevice, s), "save state");
+        else cuda_check(cudaMemcpyAsync(dev, base + off, bytes, cudaMemcpyDeviceToDevice, s), "restore state");
+        off += bytes;
+    };
+    move(c->count.p + species, 8);
+    if (c->precision == PSUM_PIC_MIXED) {
+        move(sp.key[cur].p, 4 * n);
+        for (int a = 0; a < D; ++a) move(sp.off[a][cur].p, 4 * n);
+        for (int q = 0; q < 3; ++q) move(sp.vel[q][cur].p, 4 * n);
+    } else {
+        for (int a = 0; a < D; ++a) move(sp.pos64[a][cur].p, 8 * n);
+        for (int q = 0; q < 3; ++q) move(sp.vel64[q][cur].p, 8 * n);
+        move(sp.key[cur].p, 4 * n);
+    }
+}
+
+EXPORT int psum_pic_state_bytes(psum_pic_ctx* ctx, int species, unsigned long long* bytes) {
+    return guarded([&] {
+        ctx_check(ctx);
+        if (!bytes) throw std::invalid_argument("state_bytes: null output");
+        *bytes = state_bytes(ctx, species_at(ctx, species));
+    });
+}
+
+EXPORT int psum_pic_save_state(psum_pic_ctx* ctx, int species, void* dst_dev) {
+    return guarded([&] {
+        ctx_check(ctx);
+        Species& sp = species_at(ctx, species);
+        if (!dst_dev) throw std::invalid_argument("save_state: null destination");
+        if (ctx->precision == PSUM_PIC_MIXED) ensure_keys(ctx, sp);
+        state_copy(ctx, species, static_cast<char*>(dst_dev), true);
+        cuda_check(cudaGetLastError(), "save state");
+    });
+}
+
+EXPORT int psum_pic_restore_state(psum_pic_ctx* ctx, int species, const void* src_dev) {
+    return guarded([&] {
+        ctx_check(ctx);
+        Species& sp = species_at(ctx, species);
+        if (!src_dev) throw std::invalid_argument("restore_state: null source");
+        state_copy(ctx, species, static_cast<char*>(const_cast<void*>(src_dev)), false);
+        sp.sorted = false;      // cell offsets are not part of the snapshot
+        sp.keys_stale = false;
+        cuda_check(cudaGetLastError(), "restore state");
     });
 }
 

@@ -73,8 +73,19 @@ struct psum_pic_ctx {
         }
         events.clear();
     }
+    // adjoint scratch: int64 node accumulator, its fixed-point scale, the max
+    psum_b200::DevBuf<unsigned long long> adj_acc;
+    psum_b200::DevBuf<double> adj_scale;
+    psum_b200::DevBuf<unsigned> adj_max;
     ~psum_pic_ctx() {
         drop_events();
         if (own_stream) cudaStreamDestroy(own_stream);
     }
 };
+
+namespace psum_b200 {
+// pic.cu: handle and index checks, and the key fill of a sorted mixed state
+psum_pic_ctx* ctx_check(psum_pic_ctx* c);
+Species& species_at(psum_pic_ctx* c, int s);
+void ensure_keys(psum_pic_ctx* c, Species& sp);
+}  // namespace psum_b200

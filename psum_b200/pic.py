@@ -155,3 +155,33 @@ class ParticleContext:
         f = C.c_uint()
         check(lib().psum_pic_device_errors(self.handle, C.byref(f)))
         return f.value
+
+    # ---- differentiable runs: state snapshots and the adjoint of one step
+    def state_bytes(self, species):
+        b = C.c_ulonglong()
+        check(lib().psum_pic_state_bytes(self.handle, species, C.byref(b)))
+        return b.value
+
+    def save_state(self, species, dst):
+        """Copy the species' state into the device uint8 tensor `dst`."""
+        self._order(dst)
+        check(lib().psum_pic_save_state(self.handle, species, _ptr(dst)))
+
+    def restore_state(self, species, src):
+        self._order(src)
+        check(lib().psum_pic_restore_state(self.handle, species, _ptr(src)))
+
+    def adjoint_push(self, species, phi, dt, lam_x, lam_v, mu):
+        """Adjoint of the leapfrog kick and move at the current state: lam_x
+        (dim, n) and lam_v (3, n) go from the adjoints of the new state to
+        those of the old state (float32 in MIXED contexts, float64 in FP64);
+        the adjoint of phi is added to mu (float64 per node)."""
+        self._order(phi, lam_x, lam_v, mu)
+        check(lib().psum_pic_adjoint_push(self.handle, species, _ptr(phi), float(dt), _ptr(lam_x), _ptr(lam_v),
+                                          _ptr(mu)))
+
+    def adjoint_deposit(self, species, nu, lam_x):
+        """lam_x += gather of the CIC gradient of nu = dL/drho (float64 per node)."""
+        self._order(nu, lam_x)
+        check(lib().psum_pic_adjoint_deposit(self.handle, species, _ptr(nu), _ptr(lam_x)))
+
