@@ -22,6 +22,7 @@ a bounded sample of the same workload.
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -57,6 +58,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 GPU run and the field comparison")
     ap.add_argument("--cpu-sample", type=int, default=1 << 21, help="particles in the CPU baseline sample")
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
+                    help="c2 (default): the bench line; c1/c3/c5: the other plasmas of the scope table; "
+                         "c4: the differentiable run (forward and adjoint)")
     ap.add_argument("--mg-extra", default="", help="extra multigrid options (e.g. 'graph 0' to launch the solve's "
                     "kernels one by one, which profilers need)")
     return ap.parse_args()
@@ -486,6 +490,183 @@ def run_e2e(args, torch, P, dev, rank, dist):
                                          "of the loss counters after each, then D2H of phi"}
 
 
+# --------------------------------------------------- other workloads ---
+WORKLOADS = {
+    # name: (dim, cells, ppc or total, precision, depth, tol, dt, steps in the config)
+    "c1": dict(dim=2, cells=63, ppc=64, precision="fp64", depth=4, tol=1e-10, dt=0.1,
+               desc="2D periodic electrostatic plasma, FP64 plain method: 64x64 wrapping nodes, 64 e-/cell, "
+                    "1% mode-1 density perturbation, uniform ion background"),
+    "c3": dict(dim=3, cells=255, ppc=32, precision="mixed", depth=5, tol=1e-8, dt=0.05, gauge="mean",
+               desc="3D periodic two-stream, mixed precision: 256^3 wrapping nodes, 32 e-/cell in two beams at "
+                    "+/-5 vth along x (dt 0.05: the beams move a quarter cell per step)"),
+    "c5": dict(dim=3, cells=511, total=1_000_000_000, precision="mixed", depth=6, tol=1e-8, dt=0.1, gauge="mean",
+               desc="3D clustered-load stress: 512^3 wrapping nodes, 1e9 e- from a Gaussian blob "
+                    "(sigma = 0.05 L) drifting at 2 vth along z"),
+    "c4": dict(dim=2, cells=255, ppc=64, precision="mixed", depth=5, tol=1e-10, dt=0.1,
+               desc="2D differentiable run: 256^2 wrapping nodes, 64 e-/cell, Landau damping (5% mode-1), "
+                    "100 steps, loss = field energy at the final step, gradients by the adjoint with "
+                    "checkpoints every 10 steps"),
+}
+
+
+def periodic_problem(P, w, mg_extra=""):
+    """Grid (TSI idiom: lower corner at dx/2), gauge, solver.  The gauge is
+    the TSI pinned node, or for the 3D workloads the mean-zero potential
+    (solver option null_space 1): in FP32 V-cycles the pinned operator's
+    lowest mode, eigenvalue ~ 1/nodes, falls below single-precision
+    resolution at 256^3 and the refinement stalls near 1e-4."""
+    dim, cells = w["dim"], w["cells"]
+    nodes = cells + 1
+    lo, hi = (0.5,) * dim, (cells + 0.5,) * dim
+    grid = P.simple_grid(lo, hi, (cells,) * dim)
+    opts = (f"I {nodes} J {nodes} K {nodes if dim == 3 else 1} depth {w['depth']} pre_relax 2 post_relax 2 "
+            f"max_cycles 24 correction_interval 2 tol {w['tol']} periodic_I 1 periodic_J 1"
+            + (" periodic_K 1" if dim == 3 else "") + (" null_space 1" if w.get("gauge") == "mean" else "")
+            + (f" {mg_extra}" if mg_extra else ""))
+    fixed = [] if w.get("gauge") == "mean" else [P.Dirichlet_nodes(grid, [(0,) * dim], 0.0)]
+    backend = "cuda_multigrid64_gpu" if w["precision"] == "fp64" else "cuda_multigrid32f_gpu"
+    return grid, opts, fixed, backend
+
+
+def periodic_initial_state(torch, w, gen, dev):
+    """Positions (dim, n) and velocities (3, n), FP64 on the device."""
+    dim, L = w["dim"], w["cells"] + 1.0
+    name = w["name"]
+    n = w["total"] if "total" in w else int(L ** dim * w["ppc"])
+    if name == "c5":
+        pos = torch.randn((dim, n), generator=gen, device=dev, dtype=torch.float64) * (0.05 * L) + L / 2
+        pos = torch.remainder(pos, L)
+        vel = torch.randn((3, n), generator=gen, device=dev, dtype=torch.float64)
+        vel[2] += 2.0
+    else:
+        pos = torch.rand((dim, n), generator=gen, device=dev, dtype=torch.float64) * L
+        if name in ("c1", "c4"):   # mode-1 density perturbation by inverse-CDF displacement in x
+            amp = 0.01 if name == "c1" else 0.05
+            k = 2 * math.pi / L
+            u = pos[0].clone()
+            x = u.clone()
+            for _ in range(20):
+                x -= (x + amp / k * torch.sin(k * x) - u) / (1 + amp * torch.cos(k * x))
+            pos[0] = torch.remainder(x, L)
+        vel = torch.randn((3, n), generator=gen, device=dev, dtype=torch.float64)
+        if name == "c3":           # two counter-streaming beams along x
+            vel[0, : n // 2] += 5.0
+            vel[0, n // 2:] -= 5.0
+    return pos + 0.5, vel, n
+
+
+def run_workload(args):
+    """One of the other plasmas: its own JSON line, same timing rules."""
+    import torch
+
+    import psum_b200 as P
+    w = dict(WORKLOADS[args.workload], name=args.workload)
+    if args.workload == "c4":
+        return run_c4(args, torch, P, w)
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream()
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(SEED + int(args.workload[1]))
+    grid, opts, fixed, backend = periodic_problem(P, w, args.mg_extra)
+    pos, vel, n = periodic_initial_state(torch, w, gen, dev)
+    L = w["cells"] + 1.0
+    precision = P.FP64 if w["precision"] == "fp64" else P.MIXED
+    ctx = P.ParticleContext((w["cells"],) * w["dim"], (0.5,) * w["dim"], (w["cells"] + 0.5,) * w["dim"],
+                            (1,) * w["dim"], precision)
+    ctx.set_options(f"sort_interval {1 if precision == P.MIXED else 20}")
+    e = ctx.add_species(-1.0, 1.0, L ** w["dim"] / n, n)
+    ctx.load(e, pos, vel)
+    del pos, vel
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    ctx.sort()
+    ctx.deposit()
+    ps = P.Poisson_solver_2d() if w["dim"] == 2 else P.Poisson_solver_3d()
+    ps.set_options(opts)
+    ps.init(backend, grid, ps.Cartesian, fixed, 1.0)
+    ps.make_righthand_item()
+    ctx.set_stream(stream)
+    nn = grid.n_nodes
+    rho = torch.zeros(nn, dtype=torch.float64, device=dev)
+    phi = torch.zeros(nn, dtype=torch.float64, device=dev)
+
+    def step():
+        ctx.step(ps.backend, 1.0, rho, phi, w["dt"])   # background: the uniform ions
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ctx.get_timing(reset=True)
+    ctx.set_timing(True)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        with torch.cuda.stream(stream):
+            start.record(stream)
+            for _ in range(args.steps):
+                step()
+            stop.record(stream)
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(stop) / args.steps
+    phases = ctx.get_timing(reset=True)
+    stats = ps.backend.last_stats()
+    n_valid = ctx.count(e)[1]
+    peak, peak_kind = measured_peaks()
+    sp_bytes = (24 if w["dim"] == 2 else 28) if precision == P.MIXED else (44 if w["dim"] == 2 else 52)
+    b_step = n * 2 * sp_bytes
+    return {"workload": args.workload, "metric": "particle-steps/s incl. Poisson MG",
+            "value": n * args.steps / (ms * args.steps * 1e-3), "unit": "particle-steps/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "dtype": "f64" if precision == P.FP64 else "f32 push / f32-in-f64 MG", "data": "synthetic",
+            "config": {"workload": w["desc"], "particles": n, "nodes": nn, "dt": w["dt"], "mg": opts,
+                       "sort_interval": 1 if precision == P.MIXED else 20},
+            "particle_roofline": {"algorithmic_bytes_per_step": b_step,
+                                  "achieved": round(b_step / (ms * 1e-3) / 1e9, 1), "peak": peak,
+                                  "frac": round(b_step / (ms * 1e-3) / 1e9 / peak, 4)},
+            "phase_ms_per_step": {k: round(v[0] / max(v[1], 1), 4) for k, v in phases.items()},
+            "mg_last_solve": stats, "valid_particles_end": n_valid, "clocks": clk.summary()}
+
+
+def run_c4(args, torch, P, w):
+    """Forward and adjoint of the differentiable run, timed with CUDA events."""
+    from psum_b200.adjoint import ElectrostaticLoss, ElectrostaticRun
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(SEED + 4)
+    grid, opts, fixed, backend = periodic_problem(P, w, args.mg_extra)
+    pos, vel, n = periodic_initial_state(torch, w, gen, dev)
+    L = w["cells"] + 1.0
+    steps = 100
+    run = ElectrostaticRun(grid, (1, 1), [(-1.0, 1.0, L * L / n, pos)], fixed, opts, w["dt"], steps,
+                           checkpoint_every=10, precision=P.MIXED, background=1.0)
+    phi_ext = (torch.randn(grid.n_nodes, generator=gen, device=dev, dtype=torch.float64) * 0.01)
+    v0 = vel.to(torch.float32)
+    times = []
+    for rep in range(args.warmup + max(args.steps // 10, 1)):
+        v = v0.clone().requires_grad_(True)
+        pe = phi_ext.clone().requires_grad_(True)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record()
+        loss = ElectrostaticLoss.apply(run, pe, v)
+        e1.record()
+        loss.backward()
+        e2.record()
+        torch.cuda.synchronize()
+        if rep >= args.warmup:
+            times.append((e0.elapsed_time(e1), e1.elapsed_time(e2)))
+    fwd = statistics.median(t[0] for t in times)
+    bwd = statistics.median(t[1] for t in times)
+    return {"workload": "c4", "metric": "particle-steps/s of the differentiable run (forward; forward + adjoint)",
+            "value": n * steps / (fwd * 1e-3), "unit": "particle-steps/s", "n_gpus": 1, "steps": steps,
+            "warmup": args.warmup, "ms_forward": fwd, "ms_backward": bwd,
+            "value_forward_and_adjoint": n * steps / ((fwd + bwd) * 1e-3), "higher_is_better": True,
+            "dtype": "f32 push and adjoint arrays / f64 fields", "data": "synthetic",
+            "config": {"workload": w["desc"], "particles": n, "nodes": grid.n_nodes, "dt": w["dt"], "mg": opts,
+                       "checkpoint_every": 10},
+            "loss": float(loss.detach()), "grad_v_norm": float(v.grad.norm()), "grad_phi_ext_norm": float(pe.grad.norm())}
+
+
 def run_reference(args, rank):
     if rank != 0:
         return None
@@ -527,6 +708,8 @@ def main():
             dist = tdist
     if args.impl == "reference":
         line = run_reference(args, rank)
+    elif args.workload != "c2":
+        line = run_workload(args) if rank == 0 else None
     else:
         line = run_ours(args, rank, world, dist)
     if line is not None:

@@ -12,7 +12,10 @@
 // every correction_interval cycles; 0 = run exactly max_cycles like PSuM),
 // `max_coarse`, and `periodic_I/J/K 1` (wrap-around transfers on that axis
 // for operators whose node lattice wraps, where PSuM's open-interval
-// transfers make the V-cycle diverge).  The whole solve is enqueued on one stream without host
+// transfers make the V-cycle diverge), and `null_space 1` (a periodic
+// operator assembled without a pinned node, singular with the constants as
+// its null space: the coarse solve inverts Ahat_L + 1 1^T / n and the solve
+// returns the mean-zero solution of b minus its mean).  The whole solve is enqueued on one stream without host
 // synchronisation; func_table.solve synchronises at the end, like PSuM.
 #include <cuda_runtime.h>
 
@@ -155,6 +158,8 @@ struct SolverBase {
     int max_coarse = 8192;
     std::array<int, 3> periodic{0, 0, 0};   // wrap-around transfers per axis (option periodic_I/J/K)
     double tol = 0.0;
+    int null_space = 0;                     // option `null_space 0|1` (read by set_matrix)
+    bool ns_built = false;                  // the hierarchy was built for a singular operator
     int use_graph = 1;                      // option `graph 0|1`: replay the solve as one CUDA graph
     unsigned long long n_row = 0;
     bool ready = false;
@@ -205,7 +210,7 @@ namespace {
 template <class T>
 struct Solver : SolverBase {
     std::vector<std::unique_ptr<Level<T>>> lv;
-    DevBuf<T> coarse_inv;
+    DevBuf<double> coarse_inv;   // FP64 in both backends (see k_dense_mv)
     DevBuf<double> x64;   // FP64 level-0 iterate for the FP64 backend
     void build_device(cudaStream_t s) override {
         a0.upload(host.a0, s);
@@ -232,8 +237,7 @@ struct Solver : SolverBase {
             }
             lv.push_back(std::move(L));
         }
-        std::vector<T> ci(host.coarse_inv.begin(), host.coarse_inv.end());
-        coarse_inv.upload(ci.data(), ci.size(), s);
+        coarse_inv.upload(host.coarse_inv.data(), host.coarse_inv.size(), s);
         if (precision == 64) x64.alloc(n_row);
         cuda_check(cudaStreamSynchronize(s), "build_device");
         levels = host.L + 1;
@@ -364,10 +368,22 @@ struct Solver : SolverBase {
         if (nr > 0) { k_replace<<<grid_for(nr), kThreads, 0, s>>>(b, d_rep_idx.p, d_rep_val.p, nr); count_launch(); }
     }
 
+    // v -= mean(v) (two launches; fixed reduction order)
+    void enqueue_project(double* v, cudaStream_t s) {
+        const long long n = (long long)n_row;
+        { k_sum<<<kNormBlocks, kThreads, 0, s>>>(v, n, partials.p); count_launch(); }
+        { k_sub_mean<<<kNormBlocks, kThreads, 0, s>>>(v, n, partials.p, kNormBlocks); count_launch(); }
+    }
+
     void enqueue_solve(double* b, double* x, cudaStream_t s) override {
         const long long n = (long long)n_row;
         MGState* st = state.p;
+        if (ns_built && !rep_idx.empty())
+            throw std::invalid_argument("multigrid: null_space 1 with fixed (replaced) nodes");
         enqueue_sources(b, s);
+        // singular operator: solve for the consistent part of b (the mean-zero
+        // projection; b is the solve's scratch like PSuM's source vector)
+        if (ns_built) enqueue_project(b, s);
         { k_norm2<<<kNormBlocks, kThreads, 0, s>>>(b, n, partials.p); count_launch(); }
         { k_check<<<1, 32, 0, s>>>(partials.p, kNormBlocks, st, 0, tol, 0, 0); count_launch(); }
         Level<T>& F = *lv[0];
@@ -410,6 +426,7 @@ struct Solver : SolverBase {
             }
             cuda_check(cudaMemcpyAsync(x, xc, sizeof(double) * n, cudaMemcpyDeviceToDevice, s), "copy x");
         }
+        if (ns_built) enqueue_project(x, s);   // the mean-zero representative
         launch_residual64<double>(a0.view, x, b, nullptr, (double*)nullptr, partials.p, st, 0, s);
         { k_check<<<1, 32, 0, s>>>(partials.p, kNormBlocks, st, 2, tol, cycles_done, refinements); count_launch(); }
         cuda_check(cudaGetLastError(), "solve launch");
@@ -464,6 +481,7 @@ void solver_set_options(SolverBase* s, const char* options) {
         else if (key == "periodic_J") s->periodic[1] = parse_int(iss, key) != 0;
         else if (key == "periodic_K") s->periodic[2] = parse_int(iss, key) != 0;
         else if (key == "graph") s->use_graph = parse_int(iss, key) != 0;
+        else if (key == "null_space") s->null_space = parse_int(iss, key) != 0;
         else if (key == "correction_interval") {
             int v = 0;
             if (!(iss >> v) || v < 1) throw std::invalid_argument("correction_interval must be positive");
@@ -487,7 +505,8 @@ void solver_set_matrix(SolverBase* s, unsigned long long n_row, unsigned long lo
                        const unsigned long long* rows, const unsigned long long* cols, const double* vals) {
     if (n_row != n_col) throw std::invalid_argument("set_matrix: matrix must be square");
     HostCSR A = csr_from_coo((long long)n_row, (long long)n_col, (long long)nnz, rows, cols, vals);
-    s->host = build_hierarchy(A, s->I, s->J, s->K, s->depth, s->max_coarse, s->periodic);
+    s->host = build_hierarchy(A, s->I, s->J, s->K, s->depth, s->max_coarse, s->periodic, s->null_space != 0);
+    s->ns_built = s->null_space != 0;
     s->n_row = n_row;
     ensure_stream(s);
     // created here, outside any stream capture: the stream that captures the

@@ -287,12 +287,14 @@ void scale_rows(HostCSR& a, const std::vector<double>& d) {
         for (long long k = a.ptr[r]; k < a.ptr[r + 1]; ++k) a.val[k] *= d[r];
 }
 
-// Gauss-Jordan inverse with partial pivoting (textbook method).
-std::vector<double> dense_inverse(const HostCSR& a) {
+// Gauss-Jordan inverse with partial pivoting (textbook method) of a + shift
+// (shift added to every entry: the rank-one term of a singular operator
+// whose null space is the constants).
+std::vector<double> dense_inverse(const HostCSR& a, double shift = 0.0) {
     const long long n = a.n_row;
-    std::vector<double> m(n * n, 0.0), inv(n * n, 0.0);
+    std::vector<double> m(n * n, shift), inv(n * n, 0.0);
     for (long long r = 0; r < n; ++r) {
-        for (long long k = a.ptr[r]; k < a.ptr[r + 1]; ++k) m[r * n + a.col[k]] = a.val[k];
+        for (long long k = a.ptr[r]; k < a.ptr[r + 1]; ++k) m[r * n + a.col[k]] += a.val[k];
         inv[r * n + r] = 1.0;
     }
     for (long long c = 0; c < n; ++c) {
@@ -459,7 +461,7 @@ StencilOp decompose(const HostCSR& A, const std::array<int, 3>& dims) {
 }
 
 Hierarchy build_hierarchy(const HostCSR& A, int I, int J, int K, int depth, int max_coarse,
-                          const std::array<int, 3>& periodic) {
+                          const std::array<int, 3>& periodic, bool null_space) {
     if (A.n_row != A.n_col) throw std::runtime_error("invalid setup parameter");
     if (I < 1 || J < 1 || K < 1 || depth < 1)
         throw std::invalid_argument("multigrid: positive grid dimensions and depth required");
@@ -517,7 +519,9 @@ Hierarchy build_hierarchy(const HostCSR& A, int I, int J, int K, int depth, int 
                 throw std::runtime_error("sycl_inner_solver: coarse matrix too large (" + std::to_string(next.n_row) +
                                          " > " + std::to_string(max_coarse) + ")");
             h.ahat[l] = decompose(next, h.dims[l]);
-            h.coarse_inv = dense_inverse(next);
+            // null space = constants at every level (P reproduces constants):
+            // (Ahat_L + 1 1^T / n)^-1 solves every consistent coarse system
+            h.coarse_inv = dense_inverse(next, null_space ? 1.0 / (double)next.n_row : 0.0);
         }
         cur = std::move(next);
     }

@@ -73,8 +73,11 @@ struct Hierarchy {
 // Throws std::invalid_argument / std::runtime_error with PSuM's messages.
 // periodic[d] != 0 selects wrap-around transfers on axis d (an extension:
 // PSuM's open-interval transfers diverge on wrapping lattices).
+// null_space: A is singular with the constants as its null space (a
+// periodic operator without a pinned node); the coarse inverse then solves
+// the consistent coarse systems.
 Hierarchy build_hierarchy(const HostCSR& A, int I, int J, int K, int depth, int max_coarse = 8192,
-                          const std::array<int, 3>& periodic = {0, 0, 0});
+                          const std::array<int, 3>& periodic = {0, 0, 0}, bool null_space = false);
 
 // Stencil + exception decomposition of one operator on a node box.
 StencilOp decompose(const HostCSR& A, const std::array<int, 3>& dims);

@@ -231,26 +231,30 @@ __global__ void __launch_bounds__(kThreads) k_prolong_add(XferDev<T> X, const T*
     prolong_row<T, true>(X, xc, xf, f);
 }
 
-// x = Ainv b (dense, row-major), one warp per row, fixed shuffle tree.
+// x = Ainv b (dense, row-major), one warp per row, fixed shuffle tree.  The
+// inverse and the sums are FP64 in both backends: the coarsest operator of a
+// periodic problem pinned at one node is nearly singular (its near-constant
+// mode), so its inverse has entries far larger than FP32 can cancel.
 template <class T, bool RO>
-__device__ __forceinline__ T dense_row(const T* __restrict__ Ainv, const T* __restrict__ b, int n, int row, int lane) {
-    const T* a = Ainv + (long long)row * n;
-    T s = T(0);
-    for (int c = lane; c < n; c += 32) s += __ldg(a + c) * ldv<RO>(b + c);
+__device__ __forceinline__ double dense_row(const double* __restrict__ Ainv, const T* __restrict__ b, int n, int row,
+                                            int lane) {
+    const double* a = Ainv + (long long)row * n;
+    double s = 0.0;
+    for (int c = lane; c < n; c += 32) s += __ldg(a + c) * (double)ldv<RO>(b + c);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     return s;
 }
 
 template <class T>
-__global__ void __launch_bounds__(kThreads) k_dense_mv(const T* __restrict__ Ainv, const T* __restrict__ b,
+__global__ void __launch_bounds__(kThreads) k_dense_mv(const double* __restrict__ Ainv, const T* __restrict__ b,
                                                        T* __restrict__ x, int n, const MGState* __restrict__ st) {
     if (st && st->done) return;   // st == nullptr: ungated (inside the device-side loop)
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= n) return;
-    const T s = dense_row<T, true>(Ainv, b, n, warp, lane);
-    if (lane == 0) x[warp] = s;
+    const double s = dense_row<T, true>(Ainv, b, n, warp, lane);
+    if (lane == 0) x[warp] = (T)s;
 }
 
 // Block-level FP64 sum in a fixed order (deterministic for a fixed launch).
@@ -295,6 +299,34 @@ __global__ void __launch_bounds__(kThreads) k_norm2(const double* __restrict__ v
         acc += v[r] * v[r];
     const double t = block_sum(acc);
     if (threadIdx.x == 0) partials[blockIdx.x] = t;
+}
+
+// Per-block sums of v (the mean of a null-space solve's vectors), in the
+// fixed order of k_norm2.
+__global__ void __launch_bounds__(kThreads) k_sum(const double* __restrict__ v, long long n,
+                                                  double* __restrict__ partials) {
+    double acc = 0.0;
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x)
+        acc += v[r];
+    const double t = block_sum(acc);
+    if (threadIdx.x == 0) partials[blockIdx.x] = t;
+}
+
+// v -= sum(partials) / n: projection onto the mean-zero vectors.  Every block
+// adds the partials in the same order, so all see the same mean.
+__global__ void __launch_bounds__(kThreads) k_sub_mean(double* __restrict__ v, long long n,
+                                                       const double* __restrict__ partials, int nparts) {
+    __shared__ double mean;
+    if (threadIdx.x < 32) {
+        double a = 0.0;
+        for (int i = threadIdx.x; i < nparts; i += 32) a += partials[i];
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if (threadIdx.x == 0) mean = a / (double)n;
+    }
+    __syncthreads();
+    const double m = mean;
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x)
+        v[r] -= m;
 }
 
 // bhat = T(dinv * b) (start of an FP64 solve: hadamard_to, multigrid_core.hpp:208)

@@ -246,3 +246,71 @@ def test_graph_replay_matches_direct_launches(kind):
         assert launches[1] == launches[0]
     else:
         assert sum(launches[1]) < sum(launches[0])   # converged cycles are not launched
+
+
+def periodic_unpinned(dim, n1, seed=3):
+    """Periodic operator without a pinned node (singular; null space = the
+    constants) and a right-hand side that is not mean-zero."""
+    g = P.simple_grid((0.5,) * dim, (n1 - 0.5,) * dim, (n1 - 1,) * dim)
+    r, c, v = P.assemble_poisson(g, [], 1.0)
+    n = n1 ** dim
+    b = np.random.default_rng(seed).normal(size=n) + 0.3
+    return r, c, v, n, b
+
+
+@pytest.mark.parametrize("kind", ["cuda_multigrid32f_gpu", "cuda_multigrid64_gpu"])
+def test_null_space_solution_is_mean_zero_direct_solution(kind):
+    # null_space 1: x = the mean-zero solution of A x = b - mean(b), the
+    # pinned direct solution shifted to mean zero
+    r, c, v, n, b = periodic_unpinned(2, 128)
+    s = P.solver_backend(kind)
+    s.set_options("I 128 J 128 depth 5 pre_relax 2 post_relax 2 max_cycles 40 correction_interval 4 tol 1e-12 "
+                  "periodic_I 1 periodic_J 1 null_space 1")
+    s.set_matrix(n, n, r.size, r, c, v)
+    bd, xd = dev(b), dev(np.zeros(n))
+    code = s.solve(bd, xd)
+    st = s.last_stats()
+    assert code == 0, st
+    A = csr(r, c, v, n).tolil()
+    A[0, :] = 0.0
+    A[0, 0] = 1.0
+    bb = b - b.mean()
+    bb[0] = 0.0
+    direct = spl.spsolve(A.tocsc(), bb)
+    direct -= direct.mean()
+    got = xd.cpu().numpy()
+    assert abs(got.mean()) <= 1e-14 * np.abs(got).max()
+    assert np.linalg.norm(got - direct) / np.linalg.norm(direct) < 1e-10
+    # the projected right-hand side is what the solve returns in b
+    assert np.linalg.norm(bd.cpu().numpy() - (b - b.mean())) <= 1e-14 * np.linalg.norm(b)
+
+
+def test_null_space_mixed_converges_3d_256():
+    # 256^3 wrapping nodes: FP32 V-cycles in FP64 refinement reach 1e-10
+    # and agree with the FP64 V-cycles
+    r, c, v, n, b = periodic_unpinned(3, 256, seed=4)
+    opts = ("I 256 J 256 K 256 depth 4 pre_relax 2 post_relax 2 max_cycles 40 correction_interval 2 tol 1e-10 "
+            "periodic_I 1 periodic_J 1 periodic_K 1 null_space 1")
+    xs = {}
+    for kind in ("cuda_multigrid32f_gpu", "cuda_multigrid64_gpu"):
+        s = P.solver_backend(kind)
+        s.set_options(opts)
+        s.set_matrix(n, n, r.size, r, c, v)
+        bd, xd = dev(b), dev(np.zeros(n))
+        code = s.solve(bd, xd)
+        assert code == 0, (kind, s.last_stats())
+        xs[kind] = xd
+        s.free()
+        del bd
+    d = (xs["cuda_multigrid32f_gpu"] - xs["cuda_multigrid64_gpu"]).norm() / xs["cuda_multigrid64_gpu"].norm()
+    assert float(d) < 1e-8
+
+
+def test_null_space_rejects_fixed_nodes():
+    r, c, v, n, b = periodic_unpinned(2, 32)
+    s = P.solver_backend("cuda_multigrid32f_gpu")
+    s.set_options("I 32 J 32 depth 3 max_cycles 4 tol 1e-8 periodic_I 1 periodic_J 1 null_space 1")
+    s.set_matrix(n, n, r.size, r, c, v)
+    s.set_source_replace(np.array([0], np.uint64), np.array([0.0]))
+    with pytest.raises(P.PsumError):
+        s.solve(dev(b), dev(np.zeros(n)))
