@@ -149,9 +149,10 @@ __device__ __forceinline__ void interp_grad(const CellField<D>& F, const float f
 // cell with offset 0).  Every operation is an explicit round-to-nearest
 // intrinsic (fused multiply-adds where written), so every kernel that calls
 // this function moves the same particle bit-identically.  False when the
-// state became non-finite (the error word is flagged).
+// state became non-finite (kick_move flags the error word; kick_move_core
+// leaves that to its caller).
 template <int D, int PUSHER>
-__device__ __forceinline__ bool kick_move(const PushArgs& a, const float G[3], float f[3], float v[3], int dc[3]) {
+__device__ __forceinline__ bool kick_move_core(const PushArgs& a, const float G[3], float f[3], float v[3], int dc[3]) {
     if (PUSHER == PSUM_PIC_LEAPFROG) {
 #pragma unroll
         for (int d = 0; d < D; ++d) v[d] = __fmaf_rn(-a.kE[d], G[d], v[d]);   // v += (q/m) E dt, E = -dr G
@@ -192,6 +193,12 @@ __device__ __forceinline__ bool kick_move(const PushArgs& a, const float G[3], f
         f[d] = nf;
         dc[d] = step;
     }
+    return ok;
+}
+
+template <int D, int PUSHER>
+__device__ __forceinline__ bool kick_move(const PushArgs& a, const float G[3], float f[3], float v[3], int dc[3]) {
+    const bool ok = kick_move_core<D, PUSHER>(a, G, f, v, dc);
     if (!ok) atomicOr(a.err, kErrNonFinite);
     return ok;
 }
@@ -446,7 +453,8 @@ struct ClsArgs {
     PushArgs p;                   // current state, fields, deposit, losses, error word
     const unsigned* starts;       // n_cells + 1 cell offsets of the current state
     const unsigned* block_first;  // first cell of each block (k_cls_blocks)
-    unsigned* cls;                // n_cells * classes: counts (pass 1), then group offsets (pass 2)
+    unsigned* cls;                // [class][cell]: counts (pass 1), then group offsets (pass 2);
+                                  // class-major so that k_cls_offsets reads every class coalesced
     const unsigned* new_starts;   // n_cells + 1 offsets of the new state (pass 2)
     int* far;                     // pass 1: 1 when a particle moved more than one cell on an axis
     float* off_out[3];            // new state (its keys follow from new_starts)
@@ -549,21 +557,38 @@ __device__ __forceinline__ int push_classify(const PushArgs& a, const CellField<
     float G[3];
     interp_grad<D>(F, f, G);
     int dc[3] = {0, 0, 0};
-    if (!kick_move<D, PUSHER>(a, G, f, v, dc)) return -3;
-    cn[0] = co[0];
-    cn[1] = co[1];
+    const bool ok = kick_move_core<D, PUSHER>(a, G, f, v, dc);
+    // common path: the new cell lies inside the lattice on every axis (one
+    // unsigned test per axis); wrapping, losses and non-finite states take
+    // the rare path, which follows kick_move and apply_step exactly
+    const GridView& g = a.g;
+    bool out = false;
     cn[2] = co[2];
-    const int lost = apply_step<D>(a.g, cn, dc);
-    if (lost >= 0) {
 #pragma unroll
-        for (int q = 0; q < 2 * D; ++q) lost_cnt[q] += (lost == q);
-        return -3;
+    for (int d = 0; d < D; ++d) {
+        cn[d] = co[d] + dc[d];
+        out |= (unsigned)cn[d] >= (unsigned)(g.periodic[d] ? g.M[d] : g.cells[d]);
+    }
+    if (!ok || out) {
+        if (!ok) {
+            atomicOr(a.err, kErrNonFinite);
+            return -3;
+        }
+        cn[0] = co[0];
+        cn[1] = co[1];
+        cn[2] = co[2];
+        const int lost = apply_step<D>(g, cn, dc);
+        if (lost >= 0) {
+#pragma unroll
+            for (int q = 0; q < 2 * D; ++q) lost_cnt[q] += (lost == q);
+            return -3;
+        }
     }
     int cls = 0;
     bool far = false;
 #pragma unroll
     for (int d = 0; d < D; ++d) {
-        far |= dc[d] < -1 || dc[d] > 1;
+        far |= (unsigned)(dc[d] + 1) > 2u;
         cls = cls * 3 + dc[d] + 1;
     }
     return far ? -1 : cls;
@@ -702,7 +727,7 @@ __global__ void __launch_bounds__(kPicThreads) k_cls_pass1(ClsArgs a) {
         // (for a fixed corner the classes reach distinct nodes: no conflicts)
         if (lane < NC) {
             const unsigned n = mom_lo[warp][0][lane];
-            a.cls[c * NC + lane] = n;
+            a.cls[lane * a.n_cells + c] = n;
             if (n) {
                 long long W[8];
                 W[0] = (long long)n << kCicBits;
@@ -762,7 +787,6 @@ __global__ void __launch_bounds__(kPicThreads) k_cls_pass1(ClsArgs a) {
 template <int D>
 __global__ void k_cls_offsets(GridView g, unsigned* __restrict__ cls, unsigned* __restrict__ newcount,
                               long long n_cells) {
-    constexpr int NC = MoveClasses<D>::N;
     const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c > n_cells) return;
     if (c == n_cells) {
@@ -804,7 +828,7 @@ __global__ void k_cls_offsets(GridView g, unsigned* __restrict__ cls, unsigned* 
                     d = d * 3 + st[a] + 1;
                 }
                 if (!ok) continue;
-                const long long idx = (long long)cell_to_key(g, src[0], src[1], src[2]) * NC + d;
+                const long long idx = (long long)d * n_cells + cell_to_key(g, src[0], src[1], src[2]);
                 const unsigned t = cls[idx];
                 cls[idx] = total;
                 total += t;
@@ -875,7 +899,7 @@ __global__ void __launch_bounds__(kPicThreads) k_cls_pass2(ClsArgs a) {
             fill_w[warp][lane] = 0u;
             if (class_target<D>(g, co, lane, cn))
                 base_w[warp][lane] = __ldg(a.new_starts + cell_to_key(g, cn[0], cn[1], cn[2])) +
-                                     __ldg(a.cls + c * NC + lane);
+                                     __ldg(a.cls + lane * a.n_cells + c);
         }
         CellField<D> F;
         load_cell_field<D>(a.p, co[0], co[1], co[2], F);
