@@ -139,6 +139,17 @@ EXPORT int psum_pic_get_losses(psum_pic_ctx* ctx, unsigned long long* losses_hos
 EXPORT int psum_pic_step(psum_pic_ctx* ctx, psum_field_solver_handle solver, double background,
                          double* rho_dev, double* phi_dev, double dt, int pusher, const double* B);
 
+/* With the fused sorted step (mixed precision, sort_interval 1), a step's
+ * second pass (the re-sorted particle writes) runs on a stream of the
+ * context after the step returns, so that the next step's charge density and
+ * Poisson solve overlap it; every other function of this header that reads
+ * or writes particle state orders the context's stream after it first
+ * (psum_pic_get_losses does not need to: loss counts are final earlier).
+ * psum_pic_join does only that: after it, work enqueued on the context's
+ * stream sees the complete step, e.g. an event that closes a timed region.
+ * No counterpart in the reference, whose push is synchronous. */
+EXPORT int psum_pic_join(psum_pic_ctx* ctx);
+
 /* Per-phase CUDA-event timing of psum_pic_step on the context's stream.
  * Phases: 0 rho, 1 Poisson solve, 2 gather+push+deposit, 3 sort.
  * get_timing returns accumulated milliseconds and phase executions since the

@@ -1425,8 +1425,17 @@ constexpr int kDiagBlocks = 296;
 
 // ============================================================ host side ===
 
-psum_pic_ctx* ctx_check(psum_pic_ctx* c) {
+static void finish_cls_step(psum_pic_ctx* c);
+constexpr int kPhaseContinued = 0x100;   // timing pair that adds time to a phase execution already counted
+
+psum_pic_ctx* ctx_check_nojoin(psum_pic_ctx* c) {
     if (!c || c->magic != kPicMagic) throw Error(PSUM_ERR_INVALID_ARGUMENT, "not a particle context of this library");
+    return c;
+}
+
+psum_pic_ctx* ctx_check(psum_pic_ctx* c) {
+    ctx_check_nojoin(c);
+    finish_cls_step(c);
     return c;
 }
 
@@ -1660,9 +1669,8 @@ static void sort_all(psum_pic_ctx* c) {
 // sort) for this step; their deposit from pass 1 stands.
 static long long cls_blocks(long long n, int dim) { return n / cls_block_particles(dim) + 1; }
 
-static void launch_pass(psum_pic_ctx* c, const ClsArgs& a, int dim, int pusher, int pass, long long n) {
+static void launch_pass(const ClsArgs& a, int dim, int pusher, int pass, long long n, cudaStream_t s) {
     const unsigned blocks = (unsigned)cls_blocks(n, dim);
-    cudaStream_t s = c->stream;
 #define PSUM_PASS(D_, P_) \
     do { \
         if (pass == 1) { k_cls_pass1<D_, P_><<<blocks, kPicThreads, 0, s>>>(a); count_launch(); } \
@@ -1678,17 +1686,32 @@ static void launch_pass(psum_pic_ctx* c, const ClsArgs& a, int dim, int pusher, 
 #undef PSUM_PASS
 }
 
+template <class T>
+static void grow(DevBuf<T>& b, size_t count) {
+    if (b.n < count) b.alloc(count);
+}
+
 static void ensure_cls_buffers(psum_pic_ctx* c) {
     const long long nc = c->g.n_cells;
     const int ncls = c->g.dim == 2 ? 9 : 27;
-    long long nmax = 0;
-    for (auto& sp : c->sp) nmax = std::max(nmax, sp->n);
-    c->cls_count.alloc((size_t)nc * ncls);
-    c->cls_first.alloc((size_t)cls_blocks(nmax, c->g.dim) + 1);
-    c->newcount.alloc((size_t)nc + 1);
-    c->scan_tmp1.alloc((size_t)(nc + 1 + kScanBlock - 1) / kScanBlock + 1);
-    c->scan_tmp2.alloc(16);
-    c->far_flag.alloc(8);
+    for (auto& spp : c->sp) {
+        Species& sp = *spp;
+        if (sp.n <= 0) continue;
+        grow(sp.cls_count, (size_t)nc * ncls);
+        grow(sp.cls_first, (size_t)cls_blocks(sp.n, c->g.dim) + 1);
+        grow(sp.newcount, (size_t)nc + 1);
+        grow(sp.scan_tmp1, (size_t)(nc + 1 + kScanBlock - 1) / kScanBlock + 1);
+        grow(sp.scan_tmp2, 16);
+    }
+    grow(c->far_flag, 8);
+    if (!c->side) {
+        int least = 0, greatest = 0;
+        cuda_check(cudaDeviceGetStreamPriorityRange(&least, &greatest), "cudaDeviceGetStreamPriorityRange");
+        cuda_check(cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, least), "cudaStreamCreate");
+    }
+    if (!c->ev_pass1) cuda_check(cudaEventCreateWithFlags(&c->ev_pass1, cudaEventDisableTiming), "cudaEventCreate");
+    if (!c->ev_pass2) cuda_check(cudaEventCreateWithFlags(&c->ev_pass2, cudaEventDisableTiming), "cudaEventCreate");
+    if (!c->far_host) cuda_check(cudaHostAlloc(&c->far_host, sizeof(int) * 8, cudaHostAllocDefault), "cudaHostAlloc");
 }
 
 // The fused step needs distinct source cells for the classes arriving in a
@@ -1699,6 +1722,12 @@ static bool cls_step_applies(const psum_pic_ctx* c) {
     return true;
 }
 
+// First passes of every species (push, deposit, per-group counts), the
+// group offsets and the new cell offsets on the context stream; then the
+// second passes (push again, write the re-sorted state) on the side stream.
+// The step stays pending until finish_cls_step joins it: the caller can
+// meanwhile enqueue work that needs only the deposit and the loss counts
+// (the next step's charge density and Poisson solve).
 static void cls_step(psum_pic_ctx* c, const double* phi, double dt, int pusher, const double* B) {
     cudaStream_t s = c->stream;
     ensure_cls_buffers(c);
@@ -1708,14 +1737,15 @@ static void cls_step(psum_pic_ctx* c, const double* phi, double dt, int pusher, 
     cuda_check(cudaMemsetAsync(c->far_flag.p, 0, sizeof(int) * 8, s), "memset");
     const int ns = (int)c->sp.size();
     const long long nc = c->g.n_cells;
+    std::vector<ClsArgs> args(ns);
     for (int si = 0; si < ns; ++si) {
         Species& sp = *c->sp[si];
         if (sp.n <= 0) continue;
-        ClsArgs a{};
+        ClsArgs& a = args[si];
         a.p = make_push_args(c, sp, si, dt, pusher, B);
         a.starts = sp.starts[sp.starts_cur].p;
-        a.block_first = c->cls_first.p;
-        a.cls = c->cls_count.p;
+        a.block_first = sp.cls_first.p;
+        a.cls = sp.cls_count.p;
         a.new_starts = sp.starts[1 - sp.starts_cur].p;
         a.far = c->far_flag.p + si;
         const int nxt = 1 - sp.cur;
@@ -1726,35 +1756,65 @@ static void cls_step(psum_pic_ctx* c, const double* phi, double dt, int pusher, 
         a.n_cells = nc;
         const long long nb = cls_blocks(sp.n, c->g.dim);
         { k_cls_blocks<<<blocks_for(std::max(nc, nb) + 1, 256), 256, 0, s>>>(a.starts, nc, nb, cls_block_particles(c->g.dim),
-                                                                             c->cls_first.p); count_launch(); }
-        launch_pass(c, a, c->g.dim, pusher, 1, sp.n);
-        if (c->g.dim == 2) { k_cls_offsets<2><<<blocks_for(nc + 1, 256), 256, 0, s>>>(c->g, c->cls_count.p, c->newcount.p, nc); count_launch(); }
-        else { k_cls_offsets<3><<<blocks_for(nc + 1, 256), 256, 0, s>>>(c->g, c->cls_count.p, c->newcount.p, nc); count_launch(); }
-        exclusive_scan_u32(c->newcount.p, sp.starts[1 - sp.starts_cur].p, nc + 1, c->scan_tmp1.p, c->scan_tmp2.p, s);
-        launch_pass(c, a, c->g.dim, pusher, 2, sp.n);
+                                                                             sp.cls_first.p); count_launch(); }
+        launch_pass(a, c->g.dim, pusher, 1, sp.n, s);
+        if (c->g.dim == 2) { k_cls_offsets<2><<<blocks_for(nc + 1, 256), 256, 0, s>>>(c->g, sp.cls_count.p, sp.newcount.p, nc); count_launch(); }
+        else { k_cls_offsets<3><<<blocks_for(nc + 1, 256), 256, 0, s>>>(c->g, sp.cls_count.p, sp.newcount.p, nc); count_launch(); }
+        exclusive_scan_u32(sp.newcount.p, sp.starts[1 - sp.starts_cur].p, nc + 1, sp.scan_tmp1.p, sp.scan_tmp2.p, s);
     }
-    int far[8] = {0};
-    cuda_check(cudaMemcpyAsync(far, c->far_flag.p, sizeof(int) * 8, cudaMemcpyDeviceToHost, s), "D2H");
-    cuda_check(cudaStreamSynchronize(s), "far flag sync");
+    cuda_check(cudaMemcpyAsync(c->far_host, c->far_flag.p, sizeof(int) * 8, cudaMemcpyDeviceToHost, s), "D2H");
+    cuda_check(cudaEventRecord(c->ev_pass1, s), "cudaEventRecord");
+    cuda_check(cudaStreamWaitEvent(c->side, c->ev_pass1, 0), "cudaStreamWaitEvent");
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    if (c->timing) {
+        cuda_check(cudaEventCreate(&t0), "cudaEventCreate");
+        cuda_check(cudaEventCreate(&t1), "cudaEventCreate");
+        cuda_check(cudaEventRecord(t0, c->side), "cudaEventRecord");
+    }
+    for (int si = 0; si < ns; ++si)
+        if (c->sp[si]->n > 0) launch_pass(args[si], c->g.dim, pusher, 2, c->sp[si]->n, c->side);
+    if (c->timing) {
+        cuda_check(cudaEventRecord(t1, c->side), "cudaEventRecord");
+        c->events.push_back({2 | kPhaseContinued, {t0, t1}});   // push phase: the second passes
+    }
+    cuda_check(cudaEventRecord(c->ev_pass2, c->side), "cudaEventRecord");
+    cuda_check(cudaGetLastError(), "fused step launch");
+    c->pending = true;
+    c->pend_dt = dt;
+    c->pend_pusher = pusher;
+    c->pend_has_B = B != nullptr;
+    for (int d = 0; d < 3; ++d) c->pend_B[d] = B ? B[d] : 0.0;
+}
+
+// Joins a pending fused step: the context stream waits for the second
+// passes, and each species either takes its re-sorted state or, when one of
+// its particles moved more than one cell along an axis (its second pass then
+// wrote nothing), moves in place and is radix sorted (no second deposit).
+static void finish_cls_step(psum_pic_ctx* c) {
+    if (!c->pending) return;
+    c->pending = false;
+    cudaStream_t s = c->stream;
+    cuda_check(cudaStreamWaitEvent(s, c->ev_pass2, 0), "join second passes");
+    cuda_check(cudaEventSynchronize(c->ev_pass1), "far flag wait");
+    const int ns = (int)c->sp.size();
     for (int si = 0; si < ns; ++si) {
         Species& sp = *c->sp[si];
         if (sp.n <= 0) continue;
-        if (!far[si]) {
+        if (!c->far_host[si]) {
             { k_count_from<<<1, 1, 0, s>>>(c->count.p + si, sp.starts[1 - sp.starts_cur].p + c->g.n_cells); count_launch(); }
             sp.cur = 1 - sp.cur;
             sp.starts_cur = 1 - sp.starts_cur;
             sp.keys_stale = true;
             continue;
         }
-        // general path: move in place (no second deposit), then radix sort
         ensure_keys(c, sp);
-        PushArgs pa = make_push_args(c, sp, si, dt, pusher, B);
+        PushArgs pa = make_push_args(c, sp, si, c->pend_dt, c->pend_pusher, c->pend_has_B ? c->pend_B : nullptr);
         pa.acc = nullptr;
         pa.losses = c->losses.p + 6 * 8;   // discard slot: pass 1 already counted this step's losses
-        launch_mixed(pa, c->g.dim, pusher, false, sp.n, s);
+        launch_mixed(pa, c->g.dim, c->pend_pusher, false, sp.n, s);
         sort_species(c, sp, si);
     }
-    cuda_check(cudaGetLastError(), "fused step launch");
+    cuda_check(cudaGetLastError(), "fused step finish");
 }
 
 static void rho_into(psum_pic_ctx* c, double background, double* rho, int only_species, bool with_charge) {
@@ -1848,8 +1908,14 @@ EXPORT int psum_pic_destroy(psum_pic_ctx* ctx) {
 EXPORT int psum_pic_set_stream(psum_pic_ctx* ctx, void* stream) {
     return guarded([&] {
         ctx_check(ctx);
+        // work already enqueued on the old stream completes before the new one is used
+        cuda_check(cudaStreamSynchronize(ctx->stream), "set_stream sync");
         ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
     });
+}
+
+EXPORT int psum_pic_join(psum_pic_ctx* ctx) {
+    return guarded([&] { ctx_check(ctx); });
 }
 
 EXPORT int psum_pic_set_options(psum_pic_ctx* ctx, const char* options) {
@@ -2193,7 +2259,7 @@ EXPORT int psum_pic_push(psum_pic_ctx* ctx, const double* phi_dev, double dt, in
 
 EXPORT int psum_pic_get_losses(psum_pic_ctx* ctx, unsigned long long* losses_host, int reset) {
     return guarded([&] {
-        ctx_check(ctx);
+        ctx_check_nojoin(ctx);   // a fused step's counts are final after its first passes
         if (!losses_host) throw std::invalid_argument("get_losses: null output");
         std::vector<unsigned long long> all(48);
         cuda_check(cudaMemcpyAsync(all.data(), ctx->losses.p, sizeof(unsigned long long) * 48, cudaMemcpyDeviceToHost,
@@ -2230,19 +2296,41 @@ struct PhaseTimer {
 EXPORT int psum_pic_step(psum_pic_ctx* ctx, psum_field_solver_handle solver, double background, double* rho_dev,
                          double* phi_dev, double dt, int pusher, const double* B) {
     return guarded([&] {
-        ctx_check(ctx);
+        // the charge density and the solve need only the previous step's
+        // first passes: its second passes may still run on the side stream
+        ctx_check_nojoin(ctx);
         SolverBase* sv = solver_from_handle(solver);
         if (!rho_dev || !phi_dev) throw std::invalid_argument("step: null field");
-        {
-            PhaseTimer t(ctx, 0);
-            rho_into(ctx, background, rho_dev, -1, true);
-            t.stop();
+        if (!ctx->prio) {
+            int least = 0, greatest = 0;
+            cuda_check(cudaDeviceGetStreamPriorityRange(&least, &greatest), "cudaDeviceGetStreamPriorityRange");
+            cuda_check(cudaStreamCreateWithPriority(&ctx->prio, cudaStreamNonBlocking, greatest), "cudaStreamCreate");
+            cuda_check(cudaEventCreateWithFlags(&ctx->ev_in, cudaEventDisableTiming), "cudaEventCreate");
+            cuda_check(cudaEventCreateWithFlags(&ctx->ev_out, cudaEventDisableTiming), "cudaEventCreate");
         }
-        {
-            PhaseTimer t(ctx, 1);
-            solver_solve_async(sv, rho_dev, phi_dev, ctx->stream);
-            t.stop();
+        cudaStream_t user = ctx->stream;
+        cuda_check(cudaEventRecord(ctx->ev_in, user), "cudaEventRecord");
+        cuda_check(cudaStreamWaitEvent(ctx->prio, ctx->ev_in, 0), "cudaStreamWaitEvent");
+        ctx->stream = ctx->prio;
+        try {
+            {
+                PhaseTimer t(ctx, 0);
+                rho_into(ctx, background, rho_dev, -1, true);
+                t.stop();
+            }
+            {
+                PhaseTimer t(ctx, 1);
+                solver_solve_async(sv, rho_dev, phi_dev, ctx->prio);
+                t.stop();
+            }
+        } catch (...) {
+            ctx->stream = user;
+            throw;
         }
+        ctx->stream = user;
+        cuda_check(cudaEventRecord(ctx->ev_out, ctx->prio), "cudaEventRecord");
+        cuda_check(cudaStreamWaitEvent(user, ctx->ev_out, 0), "cudaStreamWaitEvent");
+        finish_cls_step(ctx);
         bool fused = ctx->precision == PSUM_PIC_MIXED && ctx->sort_interval == 1 && cls_step_applies(ctx);
         for (auto& sp : ctx->sp) fused = fused && (sp->sorted || sp->n == 0);
         if (pusher != PSUM_PIC_LEAPFROG && pusher != PSUM_PIC_BORIS) throw std::invalid_argument("step: unknown pusher");
@@ -2287,8 +2375,9 @@ EXPORT int psum_pic_get_timing(psum_pic_ctx* ctx, double* ms_host, int* count_ho
         for (auto& e : ctx->events) {
             float ms = 0.f;
             cuda_check(cudaEventElapsedTime(&ms, e.second.first, e.second.second), "cudaEventElapsedTime");
-            ms_host[e.first] += ms;
-            if (count_host) count_host[e.first] += 1;
+            const int p = e.first & 0xff;
+            ms_host[p] += ms;
+            if (count_host && !(e.first & kPhaseContinued)) count_host[p] += 1;
         }
         if (reset) ctx->drop_events();
     });

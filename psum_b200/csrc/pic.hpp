@@ -32,6 +32,10 @@ struct Species {
     int starts_cur = 0;
     bool sorted = false;              // state sorted by cell and starts valid
     bool keys_stale = false;          // sorted mixed state whose keys follow from starts but are not written
+    // fused sorted step: per (class, cell) counts then group offsets, block
+    // table, new per-cell counts and scan scratch (per species, so that the
+    // second passes of all species run after all first passes)
+    DevBuf<unsigned> cls_count, cls_first, newcount, scan_tmp1, scan_tmp2;
 };
 
 struct SortScratch {
@@ -57,11 +61,27 @@ struct psum_pic_ctx {
     psum_b200::DevBuf<double> partials;
     psum_b200::DevBuf<long long> ipartials;
     psum_b200::SortScratch sort;
-    psum_b200::DevBuf<unsigned> cls_count;    // per (cell, move class) counts, then group offsets, of the fused sorted step
-    psum_b200::DevBuf<unsigned> cls_first;    // first cell owned by each block of the fused sorted step
-    psum_b200::DevBuf<unsigned> newcount;     // per new cell counts (n_cells + 1)
-    psum_b200::DevBuf<unsigned> scan_tmp1, scan_tmp2;
     psum_b200::DevBuf<int> far_flag;          // per species: a particle moved more than one cell on an axis
+    // The second passes of a fused step run on `side` after the first passes
+    // (event ev_pass1) and overlap what the caller enqueues next on the
+    // context stream (the next step's charge density and Poisson solve,
+    // which need only the first passes' deposit).  `pending` until joined:
+    // the context stream then waits for ev_pass2 and the host finishes the
+    // step (buffer swap, or the general path of a species whose particle
+    // moved more than one cell, with the step's dt, pusher and B kept here).
+    cudaStream_t side = nullptr;              // least priority
+    cudaEvent_t ev_pass1 = nullptr, ev_pass2 = nullptr;
+    // A step's charge density and solve run on `prio` (greatest priority),
+    // ordered after the context stream (ev_in) and before it (ev_out), so
+    // that their blocks are scheduled ahead of a pending second pass.
+    cudaStream_t prio = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    int* far_host = nullptr;                  // pinned copy of far_flag
+    bool pending = false;
+    double pend_dt = 0;
+    int pend_pusher = 0;
+    bool pend_has_B = false;
+    double pend_B[3] = {0, 0, 0};
     int sort_interval = 1;
     long long steps = 0;
     bool timing = false;
@@ -78,14 +98,28 @@ struct psum_pic_ctx {
     psum_b200::DevBuf<double> adj_scale;
     psum_b200::DevBuf<unsigned> adj_max;
     ~psum_pic_ctx() {
+        if (side) cudaStreamSynchronize(side);
         drop_events();
+        if (ev_pass1) cudaEventDestroy(ev_pass1);
+        if (ev_pass2) cudaEventDestroy(ev_pass2);
+        if (ev_in) cudaEventDestroy(ev_in);
+        if (ev_out) cudaEventDestroy(ev_out);
+        if (prio) {
+            cudaStreamSynchronize(prio);
+            cudaStreamDestroy(prio);
+        }
+        if (far_host) cudaFreeHost(far_host);
+        if (side) cudaStreamDestroy(side);
         if (own_stream) cudaStreamDestroy(own_stream);
     }
 };
 
 namespace psum_b200 {
-// pic.cu: handle and index checks, and the key fill of a sorted mixed state
+// pic.cu: handle and index checks (ctx_check also joins a pending fused
+// step; ctx_check_nojoin leaves it running), and the key fill of a sorted
+// mixed state
 psum_pic_ctx* ctx_check(psum_pic_ctx* c);
+psum_pic_ctx* ctx_check_nojoin(psum_pic_ctx* c);
 Species& species_at(psum_pic_ctx* c, int s);
 void ensure_keys(psum_pic_ctx* c, Species& sp);
 }  // namespace psum_b200

@@ -129,6 +129,11 @@ class ParticleContext:
         check(lib().psum_pic_get_losses(self.handle, _ptr(out), int(reset)))
         return out.reshape(len(self.species), self.dim, 2)
 
+    def join(self):
+        """Order the context's stream after the last step's deferred second
+        pass (see psum_pic_join); the state readers do this themselves."""
+        check(lib().psum_pic_join(self.handle))
+
     def step(self, solver, background, rho, phi, dt, pusher=LEAPFROG, B=(0.0, 0.0, 0.0)):
         Bv = (C.c_double * 3)(*B)
         self._order(rho, phi)
