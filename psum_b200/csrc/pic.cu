@@ -442,6 +442,9 @@ constexpr int kClsRounds = 4;       // rounds of 32 particles per warp iteration
 // Particles per block: 2D blocks cover a few tens of cells of one row; 3D
 // blocks stay short enough that their node box usually fits the tile.
 __host__ __device__ constexpr int cls_block_particles(int dim) { return dim == 2 ? 8192 : 2048; }
+// Second-pass blocks are short (no node tile to amortise), so that a pending
+// second pass frees SM slots often for the higher-priority work beside it.
+__host__ __device__ constexpr int cls_block_particles2(int) { return 2048; }
 
 template <int D>
 struct MoveClasses {
@@ -1668,9 +1671,10 @@ static void sort_all(psum_pic_ctx* c) {
 // than one cell along an axis take the general path (in-place push, radix
 // sort) for this step; their deposit from pass 1 stands.
 static long long cls_blocks(long long n, int dim) { return n / cls_block_particles(dim) + 1; }
+static long long cls_blocks2(long long n, int dim) { return n / cls_block_particles2(dim) + 1; }
 
 static void launch_pass(const ClsArgs& a, int dim, int pusher, int pass, long long n, cudaStream_t s) {
-    const unsigned blocks = (unsigned)cls_blocks(n, dim);
+    const unsigned blocks = (unsigned)(pass == 1 ? cls_blocks(n, dim) : cls_blocks2(n, dim));
 #define PSUM_PASS(D_, P_) \
     do { \
         if (pass == 1) { k_cls_pass1<D_, P_><<<blocks, kPicThreads, 0, s>>>(a); count_launch(); } \
@@ -1699,6 +1703,7 @@ static void ensure_cls_buffers(psum_pic_ctx* c) {
         if (sp.n <= 0) continue;
         grow(sp.cls_count, (size_t)nc * ncls);
         grow(sp.cls_first, (size_t)cls_blocks(sp.n, c->g.dim) + 1);
+        grow(sp.cls_first2, (size_t)cls_blocks2(sp.n, c->g.dim) + 1);
         grow(sp.newcount, (size_t)nc + 1);
         grow(sp.scan_tmp1, (size_t)(nc + 1 + kScanBlock - 1) / kScanBlock + 1);
         grow(sp.scan_tmp2, 16);
@@ -1758,6 +1763,9 @@ static void cls_step(psum_pic_ctx* c, const double* phi, double dt, int pusher, 
         { k_cls_blocks<<<blocks_for(std::max(nc, nb) + 1, 256), 256, 0, s>>>(a.starts, nc, nb, cls_block_particles(c->g.dim),
                                                                              sp.cls_first.p); count_launch(); }
         launch_pass(a, c->g.dim, pusher, 1, sp.n, s);
+        const long long nb2 = cls_blocks2(sp.n, c->g.dim);
+        { k_cls_blocks<<<blocks_for(std::max(nc, nb2) + 1, 256), 256, 0, s>>>(a.starts, nc, nb2, cls_block_particles2(c->g.dim),
+                                                                              sp.cls_first2.p); count_launch(); }
         if (c->g.dim == 2) { k_cls_offsets<2><<<blocks_for(nc + 1, 256), 256, 0, s>>>(c->g, sp.cls_count.p, sp.newcount.p, nc); count_launch(); }
         else { k_cls_offsets<3><<<blocks_for(nc + 1, 256), 256, 0, s>>>(c->g, sp.cls_count.p, sp.newcount.p, nc); count_launch(); }
         exclusive_scan_u32(sp.newcount.p, sp.starts[1 - sp.starts_cur].p, nc + 1, sp.scan_tmp1.p, sp.scan_tmp2.p, s);
@@ -1771,8 +1779,11 @@ static void cls_step(psum_pic_ctx* c, const double* phi, double dt, int pusher, 
         cuda_check(cudaEventCreate(&t1), "cudaEventCreate");
         cuda_check(cudaEventRecord(t0, c->side), "cudaEventRecord");
     }
-    for (int si = 0; si < ns; ++si)
-        if (c->sp[si]->n > 0) launch_pass(args[si], c->g.dim, pusher, 2, c->sp[si]->n, c->side);
+    for (int si = 0; si < ns; ++si) {
+        if (c->sp[si]->n <= 0) continue;
+        args[si].block_first = c->sp[si]->cls_first2.p;
+        launch_pass(args[si], c->g.dim, pusher, 2, c->sp[si]->n, c->side);
+    }
     if (c->timing) {
         cuda_check(cudaEventRecord(t1, c->side), "cudaEventRecord");
         c->events.push_back({2 | kPhaseContinued, {t0, t1}});   // push phase: the second passes

@@ -35,7 +35,7 @@ struct Species {
     // fused sorted step: per (class, cell) counts then group offsets, block
     // table, new per-cell counts and scan scratch (per species, so that the
     // second passes of all species run after all first passes)
-    DevBuf<unsigned> cls_count, cls_first, newcount, scan_tmp1, scan_tmp2;
+    DevBuf<unsigned> cls_count, cls_first, cls_first2, newcount, scan_tmp1, scan_tmp2;
 };
 
 struct SortScratch {
