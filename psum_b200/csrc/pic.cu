@@ -841,26 +841,26 @@ __global__ void k_cls_offsets(GridView g, unsigned* __restrict__ cls, unsigned* 
     newcount[c] = total;
 }
 
-// Mover slots per class in the pass-2 staging buffer of a warp.
-template <int D>
-struct MoverStage {
-    static constexpr int MS = D == 2 ? 8 : 4;
-    static constexpr int SLOTS = (MoveClasses<D>::N - 1) * MS;
-};
+// Movers a warp stages before writing them out (one list per warp): room for
+// one iteration's 32 * kClsRounds particles above the flush threshold.
+constexpr int kMoverCap = 192;
+constexpr int kMoverFlushAt = kMoverCap - 32 * kClsRounds;
 
+// Pass 2: push again and write the re-sorted state.  A cell's particles that
+// keep their cell are written at once, coalesced (ballot ranks).  Movers are
+// appended to the warp's list in memory order (one ballot per round) and
+// written out 32 at a time when the list is past kMoverFlushAt at the start
+// of an iteration and at the end of the cell: each gets its rank inside its class from match_any, and every
+// class keeps a running next slot (lane k holds the one of class k), so each
+// class's run is written in the old particle order.
 template <int D, int PUSHER>
 __global__ void __launch_bounds__(kPicThreads) k_cls_pass2(ClsArgs a) {
     constexpr int NC = MoveClasses<D>::N;
     constexpr int STAY = MoveClasses<D>::STAY;
-    constexpr int MS = MoverStage<D>::MS;
-    constexpr int SLOTS = MoverStage<D>::SLOTS;
     constexpr int NF = D + 3;   // offsets, then velocities
-    // per (warp, class): global slot of the first staged (or next) particle,
-    // and the number staged; movers are staged per class so that each
-    // class's run is written with consecutive lanes
-    __shared__ unsigned base_w[kClsWarps][NC];
-    __shared__ unsigned fill_w[kClsWarps][NC];
-    __shared__ float stage[kClsWarps][NF][SLOTS];
+    __shared__ float mstage[kClsWarps][NF][kMoverCap];
+    __shared__ int mcls[kClsWarps][kMoverCap];
+    __shared__ unsigned ccount[kClsWarps][32];
     if (*a.far) return;   // some particle moved too far: the caller takes the general path
     const long long ca = a.block_first[blockIdx.x], cb = a.block_first[blockIdx.x + 1];
     const GridView& g = a.p.g;
@@ -869,46 +869,49 @@ __global__ void __launch_bounds__(kPicThreads) k_cls_pass2(ClsArgs a) {
     const unsigned lt = (1u << lane) - 1u;
     unsigned lost_dummy[2 * D] = {};   // losses were counted by pass 1
     auto out_field = [&](int fld) -> float* { return fld < D ? a.off_out[fld] : a.vel_out[fld - D]; };
-    // write every staged mover, class by class, and advance the class bases
-    auto flush = [&]() {
+    unsigned mpos = 0;   // lane k < NC: next slot of move class k in the new state
+    // write the nm staged movers and advance the running slots
+    auto flush = [&](int nm) {
         __syncwarp();
-#pragma unroll
-        for (int s0 = 0; s0 < SLOTS; s0 += 32) {
+        for (int s0 = 0; s0 < nm; s0 += 32) {
             const int s = s0 + lane;
-            if (s < SLOTS) {
-                const int k = s / MS, pos = s - k * MS;
-                const int cls = k < STAY ? k : k + 1;
-                if (pos < (int)fill_w[warp][cls]) {
-                    const unsigned dest = base_w[warp][cls] + pos;
+            const bool has = s < nm;
+            const int k = has ? mcls[warp][s] : -1;
+            const unsigned peers = __match_any_sync(full, k);
+            const unsigned p = __shfl_sync(full, mpos, k & 31);
+            ccount[warp][lane] = 0u;
+            __syncwarp();
+            if (has) {
+                const unsigned dest = p + (unsigned)__popc(peers & lt);
 #pragma unroll
-                    for (int fld = 0; fld < NF; ++fld) out_field(fld)[dest] = stage[warp][fld][s];
-                }
+                for (int fld = 0; fld < NF; ++fld) out_field(fld)[dest] = mstage[warp][fld][s];
+                if (lane == __ffs(peers) - 1) ccount[warp][k] = (unsigned)__popc(peers);
             }
+            __syncwarp();
+            mpos += ccount[warp][lane];
+            __syncwarp();
         }
-        __syncwarp();
-        if (lane < NC && lane != STAY) {
-            base_w[warp][lane] += fill_w[warp][lane];
-            fill_w[warp][lane] = 0u;
-        }
-        __syncwarp();
     };
     for (long long c = ca + warp; c < cb; c += kClsWarps) {
         const long long p0 = a.starts[c], p1 = a.starts[c + 1];
         if (p1 == p0) continue;
         int co[3];
         key_to_cell(g, (int)c, co[0], co[1], co[2]);
+        mpos = 0;
         if (lane < NC) {
             int cn[3];
-            fill_w[warp][lane] = 0u;
             if (class_target<D>(g, co, lane, cn))
-                base_w[warp][lane] = __ldg(a.new_starts + cell_to_key(g, cn[0], cn[1], cn[2])) +
-                                     __ldg(a.cls + lane * a.n_cells + c);
+                mpos = __ldg(a.new_starts + cell_to_key(g, cn[0], cn[1], cn[2])) + __ldg(a.cls + lane * a.n_cells + c);
         }
         CellField<D> F;
         load_cell_field<D>(a.p, co[0], co[1], co[2], F);
-        __syncwarp();
-        unsigned stay_next = base_w[warp][STAY];   // next slot of the class that keeps its cell
+        unsigned stay_next = __shfl_sync(full, mpos, STAY);   // next slot of the class that keeps its cell
+        int nm = 0;
         for (long long base = p0; base < p1; base += 32 * kClsRounds) {
+            if (nm > kMoverFlushAt) {
+                flush(nm);
+                nm = 0;
+            }
             float f[kClsRounds][3], v[kClsRounds][3];
             bool live[kClsRounds];
 #pragma unroll
@@ -938,40 +941,22 @@ __global__ void __launch_bounds__(kPicThreads) k_cls_pass2(ClsArgs a) {
                 }
                 stay_next += (unsigned)__popc(stay);
                 const bool mover = cls >= 0 && cls != STAY;
-                if (__any_sync(full, mover)) {
-                    const unsigned peers = __match_any_sync(full, cls);
-                    const unsigned gsize = (unsigned)__popc(peers), rank = (unsigned)__popc(peers & lt);
-                    // a group larger than the class's slots is written directly, after
-                    // whatever of its class is staged; otherwise flush when it would not fit
-                    const bool direct = gsize > (unsigned)MS;
-                    if (__any_sync(full, mover && (direct ? fill_w[warp][cls] > 0u
-                                                          : fill_w[warp][cls] + gsize > (unsigned)MS)))
-                        flush();
+                const unsigned mb = __ballot_sync(full, mover);
+                if (mb) {
+                    const int cnt = __popc(mb);
                     if (mover) {
-                        if (direct) {
-                            const unsigned dest = base_w[warp][cls] + rank;   // nothing of the class staged
+                        const int slot = nm + __popc(mb & lt);
 #pragma unroll
-                            for (int d = 0; d < D; ++d) a.off_out[d][dest] = f[r][d];
+                        for (int d = 0; d < D; ++d) mstage[warp][d][slot] = f[r][d];
 #pragma unroll
-                            for (int q = 0; q < 3; ++q) a.vel_out[q][dest] = v[r][q];
-                        } else {
-                            const int slot = (cls < STAY ? cls : cls - 1) * MS + (int)(fill_w[warp][cls] + rank);
-#pragma unroll
-                            for (int d = 0; d < D; ++d) stage[warp][d][slot] = f[r][d];
-#pragma unroll
-                            for (int q = 0; q < 3; ++q) stage[warp][D + q][slot] = v[r][q];
-                        }
+                        for (int q = 0; q < 3; ++q) mstage[warp][D + q][slot] = v[r][q];
+                        mcls[warp][slot] = cls;
                     }
-                    __syncwarp();
-                    if (mover && lane == __ffs(peers) - 1) {
-                        if (direct) base_w[warp][cls] += gsize;
-                        else fill_w[warp][cls] += gsize;
-                    }
-                    __syncwarp();
+                    nm += cnt;
                 }
             }
         }
-        flush();
+        if (nm) flush(nm);
     }
 }
 
