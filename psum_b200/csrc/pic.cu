@@ -510,12 +510,16 @@ struct NodeTile {
     int vol;
 };
 
-// Node box touched by particles of the block's cells after one move (cells
-// +-1, nodes +2), clamped to the node lattice.  Wrap-around nodes fall
-// outside the box and take the direct global path.
+// Cells a block's deposit may reach (its cells +-1 on every axis, the reach
+// of a one-cell move; for a block spanning several rows the full rows),
+// clamped to the cell lattice, and the nodes of those cells.  Targets across
+// a periodic seam and boxes above the tile capacities take the direct
+// global path.
 template <int D>
-__device__ void node_tile_box(const GridView& g, long long ca, long long cb, NodeTile& t) {
-    t.on = 0;
+__device__ void deposit_boxes(const GridView& g, long long ca, long long cb, int cell_cap, int node_cap, NodeTile& ct,
+                              NodeTile& nt) {
+    ct.on = nt.on = 0;
+    ct.vol = nt.vol = 0;
     if (ca >= cb) return;
     int a[3], b[3];
     key_to_cell(g, (int)ca, a[0], a[1], a[2]);
@@ -535,20 +539,45 @@ __device__ void node_tile_box(const GridView& g, long long ca, long long cb, Nod
             hi[2] = b[2];
         }
     }
-    long long vol = 1;
+    long long cvol = 1, nvol = 1;
     for (int q = 0; q < 3; ++q) {
         if (q < D) {
-            t.lo[q] = max(lo[q] - 1, 0);
-            const int top = min(hi[q] + 2, g.N[q] - 1);
-            t.ext[q] = top - t.lo[q] + 1;
+            ct.lo[q] = nt.lo[q] = max(lo[q] - 1, 0);
+            ct.ext[q] = min(hi[q] + 1, g.M[q] - 1) - ct.lo[q] + 1;
+            nt.ext[q] = min(ct.lo[q] + ct.ext[q], g.N[q] - 1) - nt.lo[q] + 1;
         } else {
-            t.lo[q] = 0;
-            t.ext[q] = 1;
+            ct.lo[q] = nt.lo[q] = 0;
+            ct.ext[q] = nt.ext[q] = 1;
         }
-        vol *= t.ext[q];
+        cvol *= ct.ext[q];
+        nvol *= nt.ext[q];
     }
-    t.on = vol <= kClsTileMax;
-    t.vol = t.on ? (int)vol : 0;
+    ct.on = cvol <= cell_cap;
+    ct.vol = ct.on ? (int)cvol : 0;
+    nt.on = ct.on && nvol <= node_cap;
+    nt.vol = nt.on ? (int)nvol : 0;
+}
+
+// Slot of cell c in a box, or -1 outside it.
+__device__ __forceinline__ int box_slot(const NodeTile& t, const int c[3]) {
+    const int i = c[0] - t.lo[0], j = c[1] - t.lo[1], k = c[2] - t.lo[2];
+    if (!t.on || (unsigned)i >= (unsigned)t.ext[0] || (unsigned)j >= (unsigned)t.ext[1] || (unsigned)k >= (unsigned)t.ext[2])
+        return -1;
+    return (i * t.ext[1] + j) * t.ext[2] + k;
+}
+
+// Corners of moment sums W (W[0] = count * 2^26) of cell c straight into the
+// node accumulators.
+template <int D>
+__device__ __forceinline__ void deposit_direct(const PushArgs& a, const int c[3], const long long W[8]) {
+#pragma unroll
+    for (int B = 0; B < (1 << D); ++B) {
+        const long long w = cic_corner<D>(W, B);
+        if (w == 0) continue;
+        int nd[3];
+        corner_node<D>(a.g, B, c, nd);
+        atomicAdd(a.acc + node_index(a.g, nd[0], nd[1], nd[2]), (unsigned long long)w << a.dep_lsh);
+    }
 }
 
 // Push of one particle of cell co with the warp's cell field: move class
@@ -619,31 +648,54 @@ __device__ __forceinline__ unsigned long long pair64(unsigned lo, unsigned hi) {
     return (unsigned long long)lo | ((unsigned long long)hi << 32);
 }
 
+// Cells of the pass-1 moment tile and nodes of its node tile: the boxes of a
+// 2D block (one row segment +-1) and of a 3D block (a z-run +-1 in x and y;
+// 2048 particles at 32 per cell span 64 cells: 3 x 3 x 66 cells).  The tiles
+// live in dynamic shared memory (above the 48 KB static limit in 3D).
+template <int D>
+struct CellTileCap {
+    static constexpr int N = D == 2 ? 384 : 600;
+    static constexpr int NODES = D == 2 ? kClsTileMax : 1100;
+    // dynamic shared memory of pass 1: cell counts, moment low/high words, node tile
+    static constexpr size_t BYTES = sizeof(unsigned) * ((size_t)N * (1 + 2 * ((1 << D) - 1)) + 2 * (size_t)NODES);
+};
+
 template <int D, int PUSHER>
 __global__ void __launch_bounds__(kPicThreads) k_cls_pass1(ClsArgs a) {
     constexpr int NC = MoveClasses<D>::N;
     constexpr int STAY = MoveClasses<D>::STAY;
     constexpr int NM = 1 << D;
+    constexpr int CT = CellTileCap<D>::N;
+    constexpr int NT = CellTileCap<D>::NODES;
     // per (warp, moment, class): count (moment 0, low word only) and moment
-    // sums of the current cell; block node tile in units of 2^-26
+    // sums of the warp's current cell; per cell of the block's box the count
+    // and moment sums (units of 2^-26) of the particles that end there; the
+    // box's node tile
     __shared__ unsigned mom_lo[kClsWarps][NM][NC], mom_hi[kClsWarps][NM][NC];
-    __shared__ unsigned tile_lo[kClsTileMax], tile_hi[kClsTileMax];
-    __shared__ NodeTile box;
+    __shared__ NodeTile cbox, nbox;
+    extern __shared__ __align__(16) unsigned dsm[];
+    unsigned* const ct_n = dsm;                             // [CT]
+    unsigned(*const ct_lo)[CT] = reinterpret_cast<unsigned(*)[CT]>(dsm + CT);   // [NM - 1][CT]
+    unsigned(*const ct_hi)[CT] = reinterpret_cast<unsigned(*)[CT]>(dsm + CT + (NM - 1) * CT);
+    unsigned* const tile_lo = dsm + CT + 2 * (NM - 1) * CT;  // [NT]
+    unsigned* const tile_hi = tile_lo + NT;
     const long long ca = a.block_first[blockIdx.x], cb = a.block_first[blockIdx.x + 1];
     if (ca >= cb) return;
     const GridView& g = a.p.g;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned full = 0xffffffffu;
-    if (threadIdx.x == 0) node_tile_box<D>(g, ca, cb, box);
+    if (threadIdx.x == 0) deposit_boxes<D>(g, ca, cb, CT, NT, cbox, nbox);
     for (int q = threadIdx.x; q < kClsWarps * NM * NC; q += blockDim.x) {
         (&mom_lo[0][0][0])[q] = 0u;
         (&mom_hi[0][0][0])[q] = 0u;
     }
     __syncthreads();
-    for (int q = threadIdx.x; q < box.vol; q += blockDim.x) {
-        tile_lo[q] = 0u;
-        tile_hi[q] = 0u;
+    for (int q = threadIdx.x; q < cbox.vol; q += blockDim.x) {
+        ct_n[q] = 0u;
+#pragma unroll
+        for (int m = 0; m < NM - 1; ++m) ct_lo[m][q] = ct_hi[m][q] = 0u;
     }
+    for (int q = threadIdx.x; q < nbox.vol; q += blockDim.x) tile_lo[q] = tile_hi[q] = 0u;
     __syncthreads();
     unsigned lost_cnt[2 * D];
 #pragma unroll
@@ -699,15 +751,7 @@ __global__ void __launch_bounds__(kPicThreads) k_cls_pass1(ClsArgs a) {
                         long long W[8];
 #pragma unroll
                         for (int m = 0; m < NM; ++m) W[m] = q[m];
-#pragma unroll
-                        for (int B = 0; B < NM; ++B) {
-                            const long long w = cic_corner<D>(W, B);
-                            if (w == 0) continue;
-                            int nd[3];
-                            corner_node<D>(g, B, cn, nd);
-                            atomicAdd(a.p.acc + node_index(g, nd[0], nd[1], nd[2]),
-                                      (unsigned long long)w << a.p.dep_lsh);
-                        }
+                        deposit_direct<D>(a.p, cn, W);
                     }
                 }
                 if (++pending == 32 / kClsRounds || base + 32 * kClsRounds >= p1) {
@@ -726,38 +770,31 @@ __global__ void __launch_bounds__(kPicThreads) k_cls_pass1(ClsArgs a) {
             }
         }
         __syncwarp();
-        // class lanes: count out, corner sums of the class into the node tile
-        // (for a fixed corner the classes reach distinct nodes: no conflicts)
+        // class lanes: count out, the class's moment sums into its target cell
         if (lane < NC) {
             const unsigned n = mom_lo[warp][0][lane];
             a.cls[lane * a.n_cells + c] = n;
             if (n) {
-                long long W[8];
-                W[0] = (long long)n << kCicBits;
                 mom_lo[warp][0][lane] = 0u;
-                mom_hi[warp][0][lane] = 0u;
-#pragma unroll
-                for (int m = 1; m < NM; ++m) {
-                    W[m] = (long long)pair64(mom_lo[warp][m][lane], mom_hi[warp][m][lane]);
-                    mom_lo[warp][m][lane] = 0u;
-                    mom_hi[warp][m][lane] = 0u;
-                }
                 int cn[3];
                 class_target<D>(g, co, lane, cn);   // inside: the class holds no absorbed particle
+                const int sl = box_slot(cbox, cn);
+                if (sl >= 0) {
+                    atomicAdd(&ct_n[sl], n);
 #pragma unroll
-                for (int B = 0; B < NM; ++B) {
-                    const long long w = cic_corner<D>(W, B);
-                    if (w == 0) continue;
-                    int nd[3];
-                    corner_node<D>(g, B, cn, nd);
-                    const int ti = nd[0] - box.lo[0], tj = nd[1] - box.lo[1], tk = nd[2] - box.lo[2];
-                    if (box.on && (unsigned)ti < (unsigned)box.ext[0] && (unsigned)tj < (unsigned)box.ext[1] &&
-                        (unsigned)tk < (unsigned)box.ext[2]) {
-                        const int t = (ti * box.ext[1] + tj) * box.ext[2] + tk;
-                        smem_add64(&tile_lo[t], &tile_hi[t], (unsigned long long)w);
-                    } else {
-                        atomicAdd(a.p.acc + node_index(g, nd[0], nd[1], nd[2]), (unsigned long long)w << a.p.dep_lsh);
+                    for (int m = 1; m < NM; ++m) {
+                        smem_add64(&ct_lo[m - 1][sl], &ct_hi[m - 1][sl], pair64(mom_lo[warp][m][lane], mom_hi[warp][m][lane]));
+                        mom_lo[warp][m][lane] = mom_hi[warp][m][lane] = 0u;
                     }
+                } else {
+                    long long W[8];
+                    W[0] = (long long)n << kCicBits;
+#pragma unroll
+                    for (int m = 1; m < NM; ++m) {
+                        W[m] = (long long)pair64(mom_lo[warp][m][lane], mom_hi[warp][m][lane]);
+                        mom_lo[warp][m][lane] = mom_hi[warp][m][lane] = 0u;
+                    }
+                    deposit_direct<D>(a.p, cn, W);
                 }
             }
         }
@@ -771,13 +808,39 @@ __global__ void __launch_bounds__(kPicThreads) k_cls_pass1(ClsArgs a) {
         if (lane == 0 && t) atomicAdd(a.p.losses + q, (unsigned long long)t);
     }
     __syncthreads();
-    const int e2 = box.ext[2], e12 = box.ext[1] * box.ext[2];
-    for (int q = threadIdx.x; q < box.vol; q += blockDim.x) {
+    // corners of every box cell once, into the node tile
+    {
+        const int e2 = cbox.ext[2], e12 = cbox.ext[1] * cbox.ext[2];
+        for (int q = threadIdx.x; q < cbox.vol; q += blockDim.x) {
+            const unsigned n = ct_n[q];
+            if (n == 0u) continue;
+            long long W[8];
+            W[0] = (long long)n << kCicBits;
+#pragma unroll
+            for (int m = 1; m < NM; ++m) W[m] = (long long)pair64(ct_lo[m - 1][q], ct_hi[m - 1][q]);
+            const int ti = q / e12, r = q - ti * e12;
+            const int tj = r / e2;
+            const int cc[3] = {ti + cbox.lo[0], tj + cbox.lo[1], r - tj * e2 + cbox.lo[2]};
+#pragma unroll
+            for (int B = 0; B < NM; ++B) {
+                const long long w = cic_corner<D>(W, B);
+                if (w == 0) continue;
+                int nd[3];
+                corner_node<D>(g, B, cc, nd);
+                const int sl = box_slot(nbox, nd);
+                if (sl >= 0) smem_add64(&tile_lo[sl], &tile_hi[sl], (unsigned long long)w);
+                else atomicAdd(a.p.acc + node_index(g, nd[0], nd[1], nd[2]), (unsigned long long)w << a.p.dep_lsh);
+            }
+        }
+    }
+    __syncthreads();
+    const int e2 = nbox.ext[2], e12 = nbox.ext[1] * nbox.ext[2];
+    for (int q = threadIdx.x; q < nbox.vol; q += blockDim.x) {
         const unsigned long long val = pair64(tile_lo[q], tile_hi[q]);
         if (val == 0ull) continue;
         const int ti = q / e12, r = q - ti * e12;
         const int tj = r / e2, tk = r - tj * e2;
-        atomicAdd(a.p.acc + node_index(g, ti + box.lo[0], tj + box.lo[1], tk + box.lo[2]), val << a.p.dep_lsh);
+        atomicAdd(a.p.acc + node_index(g, ti + nbox.lo[0], tj + nbox.lo[1], tk + nbox.lo[2]), val << a.p.dep_lsh);
     }
 }
 
@@ -1662,7 +1725,16 @@ static void launch_pass(const ClsArgs& a, int dim, int pusher, int pass, long lo
     const unsigned blocks = (unsigned)(pass == 1 ? cls_blocks(n, dim) : cls_blocks2(n, dim));
 #define PSUM_PASS(D_, P_) \
     do { \
-        if (pass == 1) { k_cls_pass1<D_, P_><<<blocks, kPicThreads, 0, s>>>(a); count_launch(); } \
+        if (pass == 1) { \
+            constexpr size_t bytes = CellTileCap<D_>::BYTES; \
+            static bool attr = false; \
+            if (!attr) { \
+                cuda_check(cudaFuncSetAttribute(k_cls_pass1<D_, P_>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                                (int)bytes), "cudaFuncSetAttribute"); \
+                attr = true; \
+            } \
+            k_cls_pass1<D_, P_><<<blocks, kPicThreads, bytes, s>>>(a); count_launch(); \
+        } \
         else { k_cls_pass2<D_, P_><<<blocks, kPicThreads, 0, s>>>(a); count_launch(); } \
     } while (0)
     if (dim == 2) {
