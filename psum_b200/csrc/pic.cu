@@ -871,35 +871,40 @@ __global__ void k_cls_offsets(GridView g, unsigned* __restrict__ cls, unsigned* 
         ord[a][1] = seam_lo ? -1 : (seam_hi ? 1 : 0);
         ord[a][2] = seam_lo ? 1 : (seam_hi ? 0 : -1);
     }
-    unsigned total = 0;
+    // all group counts are loaded before the first offset is stored (the
+    // loads and stores address one array, so they would otherwise serialise);
+    // the store loop recomputes each group's index
     constexpr int n1 = D == 3 ? 3 : 1;
+    constexpr int NG = 9 * n1;
+    auto group = [&](int j) -> long long {   // index of the j-th arriving group, -1 when none
+        const int o0 = j / (3 * n1), o1 = (j / n1) % 3, o2 = j % n1;
+        const int st[3] = {ord[0][o0], ord[1][o1], D == 3 ? ord[2][o2] : 0};
+        int src[3] = {cc[0], cc[1], cc[2]};
+        int d = 0;
 #pragma unroll
-    for (int o0 = 0; o0 < 3; ++o0) {
-#pragma unroll
-        for (int o1 = 0; o1 < 3; ++o1) {
-#pragma unroll
-            for (int o2 = 0; o2 < n1; ++o2) {
-                const int st[3] = {ord[0][o0], ord[1][o1], D == 3 ? ord[2][o2] : 0};
-                int src[3] = {cc[0], cc[1], cc[2]};
-                bool ok = true;
-                int d = 0;
-#pragma unroll
-                for (int a = 0; a < D; ++a) {
-                    int x = cc[a] - st[a];
-                    if (x < 0 || x >= g.M[a]) {
-                        if (!g.periodic[a]) ok = false;
-                        x = x < 0 ? x + g.M[a] : x - g.M[a];
-                    }
-                    src[a] = x;
-                    d = d * 3 + st[a] + 1;
-                }
-                if (!ok) continue;
-                const long long idx = (long long)d * n_cells + cell_to_key(g, src[0], src[1], src[2]);
-                const unsigned t = cls[idx];
-                cls[idx] = total;
-                total += t;
+        for (int a = 0; a < D; ++a) {
+            int x = cc[a] - st[a];
+            if (x < 0 || x >= g.M[a]) {
+                if (!g.periodic[a]) return -1;
+                x = x < 0 ? x + g.M[a] : x - g.M[a];
             }
+            src[a] = x;
+            d = d * 3 + st[a] + 1;
         }
+        return (long long)d * n_cells + cell_to_key(g, src[0], src[1], src[2]);
+    };
+    unsigned cnt[NG];
+#pragma unroll
+    for (int j = 0; j < NG; ++j) {
+        const long long i = group(j);
+        cnt[j] = i >= 0 ? __ldg(cls + i) : 0u;
+    }
+    unsigned total = 0;
+#pragma unroll
+    for (int j = 0; j < NG; ++j) {
+        const long long i = group(j);
+        if (i >= 0) cls[i] = total;
+        total += cnt[j];
     }
     newcount[c] = total;
 }
