@@ -441,10 +441,12 @@ constexpr int kClsRounds = 4;       // rounds of 32 particles per warp iteration
 
 // Particles per block: 2D blocks cover a few tens of cells of one row; 3D
 // blocks stay short enough that their node box usually fits the tile.
-__host__ __device__ constexpr int cls_block_particles(int dim) { return dim == 2 ? 8192 : 2048; }
+__host__ __device__ constexpr int cls_block_lg(int dim) { return dim == 2 ? 13 : 11; }
+__host__ __device__ constexpr int cls_block_particles(int dim) { return 1 << cls_block_lg(dim); }
 // Second-pass blocks are short (no node tile to amortise), so that a pending
 // second pass frees SM slots often for the higher-priority work beside it.
-__host__ __device__ constexpr int cls_block_particles2(int) { return 2048; }
+__host__ __device__ constexpr int cls_block_lg2(int) { return 11; }
+__host__ __device__ constexpr int cls_block_particles2(int dim) { return 1 << cls_block_lg2(dim); }
 
 template <int D>
 struct MoveClasses {
@@ -493,15 +495,16 @@ __device__ __forceinline__ bool class_target(const GridView& g, const int c[3], 
 
 // Block -> first owned cell: first[b] = lower bound of b*T in starts,
 // clamped to n_cells; entries 0..nb.
-__global__ void k_cls_blocks(const unsigned* __restrict__ starts, long long n_cells, long long nb, long long T,
+// (T = 2^lgT particles per block.)
+__global__ void k_cls_blocks(const unsigned* __restrict__ starts, long long n_cells, long long nb, int lgT,
                              unsigned* __restrict__ first) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t <= n_cells) {
-        const long long hi = (long long)starts[t] / T;
-        for (long long b = t == 0 ? 0 : (long long)starts[t - 1] / T + 1; b <= hi && b <= nb; ++b)
+        const long long hi = (long long)(starts[t] >> lgT);
+        for (long long b = t == 0 ? 0 : (long long)(starts[t - 1] >> lgT) + 1; b <= hi && b <= nb; ++b)
             first[b] = (unsigned)t;
     }
-    if (t <= nb && t * T > (long long)starts[n_cells]) first[t] = (unsigned)n_cells;
+    if (t <= nb && (t << lgT) > (long long)starts[n_cells]) first[t] = (unsigned)n_cells;
 }
 
 struct NodeTile {
@@ -1176,6 +1179,37 @@ __global__ void k_scan_blocks(const unsigned* __restrict__ in, unsigned* __restr
     if (t == 255) totals[blockIdx.x] = sh[255];
 }
 
+// The same scan in place: every thread reads its 4 values before the
+// block's first write, and writes only those.
+__global__ void k_scan_blocks_inplace(unsigned* v_io, long long n, unsigned* __restrict__ totals) {
+    __shared__ unsigned sh[kScanBlock];
+    const long long base = (long long)blockIdx.x * kScanBlock;
+    const int t = threadIdx.x;
+    unsigned v[4], s = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const long long i = base + t * 4 + q;
+        v[q] = i < n ? v_io[i] : 0u;
+        s += v[q];
+    }
+    sh[t] = s;
+    __syncthreads();
+    for (int d = 1; d < 256; d <<= 1) {
+        const unsigned add = t >= d ? sh[t - d] : 0u;
+        __syncthreads();
+        sh[t] += add;
+        __syncthreads();
+    }
+    unsigned run = sh[t] - s;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const long long i = base + t * 4 + q;
+        if (i < n) v_io[i] = run;
+        run += v[q];
+    }
+    if (t == 255) totals[blockIdx.x] = sh[255];
+}
+
 __global__ void k_scan_add(unsigned* __restrict__ out, long long n, const unsigned* __restrict__ offsets) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] += offsets[i / kScanBlock];
@@ -1210,17 +1244,22 @@ __global__ void k_scan_single(unsigned* __restrict__ v, long long n) {
 // exclusive scan (uint32), `tmp1`/`tmp2` scratch of ceil(n/1024) and
 // ceil(n/1024^2) entries
 void exclusive_scan_u32(const unsigned* in, unsigned* out, long long n, unsigned* tmp1, unsigned* tmp2,
-                        cudaStream_t s) {
+                        cudaStream_t s, long long tmp2_cap = 0) {
     if (n <= 0) return;
     const long long nb = (n + kScanBlock - 1) / kScanBlock;
     { k_scan_blocks<<<(unsigned)nb, 256, 0, s>>>(in, out, n, tmp1); count_launch(); }
     if (nb > 1) {
-        if (nb <= 4 * 1024 * 1024) {
+        const long long nb2 = (nb + kScanBlock - 1) / kScanBlock;
+        if (nb > 4 * kScanBlock && tmp2 && nb2 <= tmp2_cap) {
+            // many block totals: scan them by blocks too (in place), then their totals
+            { k_scan_blocks_inplace<<<(unsigned)nb2, 256, 0, s>>>(tmp1, nb, tmp2); count_launch(); }
+            { k_scan_single<<<1, 1024, 0, s>>>(tmp2, nb2); count_launch(); }
+            { k_scan_add<<<blocks_for(nb, 256), 256, 0, s>>>(tmp1, nb, tmp2); count_launch(); }
+        } else if (nb <= 4 * 1024 * 1024) {
             { k_scan_single<<<1, 1024, 0, s>>>(tmp1, nb); count_launch(); }
         } else {
             throw Error(PSUM_ERR_INVALID_ARGUMENT, "scan: input too large");
         }
-        (void)tmp2;
         { k_scan_add<<<blocks_for(n, 256), 256, 0, s>>>(out, n, tmp1); count_launch(); }
     }
 }
@@ -1768,7 +1807,7 @@ static void ensure_cls_buffers(psum_pic_ctx* c) {
         grow(sp.cls_first2, (size_t)cls_blocks2(sp.n, c->g.dim) + 1);
         grow(sp.newcount, (size_t)nc + 1);
         grow(sp.scan_tmp1, (size_t)(nc + 1 + kScanBlock - 1) / kScanBlock + 1);
-        grow(sp.scan_tmp2, 16);
+        grow(sp.scan_tmp2, (size_t)((nc + 1 + kScanBlock - 1) / kScanBlock + kScanBlock - 1) / kScanBlock + 16);
     }
     grow(c->far_flag, 8);
     if (!c->side) {
@@ -1822,15 +1861,16 @@ static void cls_step(psum_pic_ctx* c, const double* phi, double dt, int pusher, 
         }
         a.n_cells = nc;
         const long long nb = cls_blocks(sp.n, c->g.dim);
-        { k_cls_blocks<<<blocks_for(std::max(nc, nb) + 1, 256), 256, 0, s>>>(a.starts, nc, nb, cls_block_particles(c->g.dim),
+        { k_cls_blocks<<<blocks_for(std::max(nc, nb) + 1, 256), 256, 0, s>>>(a.starts, nc, nb, cls_block_lg(c->g.dim),
                                                                              sp.cls_first.p); count_launch(); }
         launch_pass(a, c->g.dim, pusher, 1, sp.n, s);
         const long long nb2 = cls_blocks2(sp.n, c->g.dim);
-        { k_cls_blocks<<<blocks_for(std::max(nc, nb2) + 1, 256), 256, 0, s>>>(a.starts, nc, nb2, cls_block_particles2(c->g.dim),
+        { k_cls_blocks<<<blocks_for(std::max(nc, nb2) + 1, 256), 256, 0, s>>>(a.starts, nc, nb2, cls_block_lg2(c->g.dim),
                                                                               sp.cls_first2.p); count_launch(); }
         if (c->g.dim == 2) { k_cls_offsets<2><<<blocks_for(nc + 1, 256), 256, 0, s>>>(c->g, sp.cls_count.p, sp.newcount.p, nc); count_launch(); }
         else { k_cls_offsets<3><<<blocks_for(nc + 1, 256), 256, 0, s>>>(c->g, sp.cls_count.p, sp.newcount.p, nc); count_launch(); }
-        exclusive_scan_u32(sp.newcount.p, sp.starts[1 - sp.starts_cur].p, nc + 1, sp.scan_tmp1.p, sp.scan_tmp2.p, s);
+        exclusive_scan_u32(sp.newcount.p, sp.starts[1 - sp.starts_cur].p, nc + 1, sp.scan_tmp1.p, sp.scan_tmp2.p, s,
+                           (long long)sp.scan_tmp2.n);
     }
     cuda_check(cudaMemcpyAsync(c->far_host, c->far_flag.p, sizeof(int) * 8, cudaMemcpyDeviceToHost, s), "D2H");
     cuda_check(cudaEventRecord(c->ev_pass1, s), "cudaEventRecord");
