@@ -924,8 +924,9 @@ constexpr int kMoverFlushAt = kMoverCap - 32 * kClsRounds;
 // of an iteration and at the end of the cell: each gets its rank inside its class from match_any, and every
 // class keeps a running next slot (lane k holds the one of class k), so each
 // class's run is written in the old particle order.
+// (2D: 48 registers, 5 blocks per SM, for more loads in flight.)
 template <int D, int PUSHER>
-__global__ void __launch_bounds__(kPicThreads) k_cls_pass2(ClsArgs a) {
+__global__ void __launch_bounds__(kPicThreads, D == 2 ? 5 : 1) k_cls_pass2(ClsArgs a) {
     constexpr int NC = MoveClasses<D>::N;
     constexpr int STAY = MoveClasses<D>::STAY;
     constexpr int NF = D + 3;   // offsets, then velocities
