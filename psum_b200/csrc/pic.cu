@@ -437,7 +437,11 @@ __global__ void __launch_bounds__(kPicThreads) k_push_mixed(PushArgs a) {
 // flushed with one integer atomic per touched node.
 constexpr int kClsWarps = kPicThreads / 32;
 constexpr int kClsTileMax = 3072;   // int64 node accumulators in shared memory (24 KB)
-constexpr int kClsRounds = 4;       // rounds of 32 particles per warp iteration (all loads issued first)
+// Rounds of 32 particles per warp iteration (all loads issued first): 4, or
+// 1 for species with few particles per cell (empty rounds cost a cell's
+// whole iteration there).
+constexpr int kClsRoundsMax = 4;
+constexpr int cls_rounds(double particles_per_cell) { return particles_per_cell < 64.0 ? 1 : kClsRoundsMax; }
 
 // Particles per block: 2D blocks cover a few tens of cells of one row; 3D
 // blocks stay short enough that their node box usually fits the tile.
@@ -663,7 +667,7 @@ struct CellTileCap {
     static constexpr size_t BYTES = sizeof(unsigned) * ((size_t)N * (1 + 2 * ((1 << D) - 1)) + 2 * (size_t)NODES);
 };
 
-template <int D, int PUSHER>
+template <int D, int PUSHER, int kClsRounds>
 __global__ void __launch_bounds__(kPicThreads) k_cls_pass1(ClsArgs a) {
     constexpr int NC = MoveClasses<D>::N;
     constexpr int STAY = MoveClasses<D>::STAY;
@@ -913,9 +917,8 @@ __global__ void k_cls_offsets(GridView g, unsigned* __restrict__ cls, unsigned* 
 }
 
 // Movers a warp stages before writing them out (one list per warp): room for
-// one iteration's 32 * kClsRounds particles above the flush threshold.
+// one iteration's 32 * rounds particles above the flush threshold.
 constexpr int kMoverCap = 192;
-constexpr int kMoverFlushAt = kMoverCap - 32 * kClsRounds;
 
 // Pass 2: push again and write the re-sorted state.  A cell's particles that
 // keep their cell are written at once, coalesced (ballot ranks).  Movers are
@@ -925,8 +928,9 @@ constexpr int kMoverFlushAt = kMoverCap - 32 * kClsRounds;
 // class keeps a running next slot (lane k holds the one of class k), so each
 // class's run is written in the old particle order.
 // (2D: 48 registers, 5 blocks per SM, for more loads in flight.)
-template <int D, int PUSHER>
+template <int D, int PUSHER, int kClsRounds>
 __global__ void __launch_bounds__(kPicThreads, D == 2 ? 5 : 1) k_cls_pass2(ClsArgs a) {
+    constexpr int kMoverFlushAt = kMoverCap - 32 * kClsRounds;
     constexpr int NC = MoveClasses<D>::N;
     constexpr int STAY = MoveClasses<D>::STAY;
     constexpr int NF = D + 3;   // offsets, then velocities
@@ -1766,30 +1770,38 @@ static void sort_all(psum_pic_ctx* c) {
 static long long cls_blocks(long long n, int dim) { return n / cls_block_particles(dim) + 1; }
 static long long cls_blocks2(long long n, int dim) { return n / cls_block_particles2(dim) + 1; }
 
+template <int D, int P, int R>
+static void launch_pass_t(const ClsArgs& a, int pass, unsigned blocks, cudaStream_t s) {
+    if (pass == 1) {
+        constexpr size_t bytes = CellTileCap<D>::BYTES;
+        static bool attr = false;
+        if (!attr) {
+            cuda_check(cudaFuncSetAttribute(k_cls_pass1<D, P, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes),
+                       "cudaFuncSetAttribute");
+            attr = true;
+        }
+        { k_cls_pass1<D, P, R><<<blocks, kPicThreads, bytes, s>>>(a); count_launch(); }
+    } else {
+        { k_cls_pass2<D, P, R><<<blocks, kPicThreads, 0, s>>>(a); count_launch(); }
+    }
+}
+
+template <int D, int P>
+static void launch_pass_r(const ClsArgs& a, int pass, unsigned blocks, int rounds, cudaStream_t s) {
+    if (rounds == 1) launch_pass_t<D, P, 1>(a, pass, blocks, s);
+    else launch_pass_t<D, P, kClsRoundsMax>(a, pass, blocks, s);
+}
+
 static void launch_pass(const ClsArgs& a, int dim, int pusher, int pass, long long n, cudaStream_t s) {
     const unsigned blocks = (unsigned)(pass == 1 ? cls_blocks(n, dim) : cls_blocks2(n, dim));
-#define PSUM_PASS(D_, P_) \
-    do { \
-        if (pass == 1) { \
-            constexpr size_t bytes = CellTileCap<D_>::BYTES; \
-            static bool attr = false; \
-            if (!attr) { \
-                cuda_check(cudaFuncSetAttribute(k_cls_pass1<D_, P_>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                                (int)bytes), "cudaFuncSetAttribute"); \
-                attr = true; \
-            } \
-            k_cls_pass1<D_, P_><<<blocks, kPicThreads, bytes, s>>>(a); count_launch(); \
-        } \
-        else { k_cls_pass2<D_, P_><<<blocks, kPicThreads, 0, s>>>(a); count_launch(); } \
-    } while (0)
+    const int rounds = cls_rounds((double)n / (double)a.n_cells);
     if (dim == 2) {
-        if (pusher == PSUM_PIC_BORIS) PSUM_PASS(2, PSUM_PIC_BORIS);
-        else PSUM_PASS(2, PSUM_PIC_LEAPFROG);
+        if (pusher == PSUM_PIC_BORIS) launch_pass_r<2, PSUM_PIC_BORIS>(a, pass, blocks, rounds, s);
+        else launch_pass_r<2, PSUM_PIC_LEAPFROG>(a, pass, blocks, rounds, s);
     } else {
-        if (pusher == PSUM_PIC_BORIS) PSUM_PASS(3, PSUM_PIC_BORIS);
-        else PSUM_PASS(3, PSUM_PIC_LEAPFROG);
+        if (pusher == PSUM_PIC_BORIS) launch_pass_r<3, PSUM_PIC_BORIS>(a, pass, blocks, rounds, s);
+        else launch_pass_r<3, PSUM_PIC_LEAPFROG>(a, pass, blocks, rounds, s);
     }
-#undef PSUM_PASS
 }
 
 template <class T>

@@ -375,7 +375,8 @@ def test_load_device_buffers_reusable_immediately():
     assert np.abs(got_vel - vel.astype(np.float32)).max() == 0.0
 
 
-def _fused_vs_general(kind, pusher, dt, seed, vscale=1.0, species=2, sort_general=False, cluster=None, drift=None):
+def _fused_vs_general(kind, pusher, dt, seed, vscale=1.0, species=2, sort_general=False, cluster=None, drift=None,
+                      n=40000):
     """Runs one step on the same sorted state with the fused sorted step
     (sort_interval 1) and with the general path (push in place; with
     sort_general, followed by the stable radix sort); returns both results.
@@ -383,7 +384,7 @@ def _fused_vs_general(kind, pusher, dt, seed, vscale=1.0, species=2, sort_genera
     (per-axis) is added to every velocity."""
     out = []
     for interval in (1, 0):
-        ctx, g, pos, vel, phi = make_case(kind, P.MIXED, seed=seed, n=40000)
+        ctx, g, pos, vel, phi = make_case(kind, P.MIXED, seed=seed, n=n)
         if cluster is not None:
             rng_c = np.random.default_rng(seed + 7)
             centre, sigma = cluster
@@ -518,6 +519,23 @@ def test_fused_step_large_grid():
     # more than 4M cells (172^3): the new cell offsets take the two-level scan
     (fused, loss_f, cnt_f), (gen, loss_g, cnt_g) = _fused_vs_general("3d_large", P.LEAPFROG, 0.12, seed=36,
                                                                       sort_general=True)
+    assert cnt_f == cnt_g
+    for (pf, vf, kf, df), (pg, vg, kg, dg) in zip(fused, gen):
+        assert (kf == kg).all()
+        assert (pf.view(np.int64) == pg.view(np.int64)).all()
+        assert (vf.view(np.int64) == vg.view(np.int64)).all()
+        assert (df.view(np.int64) == dg.view(np.int64)).all()
+
+
+@pytest.mark.parametrize("kind", ["2d_absorb", "3d_periodic"])
+@pytest.mark.parametrize("pusher", [P.LEAPFROG, P.BORIS])
+def test_fused_step_many_particles_per_cell(kind, pusher):
+    # above 64 particles per cell the passes take four rounds per warp
+    # iteration (one round below): both kernel shapes give the stable sort
+    n = 120000 if kind == "2d_absorb" else 400000   # 156 and 98 per cell
+    (fused, loss_f, cnt_f), (gen, loss_g, cnt_g) = _fused_vs_general(kind, pusher, 0.12, seed=37,
+                                                                      sort_general=True, n=n)
+    assert (loss_f == loss_g).all()
     assert cnt_f == cnt_g
     for (pf, vf, kf, df), (pg, vg, kg, dg) in zip(fused, gen):
         assert (kf == kg).all()
