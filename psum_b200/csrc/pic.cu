@@ -753,12 +753,9 @@ __global__ void __launch_bounds__(kPicThreads) k_cls_pass1(ClsArgs a) {
 #pragma unroll
                         for (int m = 1; m < NM; ++m) smem_add64(&mom_lo[warp][m][cls], &mom_hi[warp][m][cls], q[m]);
                     } else if (cls == -1) {
-                        // far mover: own corners, direct atomics; the caller redoes the move
+                        // far mover: flag the species; the caller redoes its move and
+                        // its whole deposit from the re-sorted state
                         atomicOr(a.far, 1);
-                        long long W[8];
-#pragma unroll
-                        for (int m = 0; m < NM; ++m) W[m] = q[m];
-                        deposit_direct<D>(a.p, cn, W);
                     }
                 }
                 if (++pending == 32 / kClsRounds || base + 32 * kClsRounds >= p1) {
@@ -1763,6 +1760,25 @@ static void sort_all(psum_pic_ctx* c) {
     for (int s = 0; s < (int)c->sp.size(); ++s) sort_species(c, *c->sp[s], s);
 }
 
+namespace {
+struct PhaseTimer {
+    psum_pic_ctx* c;
+    int phase;
+    cudaEvent_t a = nullptr, b = nullptr;
+    PhaseTimer(psum_pic_ctx* ctx, int ph) : c(ctx), phase(ph) {
+        if (!c->timing) return;
+        cuda_check(cudaEventCreate(&a), "cudaEventCreate");
+        cuda_check(cudaEventCreate(&b), "cudaEventCreate");
+        cuda_check(cudaEventRecord(a, c->stream), "cudaEventRecord");
+    }
+    void stop() {
+        if (!c->timing) return;
+        cuda_check(cudaEventRecord(b, c->stream), "cudaEventRecord");
+        c->events.push_back({phase, {a, b}});
+    }
+};
+}  // namespace
+
 // One fused sorted step (push + deposit + re-sort) of every species; see
 // k_cls_pass1 / k_cls_pass2.  Species in which some particle moved more
 // than one cell along an axis take the general path (in-place push, radix
@@ -1915,7 +1931,8 @@ static void cls_step(psum_pic_ctx* c, const double* phi, double dt, int pusher, 
 // Joins a pending fused step: the context stream waits for the second
 // passes, and each species either takes its re-sorted state or, when one of
 // its particles moved more than one cell along an axis (its second pass then
-// wrote nothing), moves in place and is radix sorted (no second deposit).
+// wrote nothing and its first pass left far movers out of the deposit),
+// moves in place, is radix sorted and deposited again from the sorted state.
 static void finish_cls_step(psum_pic_ctx* c) {
     if (!c->pending) return;
     c->pending = false;
@@ -1933,12 +1950,19 @@ static void finish_cls_step(psum_pic_ctx* c) {
             sp.keys_stale = true;
             continue;
         }
+        // timed as the sort phase: the cost of a step in which a particle moved too far
+        PhaseTimer t(c, 3);
         ensure_keys(c, sp);
         PushArgs pa = make_push_args(c, sp, si, c->pend_dt, c->pend_pusher, c->pend_has_B ? c->pend_B : nullptr);
         pa.acc = nullptr;
         pa.losses = c->losses.p + 6 * 8;   // discard slot: pass 1 already counted this step's losses
         launch_mixed(pa, c->g.dim, c->pend_pusher, false, sp.n, s);
         sort_species(c, sp, si);
+        cuda_check(cudaMemsetAsync(sp.acc.p, 0, sizeof(unsigned long long) * c->g.n_nodes, s), "memset acc");
+        ensure_keys(c, sp);
+        PushArgs da = make_push_args(c, sp, si, 0.0, 0, nullptr);
+        launch_mixed(da, c->g.dim, 0, true, sp.n, s);
+        t.stop();
     }
     cuda_check(cudaGetLastError(), "fused step finish");
 }
@@ -2400,24 +2424,6 @@ EXPORT int psum_pic_get_losses(psum_pic_ctx* ctx, unsigned long long* losses_hos
     });
 }
 
-namespace {
-struct PhaseTimer {
-    psum_pic_ctx* c;
-    int phase;
-    cudaEvent_t a = nullptr, b = nullptr;
-    PhaseTimer(psum_pic_ctx* ctx, int ph) : c(ctx), phase(ph) {
-        if (!c->timing) return;
-        cuda_check(cudaEventCreate(&a), "cudaEventCreate");
-        cuda_check(cudaEventCreate(&b), "cudaEventCreate");
-        cuda_check(cudaEventRecord(a, c->stream), "cudaEventRecord");
-    }
-    void stop() {
-        if (!c->timing) return;
-        cuda_check(cudaEventRecord(b, c->stream), "cudaEventRecord");
-        c->events.push_back({phase, {a, b}});
-    }
-};
-}  // namespace
 
 EXPORT int psum_pic_step(psum_pic_ctx* ctx, psum_field_solver_handle solver, double background, double* rho_dev,
                          double* phi_dev, double dt, int pusher, const double* B) {
@@ -2433,6 +2439,13 @@ EXPORT int psum_pic_step(psum_pic_ctx* ctx, psum_field_solver_handle solver, dou
             cuda_check(cudaStreamCreateWithPriority(&ctx->prio, cudaStreamNonBlocking, greatest), "cudaStreamCreate");
             cuda_check(cudaEventCreateWithFlags(&ctx->ev_in, cudaEventDisableTiming), "cudaEventCreate");
             cuda_check(cudaEventCreateWithFlags(&ctx->ev_out, cudaEventDisableTiming), "cudaEventCreate");
+        }
+        // a pending step with a far mover finishes first: its deposit is redone
+        if (ctx->pending) {
+            cuda_check(cudaEventSynchronize(ctx->ev_pass1), "far flag wait");
+            bool far = false;
+            for (int si = 0; si < (int)ctx->sp.size() && si < 8; ++si) far |= ctx->far_host[si] != 0;
+            if (far) finish_cls_step(ctx);
         }
         cudaStream_t user = ctx->stream;
         cuda_check(cudaEventRecord(ctx->ev_in, user), "cudaEventRecord");
