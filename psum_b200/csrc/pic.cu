@@ -707,6 +707,7 @@ __global__ void __launch_bounds__(kPicThreads) k_cls_pass1(ClsArgs a) {
     unsigned lost_cnt[2 * D];
 #pragma unroll
     for (int q = 0; q < 2 * D; ++q) lost_cnt[q] = 0u;
+    bool far_seen = false;
     for (long long c = ca + warp; c < cb; c += kClsWarps) {
         const long long p0 = a.starts[c], p1 = a.starts[c + 1];
         int co[3];
@@ -753,9 +754,9 @@ __global__ void __launch_bounds__(kPicThreads) k_cls_pass1(ClsArgs a) {
 #pragma unroll
                         for (int m = 1; m < NM; ++m) smem_add64(&mom_lo[warp][m][cls], &mom_hi[warp][m][cls], q[m]);
                     } else if (cls == -1) {
-                        // far mover: flag the species; the caller redoes its move and
-                        // its whole deposit from the re-sorted state
-                        atomicOr(a.far, 1);
+                        // far mover: the species is flagged at the end (one atomic per
+                        // warp); the caller redoes its move and its whole deposit
+                        far_seen = true;
                     }
                 }
                 if (++pending == 32 / kClsRounds || base + 32 * kClsRounds >= p1) {
@@ -811,6 +812,7 @@ __global__ void __launch_bounds__(kPicThreads) k_cls_pass1(ClsArgs a) {
         for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(full, t, o);
         if (lane == 0 && t) atomicAdd(a.p.losses + q, (unsigned long long)t);
     }
+    if (__any_sync(full, far_seen) && lane == 0) atomicOr(a.far, 1);
     __syncthreads();
     // corners of every box cell once, into the node tile
     {
@@ -1033,15 +1035,26 @@ __global__ void __launch_bounds__(kPicThreads, D == 2 ? 5 : 1) k_cls_pass2(ClsAr
     }
 }
 
-// cell offsets of a sorted key array: starts[c] = first index with key >= c
-__global__ void k_cell_starts(const int* __restrict__ key, const long long* __restrict__ count, long long n_upper,
-                              unsigned* __restrict__ starts, long long n_cells) {
+// Cell offsets of a sorted key array in O(particles + cells): the first and
+// the last particle of every run record its bounds (first[k], last[k] =
+// one past the end; both zero for empty cells), k_run_counts turns them into
+// per-cell counts and an exclusive scan gives starts[c] = first index with
+// key >= c.  (A particle after a long run of empty cells would otherwise
+// fill their offsets alone.)
+__global__ void k_run_bounds(const int* __restrict__ key, const long long* __restrict__ count, long long n_upper,
+                             unsigned* __restrict__ first, unsigned* __restrict__ last) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long cnt = *count;
-    if (i > cnt || i > n_upper) return;
-    const long long ki = i < cnt ? key[i] : n_cells;
-    const long long kp = i == 0 ? -1 : key[i - 1];
-    for (long long c = kp + 1; c <= ki; ++c) starts[c] = (unsigned)i;
+    if (i >= cnt || i >= n_upper) return;
+    const int k = key[i];
+    if (i == 0 || key[i - 1] != k) first[k] = (unsigned)i;
+    if (i == cnt - 1 || key[i + 1] != k) last[k] = (unsigned)(i + 1);
+}
+
+__global__ void k_run_counts(const unsigned* __restrict__ first, unsigned* __restrict__ last, long long n_cells) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < n_cells) last[c] -= first[c];
+    else if (c == n_cells) last[c] = 0u;
 }
 
 __global__ void k_count_from(long long* __restrict__ count, const unsigned* __restrict__ src) { *count = *src; }
@@ -1619,9 +1632,22 @@ static void sort_species(psum_pic_ctx* c, Species& sp, int sidx) {
     { k_count_valid<<<gb, 256, 0, s>>>(skeys, n, sentinel, c->count.p + sidx); count_launch(); }
     sp.cur = nxt;
     if (c->precision == PSUM_PIC_MIXED) {
-        // cell offsets of the sorted state, for the fused sorted step
-        { k_cell_starts<<<blocks_for(n + 1, 256), 256, 0, s>>>(sp.key[nxt].p, c->count.p + sidx, n,
-                                                              sp.starts[sp.starts_cur].p, c->g.n_cells); count_launch(); }
+        // cell offsets of the sorted state, for the fused sorted step; the
+        // other offsets buffer and the new-count buffer are free scratch here
+        const long long nc = c->g.n_cells;
+        const size_t nscan1 = (size_t)(nc + 1 + kScanBlock - 1) / kScanBlock + 1;
+        const size_t nscan2 = (nscan1 + kScanBlock - 1) / kScanBlock + 16;
+        if (sp.newcount.n < (size_t)nc + 1) sp.newcount.alloc((size_t)nc + 1);
+        if (sp.scan_tmp1.n < nscan1) sp.scan_tmp1.alloc(nscan1);
+        if (sp.scan_tmp2.n < nscan2) sp.scan_tmp2.alloc(nscan2);
+        unsigned* first = sp.starts[1 - sp.starts_cur].p;
+        unsigned* last = sp.newcount.p;
+        cuda_check(cudaMemsetAsync(first, 0, sizeof(unsigned) * (nc + 1), s), "memset");
+        cuda_check(cudaMemsetAsync(last, 0, sizeof(unsigned) * (nc + 1), s), "memset");
+        { k_run_bounds<<<blocks_for(n, 256), 256, 0, s>>>(sp.key[nxt].p, c->count.p + sidx, n, first, last); count_launch(); }
+        { k_run_counts<<<blocks_for(nc + 1, 256), 256, 0, s>>>(first, last, nc); count_launch(); }
+        exclusive_scan_u32(last, sp.starts[sp.starts_cur].p, nc + 1, sp.scan_tmp1.p, sp.scan_tmp2.p, s,
+                           (long long)sp.scan_tmp2.n);
         sp.sorted = true;
     }
     cuda_check(cudaGetLastError(), "sort launch");
