@@ -428,8 +428,11 @@ __global__ void __launch_bounds__(kPicThreads) k_push_mixed(PushArgs a) {
 // cell of the pushed state, with absorbed particles removed: what the general
 // path (push in place, stable radix sort) produces.
 //
-// A block owns the cells whose first particle index lies in
-// [b*T, (b+1)*T) (table from k_cls_blocks) and gives each cell to one warp,
+// A block owns the cells whose weighted start (first particle index + the
+// cell index times T / 2048) lies in [b*T, (b+1)*T) (table from
+// k_cls_blocks): at most T particles plus one cell and at most about 2048
+// cells, so long runs of empty cells are spread over many blocks.  Each
+// cell goes to one warp,
 // so ranks and counts need no cross-warp synchronisation.  The pass-1
 // deposit sums the quantised CIC moments of the particles of one (cell,
 // class) group with warp reductions, forms the 2^D corner sums once per group
@@ -446,11 +449,11 @@ constexpr int cls_rounds(double particles_per_cell) { return particles_per_cell 
 // Particles per block: 2D blocks cover a few tens of cells of one row; 3D
 // blocks stay short enough that their node box usually fits the tile.
 __host__ __device__ constexpr int cls_block_lg(int dim) { return dim == 2 ? 13 : 11; }
-__host__ __device__ constexpr int cls_block_particles(int dim) { return 1 << cls_block_lg(dim); }
 // Second-pass blocks are short (no node tile to amortise), so that a pending
 // second pass frees SM slots often for the higher-priority work beside it.
 __host__ __device__ constexpr int cls_block_lg2(int) { return 11; }
-__host__ __device__ constexpr int cls_block_particles2(int dim) { return 1 << cls_block_lg2(dim); }
+// weight of a cell in the block table, in particles (at most 2048 cells per block)
+__host__ __device__ constexpr long long cls_cell_weight(int lgT) { return 1LL << (lgT - 11); }
 
 template <int D>
 struct MoveClasses {
@@ -497,18 +500,19 @@ __device__ __forceinline__ bool class_target(const GridView& g, const int c[3], 
     return true;
 }
 
-// Block -> first owned cell: first[b] = lower bound of b*T in starts,
-// clamped to n_cells; entries 0..nb.
-// (T = 2^lgT particles per block.)
+// Block -> first owned cell: first[b] = lower bound of b*T in the weighted
+// starts w(c) = starts[c] + c * cls_cell_weight(lgT), clamped to n_cells;
+// entries 0..nb.  (T = 2^lgT.)
 __global__ void k_cls_blocks(const unsigned* __restrict__ starts, long long n_cells, long long nb, int lgT,
                              unsigned* __restrict__ first) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long wc = cls_cell_weight(lgT);
     if (t <= n_cells) {
-        const long long hi = (long long)(starts[t] >> lgT);
-        for (long long b = t == 0 ? 0 : (long long)(starts[t - 1] >> lgT) + 1; b <= hi && b <= nb; ++b)
+        const long long hi = ((long long)starts[t] + t * wc) >> lgT;
+        for (long long b = t == 0 ? 0 : (((long long)starts[t - 1] + (t - 1) * wc) >> lgT) + 1; b <= hi && b <= nb; ++b)
             first[b] = (unsigned)t;
     }
-    if (t <= nb && (t << lgT) > (long long)starts[n_cells]) first[t] = (unsigned)n_cells;
+    if (t <= nb && (t << lgT) > (long long)starts[n_cells] + n_cells * wc) first[t] = (unsigned)n_cells;
 }
 
 struct NodeTile {
@@ -1809,8 +1813,13 @@ struct PhaseTimer {
 // k_cls_pass1 / k_cls_pass2.  Species in which some particle moved more
 // than one cell along an axis take the general path (in-place push, radix
 // sort) for this step; their deposit from pass 1 stands.
-static long long cls_blocks(long long n, int dim) { return n / cls_block_particles(dim) + 1; }
-static long long cls_blocks2(long long n, int dim) { return n / cls_block_particles2(dim) + 1; }
+// blocks of the two tables for up to n particles over nc cells
+static long long cls_blocks(long long n, long long nc, int dim) {
+    return ((n + nc * cls_cell_weight(cls_block_lg(dim))) >> cls_block_lg(dim)) + 1;
+}
+static long long cls_blocks2(long long n, long long nc, int dim) {
+    return ((n + nc * cls_cell_weight(cls_block_lg2(dim))) >> cls_block_lg2(dim)) + 1;
+}
 
 template <int D, int P, int R>
 static void launch_pass_t(const ClsArgs& a, int pass, unsigned blocks, cudaStream_t s) {
@@ -1835,7 +1844,7 @@ static void launch_pass_r(const ClsArgs& a, int pass, unsigned blocks, int round
 }
 
 static void launch_pass(const ClsArgs& a, int dim, int pusher, int pass, long long n, cudaStream_t s) {
-    const unsigned blocks = (unsigned)(pass == 1 ? cls_blocks(n, dim) : cls_blocks2(n, dim));
+    const unsigned blocks = (unsigned)(pass == 1 ? cls_blocks(n, a.n_cells, dim) : cls_blocks2(n, a.n_cells, dim));
     const int rounds = cls_rounds((double)n / (double)a.n_cells);
     if (dim == 2) {
         if (pusher == PSUM_PIC_BORIS) launch_pass_r<2, PSUM_PIC_BORIS>(a, pass, blocks, rounds, s);
@@ -1858,8 +1867,8 @@ static void ensure_cls_buffers(psum_pic_ctx* c) {
         Species& sp = *spp;
         if (sp.n <= 0) continue;
         grow(sp.cls_count, (size_t)nc * ncls);
-        grow(sp.cls_first, (size_t)cls_blocks(sp.n, c->g.dim) + 1);
-        grow(sp.cls_first2, (size_t)cls_blocks2(sp.n, c->g.dim) + 1);
+        grow(sp.cls_first, (size_t)cls_blocks(sp.n, nc, c->g.dim) + 1);
+        grow(sp.cls_first2, (size_t)cls_blocks2(sp.n, nc, c->g.dim) + 1);
         grow(sp.newcount, (size_t)nc + 1);
         grow(sp.scan_tmp1, (size_t)(nc + 1 + kScanBlock - 1) / kScanBlock + 1);
         grow(sp.scan_tmp2, (size_t)((nc + 1 + kScanBlock - 1) / kScanBlock + kScanBlock - 1) / kScanBlock + 16);
@@ -1915,11 +1924,11 @@ static void cls_step(psum_pic_ctx* c, const double* phi, double dt, int pusher, 
             a.vel_out[d] = sp.vel[d][nxt].p;
         }
         a.n_cells = nc;
-        const long long nb = cls_blocks(sp.n, c->g.dim);
+        const long long nb = cls_blocks(sp.n, nc, c->g.dim);
         { k_cls_blocks<<<blocks_for(std::max(nc, nb) + 1, 256), 256, 0, s>>>(a.starts, nc, nb, cls_block_lg(c->g.dim),
                                                                              sp.cls_first.p); count_launch(); }
         launch_pass(a, c->g.dim, pusher, 1, sp.n, s);
-        const long long nb2 = cls_blocks2(sp.n, c->g.dim);
+        const long long nb2 = cls_blocks2(sp.n, nc, c->g.dim);
         { k_cls_blocks<<<blocks_for(std::max(nc, nb2) + 1, 256), 256, 0, s>>>(a.starts, nc, nb2, cls_block_lg2(c->g.dim),
                                                                               sp.cls_first2.p); count_launch(); }
         if (c->g.dim == 2) { k_cls_offsets<2><<<blocks_for(nc + 1, 256), 256, 0, s>>>(c->g, sp.cls_count.p, sp.newcount.p, nc); count_launch(); }
