@@ -542,3 +542,62 @@ def test_fused_step_many_particles_per_cell(kind, pusher):
         assert (pf.view(np.int64) == pg.view(np.int64)).all()
         assert (vf.view(np.int64) == vg.view(np.int64)).all()
         assert (df.view(np.int64) == dg.view(np.int64)).all()
+
+
+@pytest.mark.parametrize("kind", ["2d_periodic", "3d_periodic"])
+def test_fused_steps_with_solve_match_general_steps(kind):
+    # Several steps through a real Poisson solve.  The fused step leaves its
+    # second pass running beside the next step's density and solve, and
+    # joins it before the next push; the general path pushes in place and
+    # is re-sorted after every step.  With exact integer deposits both runs
+    # see the same fields, so the states agree bit for bit after every step.
+    out = []
+    for fused in (True, False):
+        ctx, g, pos, vel, phi0 = make_case(kind, P.MIXED, seed=38, n=60000)
+        pos = wrap_into(pos, g)
+        ctx.set_options(f"sort_interval {1 if fused else 0}")
+        sps = []
+        for s in range(2):
+            sp = ctx.add_species(-1.0 if s == 0 else 1.0, 1.0 if s == 0 else 4.0, 0.5, pos.shape[1])
+            ctx.load(sp, pos, vel * (1.0 if s == 0 else 0.5))
+            sps.append(sp)
+        ctx.sort()
+        ctx.deposit()
+        cells = g.cells[:g.dim]
+        nodes = [c + 1 for c in cells]
+        grid = P.simple_grid(tuple(g.lower[:g.dim]), tuple(g.upper[:g.dim]), tuple(cells))
+        opts = (f"I {nodes[0]} J {nodes[1]} K {nodes[2] if g.dim == 3 else 1} depth 3 pre_relax 2 post_relax 2 "
+                f"max_cycles 20 correction_interval 2 tol 1e-10 periodic_I 1 periodic_J 1"
+                + (" periodic_K 1" if g.dim == 3 else ""))
+        ps = P.Poisson_solver_2d() if g.dim == 2 else P.Poisson_solver_3d()
+        ps.set_options(opts)
+        ps.init("cuda_multigrid32f_gpu", grid, ps.Cartesian, [P.Dirichlet_nodes(grid, [(0,) * g.dim], 0.0)], 1.0)
+        ps.make_righthand_item()
+        stream = torch.cuda.Stream()
+        ctx.set_stream(stream)
+        nn = ctx.n_nodes
+        rho = dev(np.zeros(nn))
+        phi = dev(np.zeros(nn))
+        states = []
+        with torch.cuda.stream(stream):
+            for _ in range(4):
+                ctx.step(ps.backend, 0.0, rho, phi, 0.12)
+                losses = ctx.losses()          # needs no join
+                if not fused:
+                    ctx.sort()
+                step_state = []
+                for sp in sps:
+                    p_, v_ = ctx.get_state(sp)  # joins the pending second pass
+                    k = torch.zeros(p_.shape[1], dtype=torch.int32, device="cuda")
+                    ctx.get_keys(sp, k)
+                    step_state.append((p_, v_, k.cpu().numpy()))
+                states.append((step_state, losses, phi.cpu().numpy()))
+        torch.cuda.synchronize()
+        out.append(states)
+    for (sf, lf, phif), (sg, lg, phig) in zip(*out):
+        assert (lf == lg).all()
+        assert (phif.view(np.int64) == phig.view(np.int64)).all()
+        for (pf, vf, kf), (pg, vg, kg) in zip(sf, sg):
+            assert (kf == kg).all()
+            assert (pf.view(np.int64) == pg.view(np.int64)).all()
+            assert (vf.view(np.int64) == vg.view(np.int64)).all()
