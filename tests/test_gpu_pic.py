@@ -601,3 +601,30 @@ def test_fused_steps_with_solve_match_general_steps(kind):
             assert (kf == kg).all()
             assert (pf.view(np.int64) == pg.view(np.int64)).all()
             assert (vf.view(np.int64) == vg.view(np.int64)).all()
+
+
+@pytest.mark.parametrize("kind", ["2d_absorb", "3d_periodic"])
+def test_mas_particle_group_round_trip(kind, tmp_path):
+    # a group saved in PSuM's MAS layout and loaded into a fresh context
+    # gives back the same particles (cells and offsets exactly: dx = 1)
+    from psum_b200 import mas
+    ctx, g, pos, vel, _ = make_case(kind, P.MIXED, seed=39, n=20000)
+    pos = wrap_into(pos, g)
+    sp = ctx.add_species(-1.0, 1.0, 1.0, pos.shape[1])
+    ctx.load(sp, pos, vel)
+    ctx.sort()
+    p0, v0 = ctx.get_state(sp)
+    path = tmp_path / "group.mas"
+    n = mas.save_particle_group(mas.MasFile(path, "replace"), "electrons", ctx, sp)
+    assert n == p0.shape[1]
+    fp = mas.MasFile(path)
+    assert fp.keys() == ["electrons.data.device", "electrons.data.content.position",
+                         "electrons.data.content.velocity"]
+    assert fp.read("electrons.data.content.position")[0].shape == (n, g.dim, 1)
+    ctx2, _, _, _, _ = make_case(kind, P.MIXED, seed=39, n=20000)
+    sp2 = ctx2.add_species(-1.0, 1.0, 1.0, n)
+    mas.load_particle_group(fp, "electrons", ctx2, sp2)
+    ctx2.sort()
+    p1, v1 = ctx2.get_state(sp2)
+    assert (p1.view(np.int64) == p0.view(np.int64)).all()
+    assert (v1.view(np.int64) == v0.view(np.int64)).all()
