@@ -6,10 +6,12 @@ particle-kernel set of include/psum_pic.h.  The Python modules are thin
 ctypes mirrors of the reference interfaces; there is no CPU fallback.
 """
 from ._lib import LIB_PATH, PROTOTYPES, PsumError, check, lib
-from .field_solver import (Dirichlet_line, Dirichlet_nodes, Dirichlet_plane, Poisson_solver_2d, Poisson_solver_3d,
-                           assemble_poisson, registered_table, simple_grid, solver_backend)
+from .field_solver import (Dirichlet_box, Dirichlet_func, Dirichlet_line, Dirichlet_nodes, Dirichlet_plane,
+                           MixedBoundary, Neumann_line, Poisson_solver_2d, Poisson_solver_3d, Robin_Line,
+                           assemble_poisson, assemble_poisson_2d, registered_table, simple_grid, solver_backend)
 from .pic import BORIS, FP64, LEAPFROG, MIXED, ParticleContext
 
 __all__ = ["LIB_PATH", "PROTOTYPES", "PsumError", "check", "lib", "Dirichlet_line", "Dirichlet_nodes",
-           "Dirichlet_plane", "Poisson_solver_2d", "Poisson_solver_3d", "assemble_poisson", "registered_table",
+           "Dirichlet_plane", "Dirichlet_box", "Dirichlet_func", "Neumann_line", "Robin_Line", "MixedBoundary",
+           "Poisson_solver_2d", "Poisson_solver_3d", "assemble_poisson", "assemble_poisson_2d", "registered_table",
            "simple_grid", "solver_backend", "ParticleContext", "MIXED", "FP64", "LEAPFROG", "BORIS"]

@@ -10,8 +10,12 @@
   creates the backend, replays the cached options and calls ``set_matrix``;
   ``solve(phi, rho)`` sets the Dirichlet values with ``set_source_replace``
   and solves on device buffers, overwriting ``rho`` like PSuM does.
-* ``Dirichlet_line`` / ``Dirichlet_plane`` / ``Dirichlet_nodes`` mirror the
-  boundary creators of src/field_solver/boundary_creator/Dirichlet.hpp.
+* ``Dirichlet_line`` / ``Dirichlet_plane`` / ``Dirichlet_nodes`` /
+  ``Dirichlet_box`` / ``Dirichlet_func`` mirror the boundary creators of
+  src/field_solver/boundary_creator/Dirichlet.hpp; ``Neumann_line`` and
+  ``Robin_Line`` those of Neumann.hpp / Robin.hpp.  In 2-D, ``init`` also
+  takes mixed (Neumann / Robin) boundaries, the cylindrical (z, r) operator
+  and a position-dependent epsilon (``assemble_poisson_2d``).
 
 Device buffers are torch CUDA float64 tensors (or raw device addresses).
 Errors raise ``PsumError`` (a RuntimeError), as PSuM's frontends rethrow.
@@ -23,7 +27,8 @@ import numpy as np
 from ._lib import PsumError, check, lib
 
 __all__ = ["simple_grid", "solver_backend", "Poisson_solver_2d", "Poisson_solver_3d", "Dirichlet_line",
-           "Dirichlet_plane", "Dirichlet_nodes", "assemble_poisson", "registered_table"]
+           "Dirichlet_plane", "Dirichlet_nodes", "Dirichlet_box", "Dirichlet_func", "Neumann_line", "Robin_Line",
+           "MixedBoundary", "assemble_poisson", "assemble_poisson_2d", "registered_table"]
 
 
 def _ptr(a):
@@ -116,6 +121,242 @@ def Dirichlet_nodes(grid, nodes, value):
     periodic operator non-singular, application/benchmark/TSI/main.cpp:106-113)."""
     idx = [grid.n2i(*n) for n in nodes]
     return np.asarray(idx, np.uint64), np.full(len(idx), float(value))
+
+
+def Dirichlet_box(grid, x0, y0, x1, y1, value, geo_tolerance=1e-10):
+    """Nodes inside a box, with a tolerance of geo_tolerance times the
+    grid's size (Dirichlet.hpp:104-119)."""
+    x, y = _node_positions(grid)
+    tol = geo_tolerance * np.sqrt((grid.upper[0] - grid.lower[0]) * (grid.upper[1] - grid.lower[1]))
+    sel = (x >= x0 - tol) & (x <= x1 + tol) & (y >= y0 - tol) & (y <= y1 + tol)
+    idx = np.nonzero(sel.reshape(-1))[0].astype(np.uint64)
+    return idx, np.full(idx.size, float(value))
+
+
+def Dirichlet_func(grid, predicate, value):
+    """Nodes where predicate(x, y) holds (Dirichlet.hpp:121-135)."""
+    x, y = _node_positions(grid)
+    sel = np.array([bool(predicate(a, b)) for a, b in zip(x.reshape(-1), y.reshape(-1))])
+    idx = np.nonzero(sel)[0].astype(np.uint64)
+    return idx, np.full(idx.size, float(value))
+
+
+def _node_positions(grid):
+    """(x, y) of every node of a 2-D grid, shaped (I + 1, J + 1)."""
+    if grid.dim != 2:
+        raise ValueError("a 2-D grid is required")
+    i = np.arange(grid.cells[0] + 1)
+    j = np.arange(grid.cells[1] + 1)
+    return np.meshgrid(grid.lower[0] + i * grid.delta[0], grid.lower[1] + j * grid.delta[1], indexing="ij")
+
+
+class MixedBoundary:
+    """mixed_boundary<2> (src/field_solver/mixed_boundary.hpp:17-150): the
+    nodes of one boundary line with the condition
+
+        a * phi + b * dphi/dn = value      (n: the outward normal of `direction`)
+
+    where (a, b) = coeffs (a pair, or a function of (x, y) giving one) and
+    value is a number or a function of (x, y).  ``set`` plays the role of
+    PSuM's ``boundary = value``."""
+
+    def __init__(self, grid, nodes, direction, coeffs, value=None):
+        if direction not in ("N", "S", "E", "W"):
+            raise ValueError("direction must be one of N, S, E, W")
+        self.grid = grid
+        self.nodes = np.asarray(nodes, np.int64)
+        self.direction = direction
+        self.coeffs = coeffs
+        self.value = value
+
+    def set(self, value):
+        self.value = value
+        return self
+
+    def _positions(self):
+        x, y = _node_positions(self.grid)
+        return x.reshape(-1)[self.nodes], y.reshape(-1)[self.nodes]
+
+    def values(self):
+        if self.value is None:
+            raise ValueError("mixed_boundary::evaluate: no value is set")
+        x, y = self._positions()
+        if callable(self.value):
+            return np.array([float(self.value(a, b)) for a, b in zip(x, y)])
+        return np.full(self.nodes.size, float(self.value))
+
+    def coefficient_pairs(self):
+        x, y = self._positions()
+        if callable(self.coeffs):
+            pairs = np.array([self.coeffs(a, b) for a, b in zip(x, y)], np.float64).reshape(-1, 2)
+        else:
+            pairs = np.tile(np.asarray(self.coeffs, np.float64), (self.nodes.size, 1))
+        return pairs[:, 0], pairs[:, 1]
+
+
+def _line_nodes(grid, direction, min_max):
+    """Boundary line nodes (Neumann.hpp:48-88): S / N are j = 0 / J, W / E
+    i = 0 / I; with min_max only those whose coordinate along the line lies
+    in [min, max]."""
+    I, J = grid.cells
+    if direction == "S":
+        ij = [(i, 0) for i in range(I + 1)]
+    elif direction == "N":
+        ij = [(i, J) for i in range(I + 1)]
+    elif direction == "W":
+        ij = [(0, j) for j in range(J + 1)]
+    elif direction == "E":
+        ij = [(I, j) for j in range(J + 1)]
+    else:
+        raise ValueError("direction must be one of N, S, E, W")
+    out = []
+    for i, j in ij:
+        along = grid.lower[1] + j * grid.delta[1] if direction in ("W", "E") else grid.lower[0] + i * grid.delta[0]
+        if min_max is None or not (along < min_max[0] or along > min_max[1]):
+            out.append(grid.n2i(i, j))
+    return out
+
+
+def Neumann_line(grid, direction, value=None, min_max=None):
+    """dphi/dn = value on a boundary line (Neumann.hpp:48-93)."""
+    return MixedBoundary(grid, _line_nodes(grid, direction, min_max), direction, (0.0, 1.0), value)
+
+
+def Robin_Line(grid, direction, coef_value_and_grad, value=None, min_max=None):
+    """a * phi + b * dphi/dn = value on a boundary line (Robin.hpp:55-110);
+    coef_value_and_grad is (a, b) or a function of (x, y) giving it."""
+    return MixedBoundary(grid, _line_nodes(grid, direction, min_max), direction, coef_value_and_grad, value)
+
+
+def _merge_mixed(mixed_boundaries, fixed_idx):
+    """mixed_boundary_list (mixed_boundary.hpp:158-190): keyed by (node,
+    direction), a later boundary covers an earlier one's (node, direction)
+    pairs, so a corner node keeps one condition per direction; fixed nodes
+    cover every mixed condition of theirs (Poisson_solver_2d.hpp:191-199).
+    Returns (node, direction, boundary index, position in that boundary) per
+    mixed condition."""
+    fixed = set(int(v) for v in np.asarray(fixed_idx, np.int64).tolist())
+    taken = set()
+    entries = []
+    for b in reversed(range(len(mixed_boundaries))):
+        mb = mixed_boundaries[b]
+        for k, node in enumerate(mb.nodes.tolist()):
+            if (node, mb.direction) in taken or node in fixed:
+                continue
+            taken.add((node, mb.direction))
+            entries.append((node, mb.direction, b, k))
+    entries.sort()
+    return entries
+
+
+def assemble_poisson_2d(grid, domain, fixed_nodes, mixed_boundaries=(), epsilon=8.854e-12):
+    """Operator of Poisson_solver_2d::_init_impl (Poisson_solver_2d.hpp:182-368)
+    for Cartesian or cylindrical (z along axis 0, r along axis 1) domains,
+    epsilon a number or a function of (x, y) taken at the face midpoints, and
+    mixed boundaries by ghost nodes: a mixed node's neighbour across its
+    boundary is a ghost defined by the boundary condition with a central
+    difference, and eliminating it changes the node's row and adds
+    M * boundary values to its right-hand side (ghost_element_manager.hpp:
+    A' = A - B D^-1 C, M = -B D^-1; here each ghost has its own equation, so
+    D is diagonal and the elimination is per node).
+
+    Returns ((rows, cols, vals) of A', (addback_rows, M_vals, mixed_entries)),
+    where the right-hand side of row addback_rows[t] gains M_vals[t] times the
+    value of mixed node t."""
+    if grid.dim != 2:
+        raise ValueError("a 2-D grid is required")
+    if domain not in ("Cartesian", "Cylindrical"):
+        raise ValueError("domain must be Cartesian or Cylindrical")
+    I, J = grid.cells
+    nI, nJ = I + 1, J + 1
+    n = nI * nJ
+    dx, dy = grid.delta
+    dxr, dyr = 1.0 / dx, 1.0 / dy
+    x, y = _node_positions(grid)
+    ii, jj = np.meshgrid(np.arange(nI), np.arange(nJ), indexing="ij")
+    node = (ii * nJ + jj).reshape(-1)
+    nbr = {   # cyclic neighbours (the :225-231 cyclic_index)
+        "N": (ii * nJ + (jj + 1) % nJ).reshape(-1), "S": (ii * nJ + (jj - 1) % nJ).reshape(-1),
+        "E": (((ii + 1) % nI) * nJ + jj).reshape(-1), "W": (((ii - 1) % nI) * nJ + jj).reshape(-1),
+    }
+    if callable(epsilon):
+        eps_f = np.vectorize(lambda a, b: float(epsilon(a, b)), otypes=[np.float64])
+    else:
+        eps_f = lambda a, b: np.full(np.shape(a), float(epsilon))
+    # face midpoints of the unwrapped neighbours, as PSuM takes them
+    eps = {"N": eps_f(x, y + 0.5 * dy), "S": eps_f(x, y - 0.5 * dy),
+           "E": eps_f(x + 0.5 * dx, y), "W": eps_f(x - 0.5 * dx, y)}
+    eps = {k: v.reshape(-1) for k, v in eps.items()}
+    xf, yf = x.reshape(-1), y.reshape(-1)
+    if domain == "Cylindrical":
+        r_up = (yf + (yf + dy)) / 2
+        r_lo = np.maximum((yf + (yf - dy)) / 2, 0.0)
+        s_n = dx * np.pi * 2 * r_up
+        s_s = dx * np.pi * 2 * r_lo
+        s_e = s_w = np.pi * (r_up * r_up - r_lo * r_lo)
+        vol = dx * np.pi * (r_up * r_up - r_lo * r_lo)
+    else:
+        s_n = s_s = np.full(n, dx)
+        s_e = s_w = np.full(n, dy)
+        vol = np.full(n, dx * dy)
+    m = -1.0 / vol
+    # (grad_E S_E eps_E - grad_W S_W eps_W + grad_N S_N eps_N - grad_S S_S eps_S) * (-1 / V)
+    c = {"E": ((dxr * s_e) * eps["E"]) * m, "W": ((dxr * s_w) * eps["W"]) * m,
+         "N": ((dyr * s_n) * eps["N"]) * m, "S": ((dyr * s_s) * eps["S"]) * m}
+    cen = ((((-dxr * s_e) * eps["E"] - (dxr * s_w) * eps["W"]) + (-dyr * s_n) * eps["N"]) - (dyr * s_s) * eps["S"]) * m
+    fixed = np.zeros(n, bool)
+    fixed[np.asarray(fixed_nodes, np.int64)] = True
+    entries = _merge_mixed(list(mixed_boundaries), np.nonzero(fixed)[0])
+    opposite = {"N": "S", "S": "N", "E": "W", "W": "E"}
+    ghost = {d: np.zeros(n, bool) for d in "NSEW"}
+    extra_r, extra_c, extra_v = [], [], []
+    add_rows, add_vals = [], []
+    coef_cache = {}
+    for t, (nd, d, b, k) in enumerate(entries):
+        if b not in coef_cache:
+            coef_cache[b] = mixed_boundaries[b].coefficient_pairs()
+        a_val, b_grad = coef_cache[b][0][k], coef_cache[b][1][k]
+        if b_grad == 0.0:
+            raise ValueError("a mixed boundary needs a non-zero gradient coefficient (use a fixed boundary)")
+        dr = dyr if d in ("N", "S") else dxr
+        if ghost[opposite[d]][nd]:
+            raise ValueError("a node with mixed boundaries on opposite sides is not supported")
+        ghost[d][nd] = True
+        cg = c[d][nd]
+        # ghost = phi_opposite + 2 (value - a phi) / (b dr)
+        extra_r += [nd, nd]
+        extra_c += [nbr[opposite[d]][nd], nd]
+        extra_v += [cg, cg * (-2.0 * a_val / (b_grad * dr))]
+        add_rows.append(nd)
+        add_vals.append(-cg * 2.0 / (b_grad * dr))
+    free = ~fixed
+    rows, cols, vals = [np.nonzero(fixed)[0]], [np.nonzero(fixed)[0]], [np.ones(int(fixed.sum()))]
+    rows.append(node[free])
+    cols.append(node[free])
+    vals.append(cen[free])
+    for d in "NSEW":
+        sel = free & ~ghost[d]
+        rows.append(node[sel])
+        cols.append(nbr[d][sel])
+        vals.append(c[d][sel])
+    if extra_r:
+        rows.append(np.asarray(extra_r, np.int64))
+        cols.append(np.asarray(extra_c, np.int64))
+        vals.append(np.asarray(extra_v))
+    r = np.concatenate(rows).astype(np.int64)
+    cc = np.concatenate(cols).astype(np.int64)
+    v = np.concatenate(vals)
+    # coalesce duplicates (a cyclic neighbour or a ghost's partner can repeat a column)
+    key = r * n + cc
+    order = np.argsort(key, kind="stable")
+    key, v = key[order], v[order]
+    uniq, start = np.unique(key, return_index=True)
+    v = np.add.reduceat(v, start)
+    keep = v != 0.0
+    uniq, v = uniq[keep], v[keep]
+    A = ((uniq // n).astype(np.uint64), (uniq % n).astype(np.uint64), v)
+    M = (np.asarray(add_rows, np.int64), np.asarray(add_vals), entries)
+    return A, M
 
 
 def _merge_fixed(fixed_boundaries):
@@ -237,6 +478,7 @@ class solver_backend:
 class _PoissonFrontend:
     dim = 0
     Cartesian = "Cartesian"
+    Cylindrical = "Cylindrical"
 
     def __init__(self):
         self.backend_name = "native"
@@ -246,6 +488,8 @@ class _PoissonFrontend:
         self.replace_val = np.zeros(0)
         self.coo = None
         self.grid = None
+        self.mixed = []
+        self.mixed_M = None
 
     def set_options(self, options):
         """Cached and replayed at init, like Poisson_solver_2d::set_options (:158-165)."""
@@ -253,17 +497,27 @@ class _PoissonFrontend:
         if not self.backend.is_null():
             self.backend.set_options(options)
 
-    def init(self, backend_name, grid, domain, fixed_boundaries, epsilon=8.854e-12):
+    def init(self, backend_name, grid, domain, fixed_boundaries, epsilon=8.854e-12, mixed_boundaries=()):
+        """Poisson_solver_2d::init / _init_impl (:182-404): fixed (Dirichlet)
+        boundaries, and in 2-D mixed (Neumann / Robin) boundaries, the
+        cylindrical domain and an epsilon function of (x, y)."""
         if grid.dim != self.dim:
             raise ValueError(f"grid must be {self.dim}-D")
-        if domain != self.Cartesian:
-            raise ValueError("only the Cartesian operator is provided by this frontend")
+        general = bool(mixed_boundaries) or domain != self.Cartesian or callable(epsilon)
+        if domain not in (self.Cartesian, self.Cylindrical) or (general and self.dim != 2):
+            raise ValueError("mixed boundaries, the cylindrical domain and epsilon functions are provided in 2-D")
         if backend_name == "native":
             raise PsumError(1, "the 'native' Eigen direct solver is not part of this backend; "
                                "use cuda_multigrid32f_gpu or cuda_multigrid64_gpu")
         self.grid = grid
         self.replace_idx, self.replace_val = _merge_fixed(fixed_boundaries)
-        rows, cols, vals = assemble_poisson(grid, self.replace_idx, epsilon)
+        if general:
+            (rows, cols, vals), self.mixed_M = assemble_poisson_2d(grid, domain, self.replace_idx,
+                                                                   list(mixed_boundaries), epsilon)
+            self.mixed = list(mixed_boundaries)
+        else:
+            rows, cols, vals = assemble_poisson(grid, self.replace_idx, epsilon)
+            self.mixed, self.mixed_M = [], None
         self.coo = (rows, cols, vals)
         self.backend_name = backend_name
         self.backend = solver_backend(backend_name)
@@ -275,9 +529,23 @@ class _PoissonFrontend:
     def coeff_matrix(self):
         return self.coo
 
+    def addback(self):
+        """(rows, values) added to the right-hand side for the mixed
+        boundaries: M times the boundary values, summed per row."""
+        if not self.mixed_M or len(self.mixed_M[0]) == 0:
+            return np.zeros(0, np.uint64), np.zeros(0)
+        rows, mvals, entries = self.mixed_M
+        vals_of = [mb.values() for mb in self.mixed]
+        bv = np.array([vals_of[b][k] for (_, _, b, k) in entries])
+        contrib = mvals * bv
+        uniq, inv = np.unique(rows, return_inverse=True)
+        return uniq.astype(np.uint64), np.bincount(inv, weights=contrib, minlength=uniq.size)
+
     def make_righthand_item(self):
-        """Poisson_solver_2d::make_righthand_item (:73-103) without mixed boundaries."""
-        self.backend.set_source_addback(np.zeros(0, np.uint64), np.zeros(0))
+        """Poisson_solver_2d::make_righthand_item (:73-103): the mixed
+        boundaries' add-back, then the fixed values."""
+        idx, val = self.addback()
+        self.backend.set_source_addback(idx, val)
         self.backend.set_source_replace(self.replace_idx, self.replace_val)
 
     def solve(self, phi, source):
