@@ -85,20 +85,13 @@ class simple_grid:
         return tuple(c + 1 for c in self.cells)
 
 
-def Dirichlet_line(grid, direction, value):
+def Dirichlet_line(grid, direction, value, min_max=None):
     """Nodes of one boundary line of a 2-D grid (Dirichlet.hpp:58-99): S/N fix
-    j = 0 / j = J, W/E fix i = 0 / i = I."""
-    I, J = grid.cells
-    if direction == "S":
-        idx = [grid.n2i(i, 0) for i in range(I + 1)]
-    elif direction == "N":
-        idx = [grid.n2i(i, J) for i in range(I + 1)]
-    elif direction == "W":
-        idx = [grid.n2i(0, j) for j in range(J + 1)]
-    elif direction == "E":
-        idx = [grid.n2i(I, j) for j in range(J + 1)]
-    else:
+    j = 0 / j = J, W/E fix i = 0 / i = I; with min_max = (lo, hi) only the
+    nodes whose coordinate along the line lies in [lo, hi]."""
+    if direction not in ("N", "S", "E", "W"):
         raise ValueError("direction must be one of N, S, E, W")
+    idx = _line_nodes(grid, direction, min_max)
     return np.asarray(idx, np.uint64), np.full(len(idx), float(value))
 
 

@@ -326,7 +326,7 @@ def test_mixed_boundaries_multigrid_matches_direct(kind):
     # 1e-8 in FP64 (the restated algorithm stalls there too) while the
     # solution is then accurate to ~1e-14, so that case stops at 1e-8.
     import math
-    from test_mixed_boundaries import direct_solve, node_xy
+    from test_mixed_boundaries import collisionless_flow_field, direct_solve, node_xy
     cases = []
     g = P.simple_grid((0.0, 0.0), (1.0, 1.67), (60, 40))
     _, r = node_xy(g)
@@ -339,6 +339,8 @@ def test_mixed_boundaries_multigrid_matches_direct(kind):
                   [P.Neumann_line(g, "N", 0.0), P.Neumann_line(g, "S", lambda a, b: 0.1 * a),
                    P.Robin_Line(g, "E", (2.0, 0.5), 0.3)],
                   np.cos(x) + y, lambda a, b: 1.0 + 0.5 * b, 1e-11))
+    g, fixed, mixed, rho = collisionless_flow_field()
+    cases.append((g, "Cylindrical", fixed, mixed, rho, 8.854e-12, 1e-8))
     for g, domain, fixed, mixed, rho, eps, stop in cases:
         nodes = [c + 1 for c in g.cells]
         ps = P.Poisson_solver_2d()

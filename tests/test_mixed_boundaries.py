@@ -128,3 +128,36 @@ def test_overlap_rules_and_creators():
     assert late.nodes.tolist() == [g.n2i(4, 1), g.n2i(4, 2)]
     with pytest.raises(ValueError):
         P.assemble_poisson_2d(g, "Cartesian", [], [P.Robin_Line(g, "W", (1.0, 0.0), 0.0)], 1.0)
+
+
+def collisionless_flow_field(N=48):
+    """The field set-up of PSuM's collision-less-flow application
+    (application/collision-less-flow/field_ops.hpp:92-124): (z, r) domain,
+    Robin lines on E and N with coefficients (1, (z^2 + r^2) / z) and
+    (1, (z^2 + r^2) / r), zero flux on the axis, grounded W for r <= r_length."""
+    g = P.simple_grid((0.0, 0.0), (2.0, 1.0), (2 * N, N))
+    mixed = [P.Robin_Line(g, "E", lambda z, r: (1.0, (z * z + r * r) / z), lambda z, r: 0.5 * r),
+             P.Robin_Line(g, "N", lambda z, r: (1.0, (z * z + r * r) / r), lambda z, r: 0.2 * z),
+             P.Neumann_line(g, "S", 0.0)]
+    fixed = [P.Dirichlet_line(g, "W", 0.0, (0.0, 0.6))]
+    z, r = node_xy(g)
+    rho = 1e-9 * np.exp(-((z - 0.5) ** 2 + r ** 2) / 0.05)
+    return g, fixed, mixed, rho
+
+
+def test_collisionless_flow_field_setup():
+    g, fixed, mixed, rho = collisionless_flow_field()
+    # the partial Dirichlet line: W nodes with r in [0, 0.6] only
+    idx, _ = fixed[0]
+    assert len(idx) == sum(1 for j in range(g.cells[1] + 1) if j * g.delta[1] <= 0.6 + 1e-12)
+    phi = direct_solve(g, "Cylindrical", fixed, mixed, rho)
+    assert np.isfinite(phi).all()
+    # the Robin condition holds at the E boundary to O(h): phi + b dphi/dz = 0.5 r
+    I = g.cells[0]
+    dz = g.delta[0]
+    for j in (g.cells[1] // 4, g.cells[1] // 2):
+        z, r = g.lower[0] + I * dz, j * g.delta[1]
+        b = (z * z + r * r) / z
+        dphi = (3 * phi[g.n2i(I, j)] - 4 * phi[g.n2i(I - 1, j)] + phi[g.n2i(I - 2, j)]) / (2 * dz)
+        lhs = phi[g.n2i(I, j)] + b * dphi
+        assert abs(lhs - 0.5 * r) < 0.05 * max(abs(0.5 * r), np.abs(phi).max() * 1e-3) + 1e-3
