@@ -91,6 +91,18 @@ EXPORT int psum_pic_load(psum_pic_ctx* ctx, int species, unsigned long long n,
  * arrays have been consumed, so the caller may free them right away. */
 EXPORT int psum_pic_load_device(psum_pic_ctx* ctx, int species, unsigned long long n,
                                 const double* pos_dev, const double* vel_dev);
+/* Adds `n` particles (FP64 SoA, as psum_pic_load) after the stored ones:
+ * particle_group::insert (src/particle_container/particle_group.hpp:103-167),
+ * which fills the group's invalid slots first; groups here are compacted,
+ * so the new particles go to the end.  The species is unsorted afterwards
+ * (the next psum_pic_sort or step re-sorts it).  As after psum_pic_load,
+ * the charge accumulators still hold the last deposit: call
+ * psum_pic_deposit before the next step.  PSUM_ERR_OVERFLOW beyond the
+ * capacity, with nothing stored. */
+EXPORT int psum_pic_append(psum_pic_ctx* ctx, int species, unsigned long long n,
+                           const double* pos_host, const double* vel_host);
+EXPORT int psum_pic_append_device(psum_pic_ctx* ctx, int species, unsigned long long n,
+                                  const double* pos_dev, const double* vel_dev);
 /* Current array length (valid + not yet compacted invalid) and valid count. */
 EXPORT int psum_pic_count(psum_pic_ctx* ctx, int species, unsigned long long* n_stored,
                           unsigned long long* n_valid);

@@ -78,6 +78,8 @@ PROTOTYPES = {
     "psum_pic_push": (I, [P, P, D, I, P]),
     "psum_pic_get_losses": (I, [P, P, I]),
     "psum_pic_join": (I, [P]),
+    "psum_pic_append": (I, [P, I, ULL, P, P]),
+    "psum_pic_append_device": (I, [P, I, ULL, P, P]),
     "psum_pic_step": (I, [P, P, D, P, P, D, I, P]),
     "psum_pic_set_timing": (I, [P, I]),
     "psum_pic_get_timing": (I, [P, P, P, I]),

@@ -2179,6 +2179,71 @@ static void load_common(psum_pic_ctx* ctx, int species, unsigned long long n, co
     cuda_check(cudaGetLastError(), "load launch");
 }
 
+// Appends n particles after the stored ones, in the current buffers (the
+// insert of particle_group.hpp:103-167; this library's groups have no holes,
+// so the new particles go to the end).  The species is unsorted afterwards:
+// the next sort, or the next step, re-sorts it.
+static void append_common(psum_pic_ctx* ctx, int species, unsigned long long n, const double* pos_dev,
+                          const double* vel_dev) {
+    Species& sp = species_at(ctx, species);
+    cudaStream_t s = ctx->stream;
+    if (ctx->precision == PSUM_PIC_MIXED) ensure_keys(ctx, sp);
+    long long cnt = 0;
+    cuda_check(cudaMemcpyAsync(&cnt, ctx->count.p + species, sizeof(long long), cudaMemcpyDeviceToHost, s), "D2H");
+    cuda_check(cudaStreamSynchronize(s), "append sync");
+    if (cnt + (long long)n > sp.cap) throw Error(PSUM_ERR_OVERFLOW, "append: more particles than the species capacity");
+    const int c = sp.cur;
+    if (n > 0) {
+        const unsigned gb = blocks_for((long long)n, 256);
+        if (ctx->precision == PSUM_PIC_MIXED) {
+            { k_load_mixed<<<gb, 256, 0, s>>>(ctx->g, (long long)n, pos_dev, vel_dev, sp.key[c].p + cnt,
+                                            sp.off[0][c].p + cnt, ctx->g.dim > 1 ? sp.off[1][c].p + cnt : nullptr,
+                                            ctx->g.dim > 2 ? sp.off[2][c].p + cnt : sp.off[0][1 - c].p,
+                                            sp.vel[0][c].p + cnt, sp.vel[1][c].p + cnt, sp.vel[2][c].p + cnt); count_launch(); }
+        } else {
+            { k_load64<<<gb, 256, 0, s>>>(ctx->g, (long long)n, pos_dev, vel_dev, sp.pos64[0][c].p + cnt,
+                                        ctx->g.dim > 1 ? sp.pos64[1][c].p + cnt : nullptr,
+                                        ctx->g.dim > 2 ? sp.pos64[2][c].p + cnt : sp.pos64[0][1 - c].p,
+                                        sp.vel64[0][c].p + cnt, sp.vel64[1][c].p + cnt, sp.vel64[2][c].p + cnt); count_launch(); }
+        }
+    }
+    const long long total = cnt + (long long)n;
+    { k_set_count<<<1, 1, 0, s>>>(ctx->count.p + species, total); count_launch(); }
+    sp.n = total;
+    sp.sorted = false;
+    sp.keys_stale = false;
+    if (ctx->precision == PSUM_PIC_FP64 && total > 0) {
+        double* p3[3] = {sp.pos64[0][c].p, ctx->g.dim > 1 ? sp.pos64[1][c].p : nullptr,
+                         ctx->g.dim > 2 ? sp.pos64[2][c].p : nullptr};
+        launch_keys64(ctx->g, p3, sp.key[c].p, ctx->count.p + species, total, s);
+    }
+    cuda_check(cudaGetLastError(), "append launch");
+}
+
+EXPORT int psum_pic_append(psum_pic_ctx* ctx, int species, unsigned long long n, const double* pos_host,
+                           const double* vel_host) {
+    return guarded([&] {
+        ctx_check(ctx);
+        if (n > 0 && (!pos_host || !vel_host)) throw std::invalid_argument("append: null host array");
+        DevBuf<double> dp, dv;
+        dp.upload(pos_host, (size_t)n * ctx->g.dim, ctx->stream);
+        dv.upload(vel_host, (size_t)n * 3, ctx->stream);
+        append_common(ctx, species, n, dp.p, dv.p);
+        cuda_check(cudaStreamSynchronize(ctx->stream), "append sync");
+    });
+}
+
+EXPORT int psum_pic_append_device(psum_pic_ctx* ctx, int species, unsigned long long n, const double* pos_dev,
+                                  const double* vel_dev) {
+    return guarded([&] {
+        ctx_check(ctx);
+        if (n > 0 && (!pos_dev || !vel_dev)) throw std::invalid_argument("append: null device array");
+        cuda_check(cudaStreamSynchronize(ctx->stream), "append sync");
+        append_common(ctx, species, n, pos_dev, vel_dev);
+        cuda_check(cudaStreamSynchronize(ctx->stream), "append sync");
+    });
+}
+
 EXPORT int psum_pic_load(psum_pic_ctx* ctx, int species, unsigned long long n, const double* pos_host,
                          const double* vel_host) {
     return guarded([&] {

@@ -82,6 +82,20 @@ class ParticleContext:
             n = pos.shape[1]
             check(lib().psum_pic_load(self.handle, species, n, _ptr(pos), _ptr(vel)))
 
+    def append(self, species, pos, vel):
+        """Add particles after the stored ones (PSuM's particle_group::insert);
+        the same array conventions as load.  The species is unsorted afterwards
+        and, as after load, deposit() must run before the next step."""
+        if hasattr(pos, "data_ptr") and getattr(pos, "is_cuda", False):
+            n = pos.shape[1]
+            _ready(pos, vel)
+            check(lib().psum_pic_append_device(self.handle, species, n, pos.data_ptr(), vel.data_ptr()))
+        else:
+            pos = np.ascontiguousarray(pos, np.float64)
+            vel = np.ascontiguousarray(vel, np.float64)
+            n = pos.shape[1]
+            check(lib().psum_pic_append(self.handle, species, n, _ptr(pos), _ptr(vel)))
+
     def count(self, species):
         ns, nv = C.c_ulonglong(), C.c_ulonglong()
         check(lib().psum_pic_count(self.handle, species, C.byref(ns), C.byref(nv)))

@@ -628,3 +628,82 @@ def test_mas_particle_group_round_trip(kind, tmp_path):
     p1, v1 = ctx2.get_state(sp2)
     assert (p1.view(np.int64) == p0.view(np.int64)).all()
     assert (v1.view(np.int64) == v0.view(np.int64)).all()
+
+
+def _identity_solver(g, nn):
+    solver = P.solver_backend("cuda_multigrid64_gpu")
+    dims = [c + 1 for c in g.cells[:g.dim]] + [1] * (3 - g.dim)
+    depth = 1 if nn <= 8192 * 8 else 5
+    solver.set_options(f"I {dims[0]} J {dims[1]} K {dims[2]} depth {depth} max_cycles 0")
+    idx = np.arange(nn, dtype=np.uint64)
+    solver.set_matrix(nn, nn, nn, idx, idx, np.ones(nn))
+    return solver
+
+
+@pytest.mark.parametrize("precision", [P.MIXED, P.FP64])
+@pytest.mark.parametrize("kind", ["2d_absorb", "3d_periodic"])
+def test_append_after_step_equals_load_of_concatenation(precision, kind):
+    # particle_group::insert (particle_group.hpp:103-167) after a step: the
+    # fused step leaves its state in the other buffer with keys implied by
+    # the cell offsets; appended particles follow the stored ones in their
+    # given order, non-finite ones stored as invalid, and the state, its
+    # sort and the next step equal those of one load of the concatenation.
+    ctx, g, pos, vel, phi = make_case(kind, precision, seed=41, n=30000)
+    pos = wrap_into(pos, g)
+    n1 = 18000
+    cap = pos.shape[1] + 64
+    sp = ctx.add_species(-1.0, 1.0, 1.0, cap)
+    ctx.load(sp, pos[:, :n1], vel[:, :n1])
+    ctx.sort()
+    nn = ctx.n_nodes
+    solver = _identity_solver(g, nn)
+    rho, phi_t = dev(np.zeros(nn)), dev(phi)
+    ctx.step(solver, 0.0, rho, phi_t, 0.3)
+    p_a, v_a = ctx.get_state(sp)
+    na = p_a.shape[1]
+    extra_pos, extra_vel = pos[:, n1:].copy(), vel[:, n1:]
+    extra_pos[0, ::9] = np.nan
+    ctx.append(sp, extra_pos, extra_vel)
+    ns, nv = ctx.count(sp)
+    assert ns == na + extra_pos.shape[1]
+    assert nv == na + extra_pos.shape[1] - len(range(0, extra_pos.shape[1], 9))
+
+    ref, _, _, _, _ = make_case(kind, precision, seed=41, n=30000)
+    sr = ref.add_species(-1.0, 1.0, 1.0, cap)
+    ref.load(sr, np.concatenate([p_a, extra_pos], 1), np.concatenate([v_a, extra_vel], 1))
+
+    def same(c1, s1, c2, s2):
+        p1, v1 = c1.get_state(s1)
+        p2, v2 = c2.get_state(s2)
+        k1 = torch.zeros(p1.shape[1], dtype=torch.int32, device="cuda")
+        k2 = torch.zeros(p2.shape[1], dtype=torch.int32, device="cuda")
+        c1.get_keys(s1, k1)
+        c2.get_keys(s2, k2)
+        assert p1.shape == p2.shape
+        assert (np.isnan(p1[0]) == np.isnan(p2[0])).all()
+        ok = ~np.isnan(p1[0])
+        assert (p1[:, ok].view(np.int64) == p2[:, ok].view(np.int64)).all()
+        assert (v1.view(np.int64) == v2.view(np.int64)).all()
+        assert (k1.cpu().numpy() == k2.cpu().numpy()).all()
+
+    same(ctx, sp, ref, sr)
+    ctx.sort()
+    ref.sort()
+    same(ctx, sp, ref, sr)
+    ctx.deposit()          # the accumulators still hold the first step's deposit
+    ref.deposit()
+    rho2 = dev(np.zeros(nn))
+    ref.step(_identity_solver(g, nn), 0.0, rho2, dev(phi), 0.3)
+    ctx.step(solver, 0.0, rho, phi_t, 0.3)
+    torch.cuda.synchronize()
+    same(ctx, sp, ref, sr)
+    assert (rho.cpu().numpy().view(np.int64) == rho2.cpu().numpy().view(np.int64)).all()
+    # beyond the capacity: an error status, nothing stored
+    ns0, _ = ctx.count(sp)
+    with pytest.raises(P.PsumError) as e:
+        ctx.append(sp, pos[:, :cap], vel[:, :cap])
+    assert e.value.code == 6
+    assert ctx.count(sp)[0] == ns0
+    # from device arrays
+    ctx.append(sp, dev(pos[:, :10]), dev(vel[:, :10]))
+    assert ctx.count(sp)[0] == ns0 + 10
