@@ -58,9 +58,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 GPU run and the field comparison")
     ap.add_argument("--cpu-sample", type=int, default=1 << 21, help="particles in the CPU baseline sample")
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "bspline"],
                     help="c2 (default): the bench line; c1/c3/c5: the other plasmas of the scope table; "
-                         "c4: the differentiable run (forward and adjoint)")
+                         "c4: the differentiable run (forward and adjoint); bspline: B-spline gather + deposit")
+    ap.add_argument("--order", type=int, default=2, help="B-spline order of the bspline workload (1-4)")
+    ap.add_argument("--bs-cells", type=int, default=1023, help="cells per axis of the bspline workload")
     ap.add_argument("--mg-extra", default="", help="extra multigrid options (e.g. 'graph 0' to launch the solve's "
                     "kernels one by one, which profilers need)")
     return ap.parse_args()
@@ -562,6 +564,8 @@ def run_workload(args):
     import torch
 
     import psum_b200 as P
+    if args.workload == "bspline":
+        return run_bspline(args, torch, P)
     w = dict(WORKLOADS[args.workload], name=args.workload)
     if args.workload == "c4":
         return run_c4(args, torch, P, w)
@@ -628,6 +632,99 @@ def run_workload(args):
                                   "frac": round(b_step / (ms * 1e-3) / 1e9 / peak, 4)},
             "phase_ms_per_step": {k: round(v[0] / max(v[1], 1), 4) for k, v in phases.items()},
             "mg_last_solve": stats, "valid_particles_end": n_valid, "clocks": clk.summary()}
+
+
+BSPLINE_PPC = 64
+
+
+def run_bspline(args, torch, P):
+    """B-spline gather of the potential's gradient and deposit of every
+    particle (interp_diff_B_spline + add_back_B_spline at --order) on a
+    1024^2-node grid, 64 particles per cell stored cell by cell (the order a
+    sorted PIC state has); one step = one gradient gather and one deposit of
+    all particles.  Algorithmic bytes: per particle the 16 B position read by
+    each kernel and the 16 B gradient written; per node the potential read,
+    the fixed-point words zeroed, accumulated and read, and the field
+    read-modify-write."""
+    from psum_b200 import interp as I
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    cells, ppc, order = args.bs_cells, BSPLINE_PPC, args.order
+    nodes = (cells + 1) ** 2
+    n = cells * cells * ppc
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(SEED + 10 + order)
+    grid = P.simple_grid((0.5, 0.5), (cells + 0.5, cells + 0.5), (cells, cells))
+    cell = torch.arange(n, device=dev, dtype=torch.int64) // ppc
+    pos = torch.empty((2, n), dtype=torch.float64, device=dev)
+    pos[0] = 0.5 + (cell // cells).double() + torch.rand(n, generator=gen, device=dev, dtype=torch.float64)
+    pos[1] = 0.5 + (cell % cells).double() + torch.rand(n, generator=gen, device=dev, dtype=torch.float64)
+    del cell
+    phi = torch.randn(nodes, generator=gen, device=dev, dtype=torch.float64)
+    rho = torch.zeros(nodes, dtype=torch.float64, device=dev)
+    scratch = torch.empty(nodes, dtype=torch.int64, device=dev)
+    grad = torch.empty((2, n), dtype=torch.float64, device=dev)
+    glib = P.lib()
+    gd = I.grid_desc(grid)
+    import ctypes as C
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def gather():
+        P.check(glib.psum_interp_diff_bspline(C.byref(gd), order, n, pos.data_ptr(), phi.data_ptr(), grad.data_ptr(),
+                                              None, stream))
+
+    def deposit():
+        P.check(glib.psum_add_back_bspline(C.byref(gd), order, n, pos.data_ptr(), 1.0 / ppc, rho.data_ptr(),
+                                           scratch.data_ptr(), None, stream))
+
+    for _ in range(args.warmup):
+        gather()
+        deposit()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps + 1)]
+    launches0 = P.lib().psum_kernel_launches()
+    with ClockSampler(0) as clk:
+        ev[0].record()
+        for k in range(args.steps):
+            gather()
+            ev[2 * k + 1].record()
+            deposit()
+            ev[2 * k + 2].record()
+        torch.cuda.synchronize()
+    launches = P.lib().psum_kernel_launches() - launches0
+    g_ms = sum(ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(args.steps)) / args.steps
+    d_ms = sum(ev[2 * k + 1].elapsed_time(ev[2 * k + 2]) for k in range(args.steps)) / args.steps
+    ms = g_ms + d_ms
+    peak, peak_kind = measured_peaks()
+    g_bytes = n * 32 + nodes * 8
+    d_bytes = n * 16 + nodes * (8 * 3 + 16)
+    line = {"workload": "bspline", "metric": "particle gather+deposit/s", "value": n / (ms * 1e-3),
+            "unit": "particles/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"2-D B-spline order {order} gradient gather + deposit, {cells}^2 cells, "
+                                   f"{ppc} particles per cell stored cell by cell", "particles": n, "nodes": nodes,
+                       "order": order, "l2_policy": f"inputs larger than L2 (positions {n * 16 / 1e9:.2f} GB)"},
+            "kernels": {"gather": {"ms": round(g_ms, 4), "algorithmic_bytes": g_bytes,
+                                   "achieved_GBs": round(g_bytes / (g_ms * 1e-3) / 1e9, 1),
+                                   "frac": round(g_bytes / (g_ms * 1e-3) / 1e9 / peak, 4)},
+                        "deposit": {"ms": round(d_ms, 4), "algorithmic_bytes": d_bytes,
+                                    "achieved_GBs": round(d_bytes / (d_ms * 1e-3) / 1e9, 1),
+                                    "frac": round(d_bytes / (d_ms * 1e-3) / 1e9 / peak, 4)}},
+            "peak": peak, "peak_kind": peak_kind, "gpu_launches": int(launches), "clocks": clk.summary()}
+    if not args.no_cpu_baseline:
+        # the oracle's FP64 restatement on the host cores, on a bounded sample
+        from oracle import oracle as O
+        m = min(args.cpu_sample, n)
+        sample = pos[:, :m].cpu().numpy()
+        phi_h = phi.cpu().numpy()
+        g = O.make_grid((cells, cells), (0.5, 0.5), (cells + 0.5, cells + 0.5), (0, 0))
+        t0 = time.perf_counter()
+        O.bspline_gather(g, order, sample, phi_h, grad=True)
+        O.bspline_deposit(g, order, sample, 1.0 / ppc, nodes)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": m / dt, "unit": "particles/s", "cores": os.cpu_count(), "kind": "port",
+                                "sample": f"first {m} particles of the workload, gather (OpenMP) + deposit (serial)"}
+    return line
 
 
 def run_c4(args, torch, P, w):

@@ -584,11 +584,222 @@ double norm2(const std::vector<double>& v) {
 
 thread_local std::string g_err;
 
+// ------------------------------------------------------ B-spline support --
+// The 1-D B-spline weights of orders 2-4 exactly as PSuM writes them
+// (src/field/simple_interpolation.hpp:105-184): quadratic and quartic on the
+// nearest node with s in [-0.5, 0.5], cubic on the corner node with u in
+// [0, 1), each as its piecewise kernel evaluated at the support offsets.
+double bs3(double t) {                                            // :124-130
+    const double a = std::fabs(t);
+    if (a <= 1.0) return 2.0 / 3.0 - a * a + a * a * a / 2.0;
+    if (a <= 2.0) {
+        const double r = 2.0 - a;
+        return r * r * r / 6.0;
+    }
+    return 0.0;
+}
+double bs3d(double t) {                                           // :134-140
+    const double a = std::fabs(t);
+    if (a <= 1.0) return -2.0 * t + 1.5 * t * a;
+    if (a <= 2.0) {
+        const double r = 2.0 - a;
+        return -r * r / 2.0 * (t < 0 ? -1.0 : 1.0);
+    }
+    return 0.0;
+}
+double pow4(double x) { return (x * x) * (x * x); }
+double bs4(double t) {                                            // :153-163
+    const double a = std::fabs(t);
+    if (a <= 0.5) return 115.0 / 192.0 - a * a * (5.0 / 8.0) + a * a * a * a / 4.0;
+    if (a <= 1.5) {
+        const double v = a - 0.5;
+        return 0.5 - (2.0 * v / 3.0 - v * v * v / 3.0 + v * v * v * v / 8.0) - pow4(1.5 - a) / 24.0;
+    }
+    if (a <= 2.5) return pow4(2.5 - a) / 24.0;
+    return 0.0;
+}
+double bs4d(double t) {                                           // :167-177
+    const double a = std::fabs(t);
+    const double sign = t < 0 ? -1.0 : 1.0;
+    if (a <= 0.5) return sign * (-a * 1.25 + a * a * a);
+    if (a <= 1.5) {
+        const double v = a - 0.5;
+        const double r = 1.5 - a;
+        return sign * (-(2.0 / 3.0 - v * v + v * v * v / 2.0) + r * r * r / 6.0);
+    }
+    if (a <= 2.5) {
+        const double r = 2.5 - a;
+        return sign * (-r * r * r / 6.0);
+    }
+    return 0.0;
+}
+
+// 1-D weights and their derivatives in the normalised coordinate.
+void bs_weights(int order, double x, double* w, double* dw) {
+    switch (order) {
+        case 1:                                                    // linear_interp_1D, :92-98
+            w[0] = 1 - x; w[1] = x; dw[0] = -1; dw[1] = 1;
+            break;
+        case 2:                                                    // :106-115
+            w[0] = (0.5 - x) * (0.5 - x) * 0.5; w[1] = 0.75 - x * x; w[2] = (0.5 + x) * (0.5 + x) * 0.5;
+            dw[0] = x - 0.5; dw[1] = -2.0 * x; dw[2] = x + 0.5;
+            break;
+        case 3:
+            for (int k = 0; k < 4; ++k) {
+                w[k] = bs3(x + 1.0 - k);
+                dw[k] = bs3d(x + 1.0 - k);
+            }
+            break;
+        default:
+            for (int k = 0; k < 5; ++k) {
+                w[k] = bs4(x + 2.0 - k);
+                dw[k] = bs4d(x + 2.0 - k);
+            }
+    }
+}
+
+// gen_interp / gen_interp_diff for SupportSize1D = order + 1
+// (simple_grid.hpp:316-397): odd support sizes use the nearest node nN
+// (round, :79-86), even ones the corner node cN (floor, :88-95); the support
+// runs from Shift = -(S/2) (odd) or -(S/2 - 1) (even); support index i has
+// its base-S digit 0 on the last dimension; nodes wrap once by +-(cells+1);
+// interp_tensor(_diff) products as in simple_interpolation.hpp:34-90.
+// Returns false (no support) when a wrapped node is still outside the node
+// range (a position more than a period away, which the reference does not
+// handle) or the position is not finite.
+struct BsSupport {
+    std::vector<long long> idx;
+    std::vector<double> coef;
+    std::vector<double> dcoef[3];
+};
+
+bool bs_support(const Grid& g, int order, const double* p, bool diff, BsSupport& out) {
+    const int D = g.dim, S = order + 1;
+    const bool nearest = S % 2 == 1;
+    const int shift = nearest ? -(S / 2) : -(S / 2 - 1);
+    int base[3];
+    double w1[3][5], dw1[3][5];
+    for (int a = 0; a < D; ++a) {
+        const double u = (p[a] - g.lo[a]) * g.dr[a];
+        if (!std::isfinite(u) || u < -1e9 || u > 1e9) return false;
+        base[a] = nearest ? (int)std::round(u) : (int)std::floor(u);
+        const double base_pos = g.lo[a] + base[a] * g.delta[a];        // nodePosition, :209-214
+        bs_weights(order, (p[a] - base_pos) * g.dr[a], w1[a], dw1[a]);
+        for (int k = 0; k < S; ++k) dw1[a][k] *= g.dr[a];
+    }
+    int count = 1;
+    for (int a = 0; a < D; ++a) count *= S;
+    out.idx.assign(count, 0);
+    out.coef.assign(count, 0.0);
+    for (int d = 0; d < 3; ++d) out.dcoef[d].assign(diff ? count : 0, 0.0);
+    for (int i = 0; i < count; ++i) {
+        int node[3] = {base[0], base[1], base[2]};
+        int digit[3] = {0, 0, 0};
+        int r = i;
+        for (int j = 0; j < D; ++j) {
+            const int a = D - 1 - j;
+            digit[a] = r % S;
+            node[a] += digit[a] + shift;
+            const int w = g.cells[a] + 1;
+            if (node[a] < 0) node[a] += w;
+            else if (node[a] >= w) node[a] -= w;
+            if (node[a] < 0 || node[a] >= w) return false;
+            r /= S;
+        }
+        out.idx[i] = g.n2i(node);
+        double c = 1;
+        for (int j = 0; j < D; ++j) c *= w1[D - 1 - j][digit[D - 1 - j]];
+        out.coef[i] = c;
+        if (diff)
+            for (int d = 0; d < D; ++d) {
+                double cd = 1;
+                for (int j = 0; j < D; ++j) {
+                    const int a = D - 1 - j;
+                    cd *= a == d ? dw1[a][digit[a]] : w1[a][digit[a]];
+                }
+                out.dcoef[d][i] = cd;
+            }
+    }
+    return true;
+}
+
 }  // namespace
 
 extern "C" {
 
 const char* oracle_last_error() { return g_err.c_str(); }
+
+// ------------------------------------------------------- B-spline API ----
+// Support of one point (order 1-4): writes S^D node indices, weights and
+// (dim x S^D) derivative weights; returns S^D, or 0 without support.
+int oracle_bspline_support(const og_grid* gd, int order, const double* p, long long* idx, double* coef,
+                           double* dcoef) {
+    Grid g(gd);
+    BsSupport s;
+    if (!bs_support(g, order, p, true, s)) return 0;
+    const int count = (int)s.idx.size();
+    for (int i = 0; i < count; ++i) {
+        idx[i] = s.idx[i];
+        coef[i] = s.coef[i];
+        for (int d = 0; d < g.dim; ++d) dcoef[d * count + i] = s.dcoef[d][i];
+    }
+    return count;
+}
+
+// interp_B_spline<order> / interp_diff_B_spline<order>
+// (src/field/higher_order_interp.hpp:200-228; generate_interp(_diff),
+// field_interp.hpp:78-113, which skips weights of magnitude <= tol, 1e-10 in
+// the reference) at n SoA positions; points without support give NaN.
+// grad != nullptr selects the gradient (dim x n), else the value (n) goes to out.
+void oracle_bspline_gather(const og_grid* gd, int order, long long n, const double* pos, const double* field,
+                           double* out, double* grad, double tol) {
+    Grid g(gd);
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < n; ++i) {
+        double p[3] = {0, 0, 0};
+        for (int a = 0; a < g.dim; ++a) p[a] = pos[a * n + i];
+        BsSupport s;
+        const bool ok = bs_support(g, order, p, grad != nullptr, s);
+        if (grad) {
+            for (int d = 0; d < g.dim; ++d) {
+                double res = 0;
+                if (ok)
+                    for (size_t k = 0; k < s.idx.size(); ++k)
+                        if (std::fabs(s.dcoef[d][k]) > tol) res += field[s.idx[k]] * s.dcoef[d][k];
+                grad[d * n + i] = ok ? res : NAN;
+            }
+        } else {
+            double res = 0;
+            if (ok)
+                for (size_t k = 0; k < s.idx.size(); ++k)
+                    if (std::fabs(s.coef[k]) > tol) res += field[s.idx[k]] * s.coef[k];
+            out[i] = ok ? res : NAN;
+        }
+    }
+}
+
+// add_back_B_spline<order> (higher_order_interp.hpp:230-245;
+// generate_add_back_mutable for host fields, field_interp.hpp:66-75 with the
+// weight skip at tol, 1e-10 in the reference) of n SoA positions with
+// weight w, in particle order; returns the number of points skipped for lack
+// of support.
+long long oracle_bspline_deposit(const og_grid* gd, int order, long long n, const double* pos, double w,
+                                 double* field, double tol) {
+    Grid g(gd);
+    long long skipped = 0;
+    for (long long i = 0; i < n; ++i) {
+        double p[3] = {0, 0, 0};
+        for (int a = 0; a < g.dim; ++a) p[a] = pos[a * n + i];
+        BsSupport s;
+        if (!bs_support(g, order, p, false, s)) {
+            ++skipped;
+            continue;
+        }
+        for (size_t k = 0; k < s.idx.size(); ++k)
+            if (std::fabs(s.coef[k]) > tol) field[s.idx[k]] += w * s.coef[k];
+    }
+    return skipped;
+}
 
 // ------------------------------------------------------------- CIC API ----
 int oracle_interp(const og_grid* gd, const double* p, long long* idx, double* coef) {

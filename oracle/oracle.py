@@ -66,6 +66,9 @@ def lib():
         L.oracle_kinetic_energy.argtypes = [ll, P, P, d]; L.oracle_kinetic_energy.restype = d
         L.oracle_field_energy.argtypes = [P, P, d]; L.oracle_field_energy.restype = d
         L.oracle_last_error.argtypes = []; L.oracle_last_error.restype = C.c_char_p
+        L.oracle_bspline_support.argtypes = [P, i, P, P, P, P]; L.oracle_bspline_support.restype = i
+        L.oracle_bspline_gather.argtypes = [P, i, ll, P, P, P, P, d]; L.oracle_bspline_gather.restype = None
+        L.oracle_bspline_deposit.argtypes = [P, i, ll, P, d, P, d]; L.oracle_bspline_deposit.restype = ll
         _lib = L
     return _lib
 
@@ -113,6 +116,37 @@ def deposit(grid, pos, w, n_nodes):
     rho = np.zeros(n_nodes)
     lib().oracle_deposit(C.byref(grid), pos.shape[1], _p(pos), w, _p(rho))
     return rho
+
+
+def bspline_support(grid, order, p):
+    """(node indices, weights, derivative weights (dim, S^D)) of one point at
+    B-spline order 1-4; empty arrays when the point has no support."""
+    m = (order + 1) ** grid.dim
+    idx = np.zeros(m, np.int64); coef = np.zeros(m); dcoef = np.zeros(grid.dim * m)
+    k = lib().oracle_bspline_support(C.byref(grid), order, _p(_f64(p)), _p(idx), _p(coef), _p(dcoef))
+    return idx[:k], coef[:k], dcoef[:grid.dim * k].reshape(grid.dim, k)
+
+
+def bspline_gather(grid, order, pos, field, grad=False, tol=1e-10):
+    """interp_B_spline / interp_diff_B_spline at (dim, n) positions; tol is the
+    weight skip threshold (1e-10 in the reference, 0 for the full sum)."""
+    pos = _f64(pos); field = _f64(field)
+    n = pos.shape[1]
+    if grad:
+        out = np.zeros((grid.dim, n))
+        lib().oracle_bspline_gather(C.byref(grid), order, n, _p(pos), _p(field), None, _p(out), tol)
+    else:
+        out = np.zeros(n)
+        lib().oracle_bspline_gather(C.byref(grid), order, n, _p(pos), _p(field), _p(out), None, tol)
+    return out
+
+
+def bspline_deposit(grid, order, pos, w, n_nodes, tol=1e-10):
+    """add_back_B_spline of (dim, n) positions with weight w into a zero field."""
+    pos = _f64(pos)
+    field = np.zeros(n_nodes)
+    skipped = lib().oracle_bspline_deposit(C.byref(grid), order, pos.shape[1], _p(pos), w, _p(field), tol)
+    return field, skipped
 
 
 def bin_particles(grid, pos):

@@ -1,17 +1,20 @@
 """psum_b200 -- B200 (sm_100a) electrostatic PIC step behind PSuM's plugin ABI.
 
 Native library: ``libpsum_b200.so`` (built in-tree by ``psum_b200.build``),
-exporting the solver plugin ABI of include/psum_field_solver.h and the
-particle-kernel set of include/psum_pic.h.  The Python modules are thin
+exporting the solver plugin ABI of include/psum_field_solver.h, the
+particle-kernel set of include/psum_pic.h and the B-spline interpolation of
+include/psum_interp.h.  The Python modules are thin
 ctypes mirrors of the reference interfaces; there is no CPU fallback.
 """
 from ._lib import LIB_PATH, PROTOTYPES, PsumError, check, lib
 from .field_solver import (Dirichlet_box, Dirichlet_func, Dirichlet_line, Dirichlet_nodes, Dirichlet_plane,
                            MixedBoundary, Neumann_line, Poisson_solver_2d, Poisson_solver_3d, Robin_Line,
                            assemble_poisson, assemble_poisson_2d, registered_table, simple_grid, solver_backend)
+from .interp import add_back_B_spline, interp_B_spline, interp_diff_B_spline
 from .pic import BORIS, FP64, LEAPFROG, MIXED, ParticleContext
 
 __all__ = ["LIB_PATH", "PROTOTYPES", "PsumError", "check", "lib", "Dirichlet_line", "Dirichlet_nodes",
            "Dirichlet_plane", "Dirichlet_box", "Dirichlet_func", "Neumann_line", "Robin_Line", "MixedBoundary",
            "Poisson_solver_2d", "Poisson_solver_3d", "assemble_poisson", "assemble_poisson_2d", "registered_table",
-           "simple_grid", "solver_backend", "ParticleContext", "MIXED", "FP64", "LEAPFROG", "BORIS"]
+           "simple_grid", "solver_backend", "ParticleContext", "MIXED", "FP64", "LEAPFROG", "BORIS",
+           "interp_B_spline", "interp_diff_B_spline", "add_back_B_spline"]

@@ -1,5 +1,5 @@
 """Loader and ctypes prototypes of libpsum_b200.so (include/psum_field_solver.h,
-include/psum_pic.h).
+include/psum_pic.h, include/psum_interp.h).
 
 The library is built in-tree (``psum_b200/libpsum_b200.so``) by
 ``psum_b200.build.build()``.  There is no fallback: every entry point of this
@@ -91,6 +91,11 @@ PROTOTYPES = {
     "psum_pic_adjoint_push": (I, [P, I, P, D, P, P, P]),
     "psum_pic_adjoint_deposit": (I, [P, I, P, P]),
     "psum_bin_positions_noalloc": (I, [C.POINTER(GridDesc), ULL, P, P, P, P, P, C.POINTER(ULL), P]),
+    # B-spline interpolation (include/psum_interp.h)
+    "psum_interp_bspline": (I, [C.POINTER(GridDesc), I, ULL, P, P, P, P, P]),
+    "psum_interp_diff_bspline": (I, [C.POINTER(GridDesc), I, ULL, P, P, P, P, P]),
+    "psum_add_back_bspline": (I, [C.POINTER(GridDesc), I, ULL, P, D, P, P, P, P]),
+    "psum_bspline_deposit_bits": (I, [ULL, C.POINTER(I)]),
 }
 
 STATUS = {0: "PSUM_OK", 1: "PSUM_ERR_INVALID_ARGUMENT", 2: "PSUM_ERR_NOT_READY", 3: "PSUM_ERR_CUDA",

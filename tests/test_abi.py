@@ -15,7 +15,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_symbols():
     names = set()
-    for h in ("psum_field_solver.h", "psum_pic.h"):
+    for h in ("psum_field_solver.h", "psum_pic.h", "psum_interp.h"):
         text = open(os.path.join(ROOT, "include", h)).read()
         for m in re.finditer(r"EXPORT\s+[\w\s\*]+?\b(\w+)\s*\(", text):
             names.add(m.group(1))
