@@ -84,6 +84,7 @@ public:
     particle_group& operator=(const particle_group&) = delete;
 
     int species() const { return species_; }
+    psum_pic_ctx* context() const { return ctx_; }
     std::size_t capacity() const { return capacity_; }
 
     std::size_t size() const {

@@ -109,6 +109,10 @@ EXPORT int psum_pic_count(psum_pic_ctx* ctx, int species, unsigned long long* n_
 /* Copies the species state, in storage order, into FP64 SoA host arrays of
  * n_stored entries; invalid particles have pos[0] = NaN. */
 EXPORT int psum_pic_get_state(psum_pic_ctx* ctx, int species, double* pos_host, double* vel_host);
+/* Same, into FP64 SoA device arrays of n_stored entries (pos_dev[d*n + i],
+ * vel_dev[c*n + i]); returns after the copy is complete.  These are the
+ * positions the B-spline calls of psum_interp.h take. */
+EXPORT int psum_pic_get_state_device(psum_pic_ctx* ctx, int species, double* pos_dev, double* vel_dev);
 /* Internal cell key per stored particle (row-major over the internal cell
  * lattice; invalid = -1) into an int32 device array of n_stored entries. */
 EXPORT int psum_pic_get_keys(psum_pic_ctx* ctx, int species, int* keys_dev);

@@ -69,6 +69,7 @@ PROTOTYPES = {
     "psum_pic_load_device": (I, [P, I, ULL, P, P]),
     "psum_pic_count": (I, [P, I, C.POINTER(ULL), C.POINTER(ULL)]),
     "psum_pic_get_state": (I, [P, I, P, P]),
+    "psum_pic_get_state_device": (I, [P, I, P, P]),
     "psum_pic_get_keys": (I, [P, I, P]),
     "psum_pic_sort": (I, [P]),
     "psum_pic_bin": (I, [P, I, P, P, P, P, C.POINTER(ULL)]),

@@ -342,6 +342,111 @@ __global__ void __launch_bounds__(kBsThreads) k_bs_deposit(BsGrid g, long long n
     }
 }
 
+// Deposit of the nearest-node orders (2 and 4).  Particles of one cell have
+// up to 2^D different nearest nodes, hence up to 2^D stencils; grouping lanes
+// by their floor cell instead, each lane writes its S weights into the
+// cell's union stencil of S + 1 nodes per axis (starting at floor - S/2, its
+// own stencil at offset 0 or 1), so one cell is one group.  The summed values
+// and their bits are those of k_bs_deposit: the same per-node weights, the
+// same products, integer sums.  A node of the union stencil that fails the
+// single wrap carries zero weight for every supported lane of the group (each
+// lane's own nodes all passed it), so it is never written; its offset is
+// clamped to 0 all the same.
+template <int D, int ORDER>
+__global__ void __launch_bounds__(kBsThreads) k_bs_deposit_near(BsGrid g, long long n, const double* __restrict__ pos,
+                                                                double scale, unsigned long long* __restrict__ acc,
+                                                                unsigned long long* __restrict__ skipped) {
+    constexpr int S = ORDER + 1;
+    static_assert(S % 2 == 1, "nearest-node orders only");
+    constexpr int E = S + 1;
+    constexpr int kShift = -(S / 2);
+    constexpr int E1 = D > 1 ? E : 1;
+    constexpr int E2 = D > 2 ? E : 1;
+    constexpr unsigned kFull = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = i < n;
+    int off[3][E];
+    double we[3][E];
+    long long key = 0;
+    bool ok = active;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (a < D) {
+            const double p = active ? pos[(long long)a * n + i] : 0.0;
+            const double u = (p - g.lo[a]) * g.dr[a];
+            bool oka = u > -(double)(S + 1) && u < (double)(g.N[a] + S + 1);   // also rejects NaN
+            const double uc = oka ? u : 0.0;
+            const int fl = (int)floor(uc);
+            const int nr = (int)round(uc);
+            const bool up = nr != fl;   // own stencil at offset 1 of the union stencil
+            double w[S];
+            weights<ORDER>(oka ? (p - (g.lo[a] + nr * g.delta[a])) * g.dr[a] : 0.0, w);
+            const int Na = g.N[a];
+#pragma unroll
+            for (int j = 0; j < E; ++j) {
+                int nd = fl + kShift + j;
+                if (nd < 0) nd += Na;
+                else if (nd >= Na) nd -= Na;
+                const bool valid = nd >= 0 && nd < Na;
+                const bool mine = up ? j >= 1 : j < S;
+                oka = oka && (!mine || valid);
+                off[a][j] = valid ? nd * g.stride[a] : 0;
+                const double wl = j < S ? w[j] : 0.0;
+                const double wu = j >= 1 ? w[j >= 1 ? j - 1 : 0] : 0.0;
+                we[a][j] = up ? wu : wl;
+            }
+            ok = ok && oka;
+            key = key * (long long)(Na + 2 * S + 4) + (fl + S + 2);
+        } else {
+#pragma unroll
+            for (int j = 0; j < E; ++j) {
+                off[a][j] = 0;
+                we[a][j] = j == 0 ? 1.0 : 0.0;
+            }
+        }
+    }
+    if (active && !ok && skipped) atomicAdd(skipped, 1ULL);
+    auto q_at = [&](int k0, int k1, int k2) -> unsigned long long {
+        double c = 1.0;
+        if (D > 2) c *= we[2][k2];
+        if (D > 1) c *= we[1][k1];
+        c *= we[0][k0];
+        return c > 1e-10 ? (unsigned long long)__double2ll_rn(c * scale) : 0ULL;
+    };
+    const long long gkey = ok ? key : -1LL;
+    const unsigned grp = __match_any_sync(kFull, gkey);
+    const unsigned leaders = __ballot_sync(kFull, ok && __ffs(grp) - 1 == lane);
+    if (__popc(leaders) <= kAggGroups) {
+#pragma unroll
+        for (int k0 = 0; k0 < E; ++k0)
+#pragma unroll
+            for (int k1 = 0; k1 < E1; ++k1)
+#pragma unroll
+                for (int k2 = 0; k2 < E2; ++k2) {
+                    const unsigned long long q = ok ? q_at(k0, k1, k2) : 0ULL;
+                    for (unsigned rem = leaders; rem; rem &= rem - 1) {
+                        const int l = __ffs(rem) - 1;
+                        const unsigned long long qm = (grp >> l) & 1u ? q : 0ULL;
+                        const unsigned lo = __reduce_add_sync(kFull, (unsigned)(qm & 0x7ffffffULL));
+                        const unsigned hi = __reduce_add_sync(kFull, (unsigned)(qm >> 27));
+                        const unsigned long long t = ((unsigned long long)hi << 27) + lo;
+                        if (lane == l && t) atomicAdd(acc + (off[0][k0] + off[1][k1] + off[2][k2]), t);
+                    }
+                }
+    } else if (ok) {
+#pragma unroll
+        for (int k0 = 0; k0 < E; ++k0)
+#pragma unroll
+            for (int k1 = 0; k1 < E1; ++k1)
+#pragma unroll
+                for (int k2 = 0; k2 < E2; ++k2) {
+                    const unsigned long long q = q_at(k0, k1, k2);
+                    if (q) atomicAdd(acc + (off[0][k0] + off[1][k1] + off[2][k2]), q);
+                }
+    }
+}
+
 __global__ void k_bs_finish(long long n_nodes, const unsigned long long* __restrict__ acc, double w_unit,
                             double* __restrict__ field) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -376,9 +481,9 @@ void launch_deposit_d(int order, const BsGrid& g, long long n, const double* pos
                       unsigned long long* acc, unsigned long long* skipped, cudaStream_t s) {
     switch (order) {
         case 1: k_bs_deposit<D, 1><<<blocks(n), kBsThreads, 0, s>>>(g, n, pos, scale, acc, skipped); break;
-        case 2: k_bs_deposit<D, 2><<<blocks(n), kBsThreads, 0, s>>>(g, n, pos, scale, acc, skipped); break;
+        case 2: k_bs_deposit_near<D, 2><<<blocks(n), kBsThreads, 0, s>>>(g, n, pos, scale, acc, skipped); break;
         case 3: k_bs_deposit<D, 3><<<blocks(n), kBsThreads, 0, s>>>(g, n, pos, scale, acc, skipped); break;
-        default: k_bs_deposit<D, 4><<<blocks(n), kBsThreads, 0, s>>>(g, n, pos, scale, acc, skipped); break;
+        default: k_bs_deposit_near<D, 4><<<blocks(n), kBsThreads, 0, s>>>(g, n, pos, scale, acc, skipped); break;
     }
     count_launch();
 }

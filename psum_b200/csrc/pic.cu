@@ -2294,39 +2294,64 @@ EXPORT int psum_pic_count(psum_pic_ctx* ctx, int species, unsigned long long* n_
     });
 }
 
+// The species state (n stored particles, storage order) as FP64 SoA device
+// arrays pos[d*n + i], vel[c*n + i]; invalid particles get x = NaN.
+static void export_state(psum_pic_ctx* ctx, Species& sp, long long n, double* pos, double* vel) {
+    const int D = ctx->g.dim;
+    const int cur = sp.cur;
+    if (ctx->precision == PSUM_PIC_MIXED) {
+        ensure_keys(ctx, sp);
+        { k_export_mixed<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(
+            ctx->g, n, sp.key[cur].p, sp.off[0][cur].p, D > 1 ? sp.off[1][cur].p : nullptr,
+            D > 2 ? sp.off[2][cur].p : nullptr, sp.vel[0][cur].p, sp.vel[1][cur].p, sp.vel[2][cur].p, pos, vel); count_launch(); }
+    } else {
+        for (int a = 0; a < D; ++a)
+            cuda_check(cudaMemcpyAsync(pos + (size_t)a * n, sp.pos64[a][cur].p, sizeof(double) * n,
+                                       cudaMemcpyDeviceToDevice, ctx->stream),
+                       "copy");
+        for (int q = 0; q < 3; ++q)
+            cuda_check(cudaMemcpyAsync(vel + (size_t)q * n, sp.vel64[q][cur].p, sizeof(double) * n,
+                                       cudaMemcpyDeviceToDevice, ctx->stream),
+                       "copy");
+    }
+}
+
+static long long stored_count(psum_pic_ctx* ctx, Species& sp, int species) {
+    long long n = 0;
+    cuda_check(cudaMemcpyAsync(&n, ctx->count.p + species, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream),
+               "count copy");
+    cuda_check(cudaStreamSynchronize(ctx->stream), "count sync");
+    sp.n = n;
+    return n;
+}
+
 EXPORT int psum_pic_get_state(psum_pic_ctx* ctx, int species, double* pos_host, double* vel_host) {
     return guarded([&] {
         ctx_check(ctx);
         Species& sp = species_at(ctx, species);
-        long long n = 0;
-        cuda_check(cudaMemcpyAsync(&n, ctx->count.p + species, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream),
-                   "count copy");
-        cuda_check(cudaStreamSynchronize(ctx->stream), "count sync");
-        sp.n = n;
+        const long long n = stored_count(ctx, sp, species);
         if (n == 0) return;
         if (!pos_host || !vel_host) throw std::invalid_argument("get_state: null host array");
         const int D = ctx->g.dim;
         DevBuf<double> dp, dv;
         dp.alloc((size_t)n * D);
         dv.alloc((size_t)n * 3);
-        const int cur = sp.cur;
-        if (ctx->precision == PSUM_PIC_MIXED) {
-            ensure_keys(ctx, sp);
-            { k_export_mixed<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(
-                ctx->g, n, sp.key[cur].p, sp.off[0][cur].p, D > 1 ? sp.off[1][cur].p : nullptr,
-                D > 2 ? sp.off[2][cur].p : nullptr, sp.vel[0][cur].p, sp.vel[1][cur].p, sp.vel[2][cur].p, dp.p, dv.p); count_launch(); }
-        } else {
-            for (int a = 0; a < D; ++a)
-                cuda_check(cudaMemcpyAsync(dp.p + (size_t)a * n, sp.pos64[a][cur].p, sizeof(double) * n,
-                                           cudaMemcpyDeviceToDevice, ctx->stream),
-                           "copy");
-            for (int q = 0; q < 3; ++q)
-                cuda_check(cudaMemcpyAsync(dv.p + (size_t)q * n, sp.vel64[q][cur].p, sizeof(double) * n,
-                                           cudaMemcpyDeviceToDevice, ctx->stream),
-                           "copy");
-        }
+        export_state(ctx, sp, n, dp.p, dv.p);
         cuda_check(cudaMemcpyAsync(pos_host, dp.p, sizeof(double) * n * D, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
         cuda_check(cudaMemcpyAsync(vel_host, dv.p, sizeof(double) * n * 3, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+        cuda_check(cudaStreamSynchronize(ctx->stream), "get_state sync");
+    });
+}
+
+EXPORT int psum_pic_get_state_device(psum_pic_ctx* ctx, int species, double* pos_dev, double* vel_dev) {
+    return guarded([&] {
+        ctx_check(ctx);
+        Species& sp = species_at(ctx, species);
+        const long long n = stored_count(ctx, sp, species);
+        if (n == 0) return;
+        if (!pos_dev || !vel_dev) throw std::invalid_argument("get_state_device: null device array");
+        export_state(ctx, sp, n, pos_dev, vel_dev);
+        cuda_check(cudaGetLastError(), "export launch");
         cuda_check(cudaStreamSynchronize(ctx->stream), "get_state sync");
     });
 }

@@ -108,6 +108,18 @@ class ParticleContext:
         check(lib().psum_pic_get_state(self.handle, species, _ptr(pos), _ptr(vel)))
         return pos, vel
 
+    def get_state_device(self, species):
+        """The stored particles as (dim, n) and (3, n) float64 CUDA tensors
+        (invalid particles have x = NaN): the positions the B-spline
+        functions of psum_b200.interp take."""
+        import torch
+        ns, _ = self.count(species)
+        pos = torch.empty((self.dim, ns), dtype=torch.float64, device="cuda")
+        vel = torch.empty((3, ns), dtype=torch.float64, device="cuda")
+        self._order(pos, vel)
+        check(lib().psum_pic_get_state_device(self.handle, species, _ptr(pos), _ptr(vel)))
+        return pos, vel
+
     def get_keys(self, species, out):
         self._order(out)
         check(lib().psum_pic_get_keys(self.handle, species, _ptr(out)))
