@@ -143,19 +143,32 @@ def _node_positions(grid):
     return np.meshgrid(grid.lower[0] + i * grid.delta[0], grid.lower[1] + j * grid.delta[1], indexing="ij")
 
 
+def _node_coords(grid):
+    """Flattened node coordinates per axis (nodePosition, simple_grid.hpp:209-214)."""
+    axes = [grid.lower[a] + np.arange(grid.cells[a] + 1) * grid.delta[a] for a in range(grid.dim)]
+    return [c.reshape(-1) for c in np.meshgrid(*axes, indexing="ij")]
+
+
+# boundary directions: (axis, side) of boundary_direction_2d / boundary_direction_3d
+DIRECTIONS = {2: {"E": (0, 1), "W": (0, -1), "N": (1, 1), "S": (1, -1)},
+              3: {"Xpos": (0, 1), "Xneg": (0, -1), "Ypos": (1, 1), "Yneg": (1, -1), "Zpos": (2, 1), "Zneg": (2, -1)}}
+
+
 class MixedBoundary:
-    """mixed_boundary<2> (src/field_solver/mixed_boundary.hpp:17-150): the
-    nodes of one boundary line with the condition
+    """mixed_boundary<D> (src/field_solver/mixed_boundary.hpp:17-150): the
+    nodes of one boundary line (2-D) or plane (3-D) with the condition
 
         a * phi + b * dphi/dn = value      (n: the outward normal of `direction`)
 
-    where (a, b) = coeffs (a pair, or a function of (x, y) giving one) and
-    value is a number or a function of (x, y).  ``set`` plays the role of
-    PSuM's ``boundary = value``."""
+    where (a, b) = coeffs (a pair, or a function of the node coordinates
+    giving one) and value is a number or a function of the node coordinates.
+    Directions are N, S, E, W in 2-D and Xneg, Xpos, Yneg, Ypos, Zneg, Zpos in
+    3-D.  ``set`` plays the role of PSuM's ``boundary = value``."""
 
     def __init__(self, grid, nodes, direction, coeffs, value=None):
-        if direction not in ("N", "S", "E", "W"):
-            raise ValueError("direction must be one of N, S, E, W")
+        names = DIRECTIONS.get(grid.dim, {})
+        if direction not in names:
+            raise ValueError(f"direction must be one of {', '.join(names) or '(2-D or 3-D grids only)'}")
         self.grid = grid
         self.nodes = np.asarray(nodes, np.int64)
         self.direction = direction
@@ -167,21 +180,20 @@ class MixedBoundary:
         return self
 
     def _positions(self):
-        x, y = _node_positions(self.grid)
-        return x.reshape(-1)[self.nodes], y.reshape(-1)[self.nodes]
+        return [c[self.nodes] for c in _node_coords(self.grid)]
 
     def values(self):
         if self.value is None:
             raise ValueError("mixed_boundary::evaluate: no value is set")
-        x, y = self._positions()
+        pos = self._positions()
         if callable(self.value):
-            return np.array([float(self.value(a, b)) for a, b in zip(x, y)])
+            return np.array([float(self.value(*p)) for p in zip(*pos)])
         return np.full(self.nodes.size, float(self.value))
 
     def coefficient_pairs(self):
-        x, y = self._positions()
+        pos = self._positions()
         if callable(self.coeffs):
-            pairs = np.array([self.coeffs(a, b) for a, b in zip(x, y)], np.float64).reshape(-1, 2)
+            pairs = np.array([self.coeffs(*p) for p in zip(*pos)], np.float64).reshape(-1, 2)
         else:
             pairs = np.tile(np.asarray(self.coeffs, np.float64), (self.nodes.size, 1))
         return pairs[:, 0], pairs[:, 1]
@@ -219,6 +231,40 @@ def Robin_Line(grid, direction, coef_value_and_grad, value=None, min_max=None):
     """a * phi + b * dphi/dn = value on a boundary line (Robin.hpp:55-110);
     coef_value_and_grad is (a, b) or a function of (x, y) giving it."""
     return MixedBoundary(grid, _line_nodes(grid, direction, min_max), direction, coef_value_and_grad, value)
+
+
+def _plane_nodes(grid, direction, min_max):
+    """Boundary plane nodes of a 3-D grid (Neumann.hpp:96-128, Robin.hpp:116-150):
+    i = 0 / I for Xneg / Xpos, j = 0 / J for Yneg / Ypos, k = 0 / K for Zneg /
+    Zpos; with min_max only those whose x (Y and Z planes) or y (X planes)
+    lies in [min, max]."""
+    if grid.dim != 3:
+        raise ValueError("a 3-D grid is required")
+    if direction not in DIRECTIONS[3]:
+        raise ValueError("direction must be one of " + ", ".join(DIRECTIONS[3]))
+    axis, side = DIRECTIONS[3][direction]
+    dims = tuple(c + 1 for c in grid.cells)
+    idx = np.arange(int(np.prod(dims))).reshape(dims)
+    sel = [slice(None)] * 3
+    sel[axis] = 0 if side < 0 else dims[axis] - 1
+    nodes = np.sort(idx[tuple(sel)].reshape(-1))
+    if min_max is not None:
+        coords = _node_coords(grid)
+        along = coords[1] if axis == 0 else coords[0]
+        v = along[nodes]
+        nodes = nodes[~((v < min_max[0]) | (v > min_max[1]))]
+    return nodes.tolist()
+
+
+def Neumann_plane(grid, direction, value=None, min_max=None):
+    """dphi/dn = value on a boundary plane (Neumann.hpp:96-133)."""
+    return MixedBoundary(grid, _plane_nodes(grid, direction, min_max), direction, (0.0, 1.0), value)
+
+
+def Robin_plane(grid, direction, coef_value_and_grad, value=None, min_max=None):
+    """a * phi + b * dphi/dn = value on a boundary plane (Robin.hpp:116-163);
+    coef_value_and_grad is (a, b) or a function of (x, y, z) giving it."""
+    return MixedBoundary(grid, _plane_nodes(grid, direction, min_max), direction, coef_value_and_grad, value)
 
 
 def _merge_mixed(mixed_boundaries, fixed_idx):
@@ -340,6 +386,109 @@ def assemble_poisson_2d(grid, domain, fixed_nodes, mixed_boundaries=(), epsilon=
     cc = np.concatenate(cols).astype(np.int64)
     v = np.concatenate(vals)
     # coalesce duplicates (a cyclic neighbour or a ghost's partner can repeat a column)
+    key = r * n + cc
+    order = np.argsort(key, kind="stable")
+    key, v = key[order], v[order]
+    uniq, start = np.unique(key, return_index=True)
+    v = np.add.reduceat(v, start)
+    keep = v != 0.0
+    uniq, v = uniq[keep], v[keep]
+    A = ((uniq // n).astype(np.uint64), (uniq % n).astype(np.uint64), v)
+    M = (np.asarray(add_rows, np.int64), np.asarray(add_vals), entries)
+    return A, M
+
+
+def assemble_poisson_3d(grid, fixed_nodes, mixed_boundaries=(), epsilon=8.854e-12):
+    """Operator of Poisson_solver_3d::_init_impl (Poisson_solver_3d.hpp:178-349):
+    the 7-point finite-volume stencil with epsilon a number or a function of
+    (x, y, z) taken at the face midpoints (the mean of the two node
+    positions, :311-322), cyclic neighbours (:221-227), and mixed boundaries
+    by ghost nodes eliminated per node as in assemble_poisson_2d: a mixed
+    node's neighbour across the boundary is the ghost
+    phi_opposite + 2 (value - a phi) / (b dr).
+
+    Returns ((rows, cols, vals) of A', (addback_rows, M_vals, mixed_entries))
+    with the meaning of assemble_poisson_2d's result."""
+    if grid.dim != 3:
+        raise ValueError("a 3-D grid is required")
+    dims = [c + 1 for c in grid.cells]
+    nI, nJ, nK = dims
+    n = nI * nJ * nK
+    d = list(grid.delta)
+    dr = [1.0 / v for v in d]
+    ii, jj, kk = [a.reshape(-1) for a in np.meshgrid(np.arange(nI), np.arange(nJ), np.arange(nK), indexing="ij")]
+    ijk = [ii, jj, kk]
+    node = (ii * nJ + jj) * nK + kk
+
+    def at(i, j, k):
+        return ((i % nI) * nJ + (j % nJ)) * nK + (k % nK)
+
+    names = DIRECTIONS[3]
+    nbr = {}
+    for name, (axis, side) in names.items():
+        shifted = [v.copy() for v in ijk]
+        shifted[axis] = shifted[axis] + side
+        nbr[name] = at(*shifted)
+    pos = [grid.lower[a] + ijk[a] * d[a] for a in range(3)]
+    if callable(epsilon):
+        eps_f = np.vectorize(lambda a, b, c: float(epsilon(a, b, c)), otypes=[np.float64])
+    else:
+        eps_f = lambda a, b, c: np.full(np.shape(a), float(epsilon))
+    eps = {}
+    for name, (axis, side) in names.items():
+        mid = list(pos)
+        mid[axis] = (pos[axis] + (grid.lower[axis] + (ijk[axis] + side) * d[axis])) / 2
+        eps[name] = eps_f(*mid)
+    surface = [d[1] * d[2], d[0] * d[2], d[0] * d[1]]
+    m = -1.0 / (d[0] * d[1] * d[2])
+    c = {name: ((dr[axis] * surface[axis]) * eps[name]) * m for name, (axis, _) in names.items()}
+    # (grad_E S eps_E - grad_W S eps_W + grad_N S eps_N - grad_S S eps_S + grad_U S eps_U - grad_D S eps_D) * (-1 / V)
+    cen = (-dr[0] * surface[0]) * eps["Xpos"] - (dr[0] * surface[0]) * eps["Xneg"]
+    cen = cen + (-dr[1] * surface[1]) * eps["Ypos"]
+    cen = cen - (dr[1] * surface[1]) * eps["Yneg"]
+    cen = cen + (-dr[2] * surface[2]) * eps["Zpos"]
+    cen = (cen - (dr[2] * surface[2]) * eps["Zneg"]) * m
+    fixed = np.zeros(n, bool)
+    fixed[np.asarray(fixed_nodes, np.int64)] = True
+    entries = _merge_mixed(list(mixed_boundaries), np.nonzero(fixed)[0])
+    opposite = {"Xpos": "Xneg", "Xneg": "Xpos", "Ypos": "Yneg", "Yneg": "Ypos", "Zpos": "Zneg", "Zneg": "Zpos"}
+    ghost = {name: np.zeros(n, bool) for name in names}
+    extra_r, extra_c, extra_v = [], [], []
+    add_rows, add_vals = [], []
+    coef_cache = {}
+    for nd, dname, b, k in entries:
+        if b not in coef_cache:
+            coef_cache[b] = mixed_boundaries[b].coefficient_pairs()
+        a_val, b_grad = coef_cache[b][0][k], coef_cache[b][1][k]
+        if b_grad == 0.0:
+            raise ValueError("a mixed boundary needs a non-zero gradient coefficient (use a fixed boundary)")
+        if ghost[opposite[dname]][nd]:
+            raise ValueError("a node with mixed boundaries on opposite sides is not supported")
+        ghost[dname][nd] = True
+        drd = dr[names[dname][0]]
+        cg = c[dname][nd]
+        extra_r += [nd, nd]
+        extra_c += [nbr[opposite[dname]][nd], nd]
+        extra_v += [cg, cg * (-2.0 * a_val / (b_grad * drd))]
+        add_rows.append(nd)
+        add_vals.append(-cg * 2.0 / (b_grad * drd))
+    free = ~fixed
+    rows, cols, vals = [np.nonzero(fixed)[0]], [np.nonzero(fixed)[0]], [np.ones(int(fixed.sum()))]
+    rows.append(node[free])
+    cols.append(node[free])
+    vals.append(cen[free])
+    for name in names:
+        sel = free & ~ghost[name]
+        rows.append(node[sel])
+        cols.append(nbr[name][sel])
+        vals.append(c[name][sel])
+    if extra_r:
+        rows.append(np.asarray(extra_r, np.int64))
+        cols.append(np.asarray(extra_c, np.int64))
+        vals.append(np.asarray(extra_v))
+    r = np.concatenate(rows).astype(np.int64)
+    cc = np.concatenate(cols).astype(np.int64)
+    v = np.concatenate(vals)
     key = r * n + cc
     order = np.argsort(key, kind="stable")
     key, v = key[order], v[order]
@@ -491,22 +640,27 @@ class _PoissonFrontend:
             self.backend.set_options(options)
 
     def init(self, backend_name, grid, domain, fixed_boundaries, epsilon=8.854e-12, mixed_boundaries=()):
-        """Poisson_solver_2d::init / _init_impl (:182-404): fixed (Dirichlet)
-        boundaries, and in 2-D mixed (Neumann / Robin) boundaries, the
-        cylindrical domain and an epsilon function of (x, y)."""
+        """Poisson_solver_{2,3}d::init / _init_impl (Poisson_solver_2d.hpp:182-404,
+        Poisson_solver_3d.hpp:178-395): fixed (Dirichlet) boundaries, mixed
+        (Neumann / Robin) boundaries and an epsilon function of the node
+        coordinates; in 2-D also the cylindrical domain."""
         if grid.dim != self.dim:
             raise ValueError(f"grid must be {self.dim}-D")
         general = bool(mixed_boundaries) or domain != self.Cartesian or callable(epsilon)
-        if domain not in (self.Cartesian, self.Cylindrical) or (general and self.dim != 2):
-            raise ValueError("mixed boundaries, the cylindrical domain and epsilon functions are provided in 2-D")
+        if domain not in (self.Cartesian, self.Cylindrical) or (domain == self.Cylindrical and self.dim != 2):
+            raise ValueError("the cylindrical domain is provided in 2-D; 3-D domains are Cartesian")
         if backend_name == "native":
             raise PsumError(1, "the 'native' Eigen direct solver is not part of this backend; "
                                "use cuda_multigrid32f_gpu or cuda_multigrid64_gpu")
         self.grid = grid
         self.replace_idx, self.replace_val = _merge_fixed(fixed_boundaries)
-        if general:
+        if general and self.dim == 2:
             (rows, cols, vals), self.mixed_M = assemble_poisson_2d(grid, domain, self.replace_idx,
                                                                    list(mixed_boundaries), epsilon)
+            self.mixed = list(mixed_boundaries)
+        elif general:
+            (rows, cols, vals), self.mixed_M = assemble_poisson_3d(grid, self.replace_idx, list(mixed_boundaries),
+                                                                   epsilon)
             self.mixed = list(mixed_boundaries)
         else:
             rows, cols, vals = assemble_poisson(grid, self.replace_idx, epsilon)
