@@ -29,7 +29,7 @@ import numpy as np
 import torch
 
 from . import field_solver as _fs
-from .pic import FP64, MIXED, ParticleContext
+from .pic import MIXED, ParticleContext
 
 
 def field_energy_loss(phi, shape, dx, periodic):

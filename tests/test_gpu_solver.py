@@ -1,5 +1,4 @@
 """GPU parity of the multigrid backends against the FP64 oracle (through the C ABI)."""
-import ctypes as C
 
 import numpy as np
 import pytest
@@ -325,7 +324,6 @@ def test_mixed_boundaries_multigrid_matches_direct(kind):
     # |A| |x| far above |b|: its relative residual cannot fall much below
     # 1e-8 in FP64 (the restated algorithm stalls there too) while the
     # solution is then accurate to ~1e-14, so that case stops at 1e-8.
-    import math
     from test_mixed_boundaries import collisionless_flow_field, direct_solve, node_xy
     cases = []
     g = P.simple_grid((0.0, 0.0), (1.0, 1.67), (60, 40))
