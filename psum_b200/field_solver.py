@@ -11,11 +11,12 @@
   ``solve(phi, rho)`` sets the Dirichlet values with ``set_source_replace``
   and solves on device buffers, overwriting ``rho`` like PSuM does.
 * ``Dirichlet_line`` / ``Dirichlet_plane`` / ``Dirichlet_nodes`` /
-  ``Dirichlet_box`` / ``Dirichlet_func`` mirror the boundary creators of
-  src/field_solver/boundary_creator/Dirichlet.hpp; ``Neumann_line`` and
-  ``Robin_Line`` those of Neumann.hpp / Robin.hpp.  In 2-D, ``init`` also
-  takes mixed (Neumann / Robin) boundaries, the cylindrical (z, r) operator
-  and a position-dependent epsilon (``assemble_poisson_2d``).
+  ``Dirichlet_box`` / ``Dirichlet_box_rz`` / ``Dirichlet_func`` mirror the boundary creators of
+  src/field_solver/boundary_creator/Dirichlet.hpp; ``Neumann_line`` /
+  ``Robin_Line`` (2-D) and ``Neumann_plane`` / ``Robin_plane`` (3-D) those of
+  Neumann.hpp / Robin.hpp.  ``init`` also takes mixed (Neumann / Robin)
+  boundaries and a position-dependent epsilon (``assemble_poisson_2d``,
+  ``assemble_poisson_3d``), and in 2-D the cylindrical (z, r) operator.
 
 Device buffers are torch CUDA float64 tensors (or raw device addresses).
 Errors raise ``PsumError`` (a RuntimeError), as PSuM's frontends rethrow.
@@ -27,8 +28,9 @@ import numpy as np
 from ._lib import PsumError, check, lib
 
 __all__ = ["simple_grid", "solver_backend", "Poisson_solver_2d", "Poisson_solver_3d", "Dirichlet_line",
-           "Dirichlet_plane", "Dirichlet_nodes", "Dirichlet_box", "Dirichlet_func", "Neumann_line", "Robin_Line",
-           "MixedBoundary", "assemble_poisson", "assemble_poisson_2d", "registered_table"]
+           "Dirichlet_plane", "Dirichlet_nodes", "Dirichlet_box", "Dirichlet_box_rz", "Dirichlet_func",
+           "Neumann_line", "Robin_Line", "Neumann_plane", "Robin_plane", "MixedBoundary", "assemble_poisson",
+           "assemble_poisson_2d", "assemble_poisson_3d", "registered_table"]
 
 
 def _ptr(a):
@@ -95,9 +97,11 @@ def Dirichlet_line(grid, direction, value, min_max=None):
     return np.asarray(idx, np.uint64), np.full(len(idx), float(value))
 
 
-def Dirichlet_plane(grid, direction, value):
-    """Nodes of one boundary plane of a 3-D grid (Dirichlet.hpp:139-186):
-    Xneg/Xpos fix i = 0 / I, Yneg/Ypos j, Zneg/Zpos k."""
+def Dirichlet_plane(grid, direction, value, shape=None):
+    """Nodes of one boundary plane of a 3-D grid (Dirichlet.hpp:137-181):
+    Xneg/Xpos fix i = 0 / I, Yneg/Ypos j, Zneg/Zpos k; with shape(u, v) only
+    the nodes whose in-plane coordinates satisfy it ((y, z) on X planes,
+    (x, z) on Y planes, (x, y) on Z planes)."""
     I, J, K = grid.cells
     rng = {"X": range(I + 1), "Y": range(J + 1), "Z": range(K + 1)}
     axis, side = direction[0], direction[1:]
@@ -105,7 +109,17 @@ def Dirichlet_plane(grid, direction, value):
     ii = [fixed] if axis == "X" else rng["X"]
     jj = [fixed] if axis == "Y" else rng["Y"]
     kk = [fixed] if axis == "Z" else rng["Z"]
-    idx = [grid.n2i(i, j, k) for i in ii for j in jj for k in kk]
+    idx = []
+    for i in ii:
+        for j in jj:
+            for k in kk:
+                if shape is not None:
+                    x, y, z = (grid.lower[0] + i * grid.delta[0], grid.lower[1] + j * grid.delta[1],
+                               grid.lower[2] + k * grid.delta[2])
+                    uv = {"X": (y, z), "Y": (x, z), "Z": (x, y)}[axis]
+                    if not shape(*uv):
+                        continue
+                idx.append(grid.n2i(i, j, k))
     return np.asarray(idx, np.uint64), np.full(len(idx), float(value))
 
 
@@ -116,20 +130,46 @@ def Dirichlet_nodes(grid, nodes, value):
     return np.asarray(idx, np.uint64), np.full(len(idx), float(value))
 
 
-def Dirichlet_box(grid, x0, y0, x1, y1, value, geo_tolerance=1e-10):
+def Dirichlet_box(grid, *args, geo_tolerance=1e-10):
     """Nodes inside a box, with a tolerance of geo_tolerance times the
-    grid's size (Dirichlet.hpp:104-119)."""
-    x, y = _node_positions(grid)
-    tol = geo_tolerance * np.sqrt((grid.upper[0] - grid.lower[0]) * (grid.upper[1] - grid.lower[1]))
-    sel = (x >= x0 - tol) & (x <= x1 + tol) & (y >= y0 - tol) & (y <= y1 + tol)
-    idx = np.nonzero(sel.reshape(-1))[0].astype(np.uint64)
+    grid's size: Dirichlet_box(g2, x0, y0, x1, y1, value[, geo_tolerance])
+    (Dirichlet.hpp:104-119) or Dirichlet_box(g3, x0, y0, z0, x1, y1, z1,
+    value[, geo_tolerance]) (:184-201)."""
+    D = grid.dim
+    if len(args) not in (2 * D + 1, 2 * D + 2):
+        raise TypeError(f"Dirichlet_box on a {D}-D grid takes {2 * D} bounds and a value")
+    lo, hi, value = args[:D], args[D:2 * D], args[2 * D]
+    if len(args) == 2 * D + 2:
+        geo_tolerance = args[2 * D + 1]
+    coords = _node_coords(grid)
+    span = np.prod([grid.upper[a] - grid.lower[a] for a in range(D)])
+    tol = geo_tolerance * (np.sqrt(span) if D == 2 else np.cbrt(span))
+    sel = np.ones(grid.n_nodes, bool)
+    for a in range(D):
+        sel &= (coords[a] >= lo[a] - tol) & (coords[a] <= hi[a] + tol)
+    idx = np.nonzero(sel)[0].astype(np.uint64)
+    return idx, np.full(idx.size, float(value))
+
+
+def Dirichlet_box_rz(grid, z0, r0, z1, r1, value, geo_tolerance=1e-10):
+    """Nodes of a 3-D grid inside the annular cylinder z0 <= z <= z1,
+    r0 <= sqrt(x^2 + y^2) <= r1 (Dirichlet.hpp:204-223)."""
+    if grid.dim != 3:
+        raise ValueError("a 3-D grid is required")
+    x, y, z = _node_coords(grid)
+    span = np.prod([grid.upper[a] - grid.lower[a] for a in range(3)])
+    tol = geo_tolerance * span ** (1.0 / 3)
+    r = np.sqrt(x * x + y * y)
+    sel = (z >= z0 - tol) & (z <= z1 + tol) & (r >= r0 - tol) & (r <= r1 + tol)
+    idx = np.nonzero(sel)[0].astype(np.uint64)
     return idx, np.full(idx.size, float(value))
 
 
 def Dirichlet_func(grid, predicate, value):
-    """Nodes where predicate(x, y) holds (Dirichlet.hpp:121-135)."""
-    x, y = _node_positions(grid)
-    sel = np.array([bool(predicate(a, b)) for a, b in zip(x.reshape(-1), y.reshape(-1))])
+    """Nodes where predicate(x, y) (2-D, Dirichlet.hpp:121-135) or
+    predicate(x, y, z) (3-D, :226-240) holds."""
+    coords = _node_coords(grid)
+    sel = np.array([bool(predicate(*p)) for p in zip(*coords)], bool)
     idx = np.nonzero(sel)[0].astype(np.uint64)
     return idx, np.full(idx.size, float(value))
 
