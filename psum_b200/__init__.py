@@ -8,9 +8,10 @@ ctypes mirrors of the reference interfaces; there is no CPU fallback.
 """
 from ._lib import LIB_PATH, PROTOTYPES, PsumError, check, lib
 from .field_solver import (Dirichlet_box, Dirichlet_box_rz, Dirichlet_func, Dirichlet_line, Dirichlet_nodes,
-                           Dirichlet_plane, MixedBoundary, Neumann_line, Neumann_plane, Poisson_solver_2d,
-                           Poisson_solver_3d, Robin_Line, Robin_plane, assemble_poisson, assemble_poisson_2d,
-                           assemble_poisson_3d, registered_table, simple_grid, solver_backend)
+                           Dirichlet_plane, Dirichlet_point, Dirichlet_range, MixedBoundary, Neumann_line,
+                           Neumann_plane, Neumann_point, Poisson_solver_1d, Poisson_solver_2d, Poisson_solver_3d,
+                           Robin_Line, Robin_plane, Robin_point, assemble_poisson, assemble_poisson_1d,
+                           assemble_poisson_2d, assemble_poisson_3d, registered_table, simple_grid, solver_backend)
 from .interp import add_back_B_spline, interp_B_spline, interp_diff_B_spline
 from .pic import BORIS, FP64, LEAPFROG, MIXED, ParticleContext
 
@@ -19,4 +20,5 @@ __all__ = ["LIB_PATH", "PROTOTYPES", "PsumError", "check", "lib", "Dirichlet_lin
            "Neumann_plane", "Robin_plane", "MixedBoundary", "Poisson_solver_2d", "Poisson_solver_3d",
            "assemble_poisson", "assemble_poisson_2d", "assemble_poisson_3d", "registered_table", "simple_grid",
            "solver_backend", "ParticleContext", "MIXED", "FP64", "LEAPFROG", "BORIS", "interp_B_spline",
-           "interp_diff_B_spline", "add_back_B_spline"]
+           "interp_diff_B_spline", "add_back_B_spline", "Poisson_solver_1d", "Dirichlet_point", "Dirichlet_range",
+           "Neumann_point", "Robin_point", "assemble_poisson_1d"]

@@ -30,7 +30,8 @@ from ._lib import PsumError, check, lib
 __all__ = ["simple_grid", "solver_backend", "Poisson_solver_2d", "Poisson_solver_3d", "Dirichlet_line",
            "Dirichlet_plane", "Dirichlet_nodes", "Dirichlet_box", "Dirichlet_box_rz", "Dirichlet_func",
            "Neumann_line", "Robin_Line", "Neumann_plane", "Robin_plane", "MixedBoundary", "assemble_poisson",
-           "assemble_poisson_2d", "assemble_poisson_3d", "registered_table"]
+           "assemble_poisson_2d", "assemble_poisson_3d", "registered_table", "Poisson_solver_1d",
+           "Dirichlet_point", "Dirichlet_range", "Neumann_point", "Robin_point", "assemble_poisson_1d"]
 
 
 def _ptr(a):
@@ -189,8 +190,9 @@ def _node_coords(grid):
     return [c.reshape(-1) for c in np.meshgrid(*axes, indexing="ij")]
 
 
-# boundary directions: (axis, side) of boundary_direction_2d / boundary_direction_3d
-DIRECTIONS = {2: {"E": (0, 1), "W": (0, -1), "N": (1, 1), "S": (1, -1)},
+# boundary directions: (axis, side) of boundary_direction_{1,2,3}d
+DIRECTIONS = {1: {"R": (0, 1), "L": (0, -1)},
+              2: {"E": (0, 1), "W": (0, -1), "N": (1, 1), "S": (1, -1)},
               3: {"Xpos": (0, 1), "Xneg": (0, -1), "Ypos": (1, 1), "Yneg": (1, -1), "Zpos": (2, 1), "Zneg": (2, -1)}}
 
 
@@ -202,13 +204,13 @@ class MixedBoundary:
 
     where (a, b) = coeffs (a pair, or a function of the node coordinates
     giving one) and value is a number or a function of the node coordinates.
-    Directions are N, S, E, W in 2-D and Xneg, Xpos, Yneg, Ypos, Zneg, Zpos in
-    3-D.  ``set`` plays the role of PSuM's ``boundary = value``."""
+    Directions are L, R in 1-D, N, S, E, W in 2-D and Xneg, Xpos, Yneg, Ypos,
+    Zneg, Zpos in 3-D.  ``set`` plays the role of PSuM's ``boundary = value``."""
 
     def __init__(self, grid, nodes, direction, coeffs, value=None):
         names = DIRECTIONS.get(grid.dim, {})
         if direction not in names:
-            raise ValueError(f"direction must be one of {', '.join(names) or '(2-D or 3-D grids only)'}")
+            raise ValueError(f"direction must be one of {', '.join(names) or '(1-D, 2-D or 3-D grids only)'}")
         self.grid = grid
         self.nodes = np.asarray(nodes, np.int64)
         self.direction = direction
@@ -305,6 +307,41 @@ def Robin_plane(grid, direction, coef_value_and_grad, value=None, min_max=None):
     """a * phi + b * dphi/dn = value on a boundary plane (Robin.hpp:116-163);
     coef_value_and_grad is (a, b) or a function of (x, y, z) giving it."""
     return MixedBoundary(grid, _plane_nodes(grid, direction, min_max), direction, coef_value_and_grad, value)
+
+
+def _point_node(grid, direction):
+    if grid.dim != 1:
+        raise ValueError("a 1-D grid is required")
+    if direction not in DIRECTIONS[1]:
+        raise ValueError("direction must be L or R")
+    return 0 if direction == "L" else grid.cells[0]
+
+
+def Dirichlet_point(grid, direction, value):
+    """The end node of a 1-D grid (Dirichlet.hpp:24-41): L is node 0, R node I."""
+    return np.asarray([_point_node(grid, direction)], np.uint64), np.full(1, float(value))
+
+
+def Dirichlet_range(grid, x0, x1, value, geo_tolerance=1e-10):
+    """Nodes of a 1-D grid with x0 <= x <= x1 up to geo_tolerance times the
+    grid's span (Dirichlet.hpp:43-56)."""
+    if grid.dim != 1:
+        raise ValueError("a 1-D grid is required")
+    x = _node_coords(grid)[0]
+    tol = geo_tolerance * (grid.upper[0] - grid.lower[0])
+    idx = np.nonzero((x >= x0 - tol) & (x <= x1 + tol))[0].astype(np.uint64)
+    return idx, np.full(idx.size, float(value))
+
+
+def Neumann_point(grid, direction, value=None):
+    """dphi/dn = value at an end of a 1-D grid (Neumann.hpp:24-44)."""
+    return MixedBoundary(grid, [_point_node(grid, direction)], direction, (0.0, 1.0), value)
+
+
+def Robin_point(grid, direction, coef_value_and_grad, value=None):
+    """a * phi + b * dphi/dn = value at an end of a 1-D grid (Robin.hpp:24-54);
+    coef_value_and_grad is (a, b) or a function of x giving it."""
+    return MixedBoundary(grid, [_point_node(grid, direction)], direction, coef_value_and_grad, value)
 
 
 def _merge_mixed(mixed_boundaries, fixed_idx):
@@ -435,6 +472,81 @@ def assemble_poisson_2d(grid, domain, fixed_nodes, mixed_boundaries=(), epsilon=
     uniq, v = uniq[keep], v[keep]
     A = ((uniq // n).astype(np.uint64), (uniq % n).astype(np.uint64), v)
     M = (np.asarray(add_rows, np.int64), np.asarray(add_vals), entries)
+    return A, M
+
+
+def assemble_poisson_1d(grid, fixed_nodes, mixed_boundaries=(), epsilon=8.854e-12):
+    """Operator of Poisson_solver_1d::_init_impl (Poisson_solver_1d.hpp:126-222).
+    Free nodes: (grad_R eps_R - grad_L eps_L) * (-1 / dx) with epsilon (a
+    number or a function of x) at the mean of the two node positions and
+    cyclic neighbours.  A mixed node's row is its boundary condition itself,
+    a phi + b dphi/dn, with the gradient taken one-sided to second order at
+    the ends (-1.5, 2, -0.5 at node 0; 0.5, -2, 1.5 at node I) and centred
+    elsewhere, b negated for the L direction and the row divided by the
+    number of directions at the node.  The right-hand side of a mixed row is
+    the source plus the boundary value, as PSuM's add-back makes it.
+
+    Returns ((rows, cols, vals), (addback_rows, M_vals, mixed_entries)) like
+    assemble_poisson_2d, with M_vals all 1."""
+    if grid.dim != 1:
+        raise ValueError("a 1-D grid is required")
+    I = grid.cells[0]
+    n = I + 1
+    dx = grid.delta[0]
+    dxr = 1.0 / dx
+    fixed = np.zeros(n, bool)
+    fixed[np.asarray(fixed_nodes, np.int64)] = True
+    entries = _merge_mixed(list(mixed_boundaries), np.nonzero(fixed)[0])
+    by_node = {}
+    coef_cache = {}
+    for nd, dname, b, k in entries:
+        if b not in coef_cache:
+            coef_cache[b] = mixed_boundaries[b].coefficient_pairs()
+        by_node.setdefault(nd, []).append((dname, coef_cache[b][0][k], coef_cache[b][1][k]))
+    eps_f = (lambda v: float(epsilon(v))) if callable(epsilon) else (lambda v: float(epsilon))
+    pos = lambda i: grid.lower[0] + i * dx
+    trip = {}
+
+    def add(r, c, v):
+        trip[(r, c)] = trip.get((r, c), 0.0) + v
+
+    for i in range(n):
+        if fixed[i]:
+            add(i, i, 1.0)
+            continue
+        iR, iL = (i + 1) % n, (i - 1) % n
+        if i in by_node:
+            if i == I:
+                grad = [((i - 2) % n, dxr * 0.5), (iL, dxr * -2.0), (i, dxr * 1.5)]
+            elif i == 0:
+                grad = [(i, dxr * -1.5), (iR, dxr * 2.0), ((i + 2) % n, dxr * -0.5)]
+            else:
+                grad = [(iL, dxr * -0.5), (iR, dxr * 0.5)]
+            conds = sorted(by_node[i], key=lambda t: 0 if t[0] == "L" else 1)   # enum order: L, R
+            row = {}
+            for dname, a_val, b_grad in conds:
+                g = b_grad if dname == "R" else -b_grad
+                for c, v in grad:
+                    row[c] = row.get(c, 0.0) + v * g
+                row[i] = row.get(i, 0.0) + a_val
+            scale = 1.0 / len(conds)
+            for c, v in row.items():
+                add(i, c, v * scale)
+        else:
+            eps_R = eps_f((pos(i) + pos(i + 1)) / 2)
+            eps_L = eps_f((pos(i) + pos(i - 1)) / 2)
+            m = -1.0 / dx
+            # (grad_R S eps_R - grad_L S eps_L) * (-1 / V), S = 1, V = dx
+            add(i, i, (((dxr * -1) * 1.0) * eps_R - (dxr * 1.0) * eps_L) * m)
+            add(i, iR, ((dxr * 1.0) * eps_R) * m)
+            add(i, iL, (-((dxr * -1) * 1.0) * eps_L) * m)
+    keys = sorted(trip)
+    rows = np.asarray([k[0] for k in keys], np.uint64)
+    cols = np.asarray([k[1] for k in keys], np.uint64)
+    vals = np.asarray([trip[k] for k in keys])
+    keep = vals != 0.0
+    A = (rows[keep], cols[keep], vals[keep])
+    M = (np.asarray([e[0] for e in entries], np.int64), np.ones(len(entries)), entries)
     return A, M
 
 
@@ -739,6 +851,32 @@ class _PoissonFrontend:
         """Solve A phi = source on device buffers; `source` is overwritten."""
         self.make_righthand_item()
         return self.backend.solve(source, phi)
+
+
+class Poisson_solver_1d(_PoissonFrontend):
+    """Poisson_solver_1d (Poisson_solver_1d.hpp): init(backend_name, grid,
+    fixed_boundaries, epsilon, mixed_boundaries) with the operator of
+    assemble_poisson_1d; the backend options give I = cells + 1, J = K = 1."""
+    dim = 1
+
+    def init(self, backend_name, grid, fixed_boundaries, epsilon=8.854e-12, mixed_boundaries=()):
+        if grid.dim != 1:
+            raise ValueError("grid must be 1-D")
+        if backend_name == "native":
+            raise PsumError(1, "the 'native' Eigen direct solver is not part of this backend; "
+                               "use cuda_multigrid32f_gpu or cuda_multigrid64_gpu")
+        self.grid = grid
+        self.replace_idx, self.replace_val = _merge_fixed(fixed_boundaries)
+        (rows, cols, vals), self.mixed_M = assemble_poisson_1d(grid, self.replace_idx, list(mixed_boundaries),
+                                                               epsilon)
+        self.mixed = list(mixed_boundaries)
+        self.coo = (rows, cols, vals)
+        self.backend_name = backend_name
+        self.backend = solver_backend(backend_name)
+        if self.options:
+            self.backend.set_options(self.options)
+        n = grid.n_nodes
+        self.backend.set_matrix(n, n, rows.size, rows, cols, vals)
 
 
 class Poisson_solver_2d(_PoissonFrontend):
