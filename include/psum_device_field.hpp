@@ -30,7 +30,7 @@
 
 namespace psum_b200 {
 
-inline void cuda_check(cudaError_t e, const char* what) {
+inline void check_cuda(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw error(PSUM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
@@ -41,7 +41,7 @@ class device_array {
 public:
     device_array() = default;
     explicit device_array(std::size_t n) : n_(n) {
-        if (n_) cuda_check(cudaMalloc(reinterpret_cast<void**>(&p_), n_ * sizeof(T)), "cudaMalloc");
+        if (n_) check_cuda(cudaMalloc(reinterpret_cast<void**>(&p_), n_ * sizeof(T)), "cudaMalloc");
     }
     ~device_array() {
         if (p_) cudaFree(p_);
@@ -62,12 +62,12 @@ public:
     std::size_t size() const { return n_; }
     std::vector<T> to_host() const {
         std::vector<T> h(n_);
-        if (n_) cuda_check(cudaMemcpy(h.data(), p_, n_ * sizeof(T), cudaMemcpyDeviceToHost), "cudaMemcpy D2H");
+        if (n_) check_cuda(cudaMemcpy(h.data(), p_, n_ * sizeof(T), cudaMemcpyDeviceToHost), "cudaMemcpy D2H");
         return h;
     }
     void from_host(const std::vector<T>& h) {
         if (h.size() != n_) throw error(PSUM_ERR_INVALID_ARGUMENT, "device_array: size mismatch");
-        if (n_) cuda_check(cudaMemcpy(p_, h.data(), n_ * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy H2D");
+        if (n_) check_cuda(cudaMemcpy(p_, h.data(), n_ * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy H2D");
     }
 
 private:
@@ -82,13 +82,13 @@ class device_field {
 public:
     explicit device_field(const psum_pic_grid_desc& grid) : grid_(grid), data_(node_count(grid)) {
         if (grid.dim != D) throw error(PSUM_ERR_INVALID_ARGUMENT, "device_field: grid dimension mismatch");
-        if (data_.size()) cuda_check(cudaMemset(data_.data(), 0, data_.size() * sizeof(double)), "cudaMemset");
+        if (data_.size()) check_cuda(cudaMemset(data_.data(), 0, data_.size() * sizeof(double)), "cudaMemset");
     }
     const psum_pic_grid_desc& grid() const { return grid_; }
     std::size_t size() const { return data_.size(); }
     double* data() { return data_.data(); }
     const double* data() const { return data_.data(); }
-    void set_zero() { cuda_check(cudaMemset(data_.data(), 0, data_.size() * sizeof(double)), "cudaMemset"); }
+    void set_zero() { check_cuda(cudaMemset(data_.data(), 0, data_.size() * sizeof(double)), "cudaMemset"); }
     std::vector<double> to_host() const { return data_.to_host(); }
     void from_host(const std::vector<double>& h) { data_.from_host(h); }
 
@@ -119,7 +119,7 @@ device_array<double> interp_B_spline(const particle_group<D>& grp, const device_
     const std::size_t n = pos.size() / D;
     device_array<double> out(n);
     check(psum_interp_bspline(&f.grid(), Order, n, pos.data(), f.data(), out.data(), nullptr, nullptr));
-    cuda_check(cudaDeviceSynchronize(), "interp_B_spline");
+    check_cuda(cudaDeviceSynchronize(), "interp_B_spline");
     return out;
 }
 
@@ -131,7 +131,7 @@ device_array<double> interp_diff_B_spline(const particle_group<D>& grp, const de
     const std::size_t n = pos.size() / D;
     device_array<double> out((std::size_t)D * n);
     check(psum_interp_diff_bspline(&f.grid(), Order, n, pos.data(), f.data(), out.data(), nullptr, nullptr));
-    cuda_check(cudaDeviceSynchronize(), "interp_diff_B_spline");
+    check_cuda(cudaDeviceSynchronize(), "interp_diff_B_spline");
     return out;
 }
 
@@ -142,7 +142,7 @@ void add_back_B_spline(const particle_group<D>& grp, double w, device_field<D>& 
     device_array<double> pos = positions(grp);
     const std::size_t n = pos.size() / D;
     check(psum_add_back_bspline(&f.grid(), Order, n, pos.data(), w, f.data(), nullptr, nullptr, nullptr));
-    cuda_check(cudaDeviceSynchronize(), "add_back_B_spline");
+    check_cuda(cudaDeviceSynchronize(), "add_back_B_spline");
 }
 
 }  // namespace psum_b200

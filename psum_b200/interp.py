@@ -43,7 +43,14 @@ def _stream():
 
 
 def _skip_ptr(skipped):
-    return None if skipped is None else skipped.data_ptr()
+    """Device address of the optional 64-bit skip counter."""
+    if skipped is None:
+        return None
+    import torch
+    if not (isinstance(skipped, torch.Tensor) and skipped.is_cuda and skipped.dtype in (torch.int64, torch.uint64)
+            and skipped.numel() >= 1):
+        raise TypeError("skipped must be a 64-bit integer CUDA tensor with at least one element")
+    return skipped.data_ptr()
 
 
 def interp_B_spline(order, grid, pos, field, skipped=None):
