@@ -121,3 +121,37 @@ def test_pic_create_rejects_bad_grid_without_gpu():
     g.cells[0] = 0
     assert P.lib().psum_pic_create(C.byref(g), 0, C.byref(h)) == 1
     assert b"cells" in P.lib().psum_last_error()
+
+
+def test_bspline_argument_checks_without_gpu():
+    # include/psum_interp.h: arguments are checked before any CUDA call
+    L = P.lib()
+    g = P._lib.GridDesc()
+    g.dim = 2
+    for a in range(3):
+        g.cells[a], g.lower[a], g.upper[a] = (4, 0.0, 1.0)
+    ptr = 4096   # never dereferenced: every call below fails its checks first
+    assert L.psum_interp_bspline(C.byref(g), 5, 10, ptr, ptr, ptr, None, None) == 1       # order
+    assert L.psum_interp_diff_bspline(C.byref(g), 0, 10, ptr, ptr, ptr, None, None) == 1  # order
+    assert L.psum_interp_bspline(C.byref(g), 2, 0, None, None, None, None, None) == 0     # nothing to do
+    assert L.psum_interp_bspline(C.byref(g), 2, 10, None, ptr, ptr, None, None) == 1      # null positions
+    assert L.psum_add_back_bspline(C.byref(g), 3, 10, ptr, float("nan"), ptr, None, None, None) == 7
+    g.dim = 4
+    assert L.psum_interp_bspline(C.byref(g), 2, 10, ptr, ptr, ptr, None, None) == 1
+    g.dim = 2
+    g.cells[1] = 0
+    assert L.psum_add_back_bspline(C.byref(g), 2, 10, ptr, 1.0, ptr, None, None, None) == 1
+    g.cells[1] = 4
+    g.upper[0] = g.lower[0]
+    assert L.psum_interp_diff_bspline(C.byref(g), 2, 10, ptr, ptr, ptr, None, None) == 1
+    # fixed-point fraction bits of the deposit: min(40, 62 - ceil(log2(n + 1)))
+    from psum_b200 import interp
+    assert [interp.deposit_bits(n) for n in (0, 2 ** 22 - 1, 2 ** 22, 10 ** 9, 2 ** 40 - 1)] == [40, 40, 39, 32, 22]
+    # the Python mirror refuses host arrays
+    grid = P.simple_grid((0.0, 0.0), (1.0, 1.0), (4, 4))
+    torch = pytest.importorskip("torch")
+    with pytest.raises(TypeError):
+        P.interp_B_spline(2, grid, torch.zeros((2, 3), dtype=torch.float64), torch.zeros(25, dtype=torch.float64))
+    with pytest.raises(ValueError):
+        P.add_back_B_spline(7, grid, torch.zeros((2, 3), dtype=torch.float64), 1.0,
+                            torch.zeros(25, dtype=torch.float64))
