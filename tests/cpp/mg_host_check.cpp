@@ -8,7 +8,7 @@
 // usage: mg_host_check in.bin out.bin
 //   in.bin : int64 n, nnz, I, J, K, depth; uint64 rows[nnz]; uint64 cols[nnz]; double vals[nnz]
 //   out.bin: int64 levels; per level: int64 n, m; uint64 rows[m]; uint64 cols[m]; double vals[m];
-//            double dinv[n]
+//            double dinv[n]; then int64 c and the c x c dense coarse inverse (row-major)
 #include <cstdint>
 #include <cstdio>
 #include <exception>
@@ -83,6 +83,9 @@ int main(int argc, char** argv) {
         const std::vector<double>& d = h.dinv[&op - h.ahat.data()];
         std::fwrite(d.data(), 8, d.size(), out);
     }
+    const int64_t cn = (int64_t)h.coarse_inv.size();
+    std::fwrite(&cn, 8, 1, out);
+    std::fwrite(h.coarse_inv.data(), 8, h.coarse_inv.size(), out);
     std::fclose(out);
     return 0;
 }

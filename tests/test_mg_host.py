@@ -3,7 +3,8 @@ oracle's restatement of PSuM's multigrid_core::setup (multigrid_core.hpp:49-150)
 on operators the GPU tests do not cover: 1-D, 3-D with mixed boundary planes
 and a position-dependent epsilon, and 2-D mixed boundaries.  The product's
 source is compiled into tests/cpp/mg_host_check.cpp, which writes every
-level's scaled operator and inverse diagonal (CPU only)."""
+level's scaled operator and inverse diagonal and the dense coarse inverse
+(CPU only)."""
 import glob
 import os
 import shutil
@@ -58,11 +59,16 @@ def product_levels(program, tmp_path, coo, n, dims, depth):
         rr, cc, vv = take(np.uint64, m), take(np.uint64, m), take(np.float64, m)
         dinv = take(np.float64, nl)
         levels.append((sp.csr_matrix((vv, (rr.astype(np.int64), cc.astype(np.int64))), shape=(nl, nl)), dinv))
-    return levels
+    cn = int(take(np.int64, 1)[0])
+    coarse_inv = take(np.float64, cn).reshape(levels[-1][0].shape)
+    return levels, coarse_inv
 
 
 def compare(program, tmp_path, coo, n, dims, depth):
-    mine = product_levels(program, tmp_path, coo, n, dims, depth)
+    mine, coarse_inv = product_levels(program, tmp_path, coo, n, dims, depth)
+    # the dense inverse of the coarsest scaled operator (sycl_inner_solver.hpp:51-71)
+    Ac = mine[-1][0].toarray()
+    assert np.abs(coarse_inv @ Ac - np.eye(Ac.shape[0])).max() < 1e-9
     mg = O.Multigrid(coo[0], coo[1], coo[2], n, dims[0], dims[1], dims[2], depth)
     assert len(mine) == mg.levels
     for level, (A, dinv) in enumerate(mine):
