@@ -5,11 +5,13 @@
   obtained by name from the plugin registry, with the same seven operations.
 * ``Poisson_solver_2d`` / ``Poisson_solver_3d`` mirror the FD frontends
   (src/field_solver/Poisson_solver_2d.hpp:22-411, Poisson_solver_3d.hpp:21-...)
-  for Cartesian grids with uniform epsilon and Dirichlet boundaries: ``init``
-  assembles the operator (bit-identical values, psum_poisson_assemble),
-  creates the backend, replays the cached options and calls ``set_matrix``;
-  ``solve(phi, rho)`` sets the Dirichlet values with ``set_source_replace``
-  and solves on device buffers, overwriting ``rho`` like PSuM does.
+  (and Poisson_solver_1d.hpp): ``assemble`` builds the operator on the host
+  (bit-identical values through psum_poisson_assemble for the plain Cartesian
+  case), ``init`` assembles, creates the backend, replays the cached options
+  and calls ``set_matrix``; ``solve(phi, rho)`` hands the backend the mixed
+  add-back and the Dirichlet values and solves on device buffers,
+  overwriting ``rho`` like PSuM does; ``coeff_matrix()`` and
+  ``make_righthand_item(rho)`` give the discrete system on the host.
 * ``Dirichlet_line`` / ``Dirichlet_plane`` / ``Dirichlet_nodes`` /
   ``Dirichlet_box`` / ``Dirichlet_box_rz`` / ``Dirichlet_func`` mirror the boundary creators of
   src/field_solver/boundary_creator/Dirichlet.hpp; ``Neumann_line`` /
@@ -791,19 +793,18 @@ class _PoissonFrontend:
         if not self.backend.is_null():
             self.backend.set_options(options)
 
-    def init(self, backend_name, grid, domain, fixed_boundaries, epsilon=8.854e-12, mixed_boundaries=()):
-        """Poisson_solver_{2,3}d::init / _init_impl (Poisson_solver_2d.hpp:182-404,
-        Poisson_solver_3d.hpp:178-395): fixed (Dirichlet) boundaries, mixed
-        (Neumann / Robin) boundaries and an epsilon function of the node
-        coordinates; in 2-D also the cylindrical domain."""
+    def assemble(self, grid, domain, fixed_boundaries, epsilon=8.854e-12, mixed_boundaries=()):
+        """The host half of Poisson_solver_{2,3}d::_init_impl
+        (Poisson_solver_2d.hpp:182-368, Poisson_solver_3d.hpp:178-349): merge
+        the fixed boundaries and assemble the operator, with mixed (Neumann /
+        Robin) boundaries, an epsilon function of the node coordinates and, in
+        2-D, the cylindrical domain.  Needs no GPU; ``coeff_matrix`` and
+        ``make_righthand_item(rho)`` then give the discrete system."""
         if grid.dim != self.dim:
             raise ValueError(f"grid must be {self.dim}-D")
         general = bool(mixed_boundaries) or domain != self.Cartesian or callable(epsilon)
         if domain not in (self.Cartesian, self.Cylindrical) or (domain == self.Cylindrical and self.dim != 2):
             raise ValueError("the cylindrical domain is provided in 2-D; 3-D domains are Cartesian")
-        if backend_name == "native":
-            raise PsumError(1, "the 'native' Eigen direct solver is not part of this backend; "
-                               "use cuda_multigrid32f_gpu or cuda_multigrid64_gpu")
         self.grid = grid
         self.replace_idx, self.replace_val = _merge_fixed(fixed_boundaries)
         if general and self.dim == 2:
@@ -818,11 +819,24 @@ class _PoissonFrontend:
             rows, cols, vals = assemble_poisson(grid, self.replace_idx, epsilon)
             self.mixed, self.mixed_M = [], None
         self.coo = (rows, cols, vals)
+
+    def init(self, backend_name, grid, domain, fixed_boundaries, epsilon=8.854e-12, mixed_boundaries=()):
+        """Poisson_solver_{2,3}d::init / _init_impl (Poisson_solver_2d.hpp:182-404,
+        Poisson_solver_3d.hpp:178-395): ``assemble``, then create the backend,
+        replay the cached options and hand it the operator."""
+        if backend_name == "native":
+            raise PsumError(1, "the 'native' Eigen direct solver is not part of this backend; "
+                               "use cuda_multigrid32f_gpu or cuda_multigrid64_gpu")
+        self.assemble(grid, domain, fixed_boundaries, epsilon, mixed_boundaries)
+        self._attach(backend_name)
+
+    def _attach(self, backend_name):
+        rows, cols, vals = self.coo
         self.backend_name = backend_name
         self.backend = solver_backend(backend_name)
         if self.options:
             self.backend.set_options(self.options)
-        n = grid.n_nodes
+        n = self.grid.n_nodes
         self.backend.set_matrix(n, n, rows.size, rows, cols, vals)
 
     def coeff_matrix(self):
@@ -840,10 +854,18 @@ class _PoissonFrontend:
         uniq, inv = np.unique(rows, return_inverse=True)
         return uniq.astype(np.uint64), np.bincount(inv, weights=contrib, minlength=uniq.size)
 
-    def make_righthand_item(self):
-        """Poisson_solver_2d::make_righthand_item (:73-103): the mixed
-        boundaries' add-back, then the fixed values."""
+    def make_righthand_item(self, rho=None):
+        """Poisson_solver_2d::make_righthand_item (:73-131).  Without an
+        argument: hand the backend the mixed boundaries' add-back and the
+        fixed values, which it applies to the source at solve time.  With a
+        host array rho: return the right-hand side itself, rho plus the
+        add-back with the fixed values replaced (the (rho, b) overload)."""
         idx, val = self.addback()
+        if rho is not None:
+            b = np.array(rho, np.float64, copy=True)
+            np.add.at(b, idx.astype(np.int64), val)
+            b[self.replace_idx.astype(np.int64)] = self.replace_val
+            return b
         self.backend.set_source_addback(idx, val)
         self.backend.set_source_replace(self.replace_idx, self.replace_val)
 
@@ -859,24 +881,22 @@ class Poisson_solver_1d(_PoissonFrontend):
     assemble_poisson_1d; the backend options give I = cells + 1, J = K = 1."""
     dim = 1
 
-    def init(self, backend_name, grid, fixed_boundaries, epsilon=8.854e-12, mixed_boundaries=()):
+    def assemble(self, grid, fixed_boundaries, epsilon=8.854e-12, mixed_boundaries=()):
+        """The host half of Poisson_solver_1d::_init_impl: merge the fixed
+        boundaries and assemble the operator (no GPU needed)."""
         if grid.dim != 1:
             raise ValueError("grid must be 1-D")
+        self.grid = grid
+        self.replace_idx, self.replace_val = _merge_fixed(fixed_boundaries)
+        self.coo, self.mixed_M = assemble_poisson_1d(grid, self.replace_idx, list(mixed_boundaries), epsilon)
+        self.mixed = list(mixed_boundaries)
+
+    def init(self, backend_name, grid, fixed_boundaries, epsilon=8.854e-12, mixed_boundaries=()):
         if backend_name == "native":
             raise PsumError(1, "the 'native' Eigen direct solver is not part of this backend; "
                                "use cuda_multigrid32f_gpu or cuda_multigrid64_gpu")
-        self.grid = grid
-        self.replace_idx, self.replace_val = _merge_fixed(fixed_boundaries)
-        (rows, cols, vals), self.mixed_M = assemble_poisson_1d(grid, self.replace_idx, list(mixed_boundaries),
-                                                               epsilon)
-        self.mixed = list(mixed_boundaries)
-        self.coo = (rows, cols, vals)
-        self.backend_name = backend_name
-        self.backend = solver_backend(backend_name)
-        if self.options:
-            self.backend.set_options(self.options)
-        n = grid.n_nodes
-        self.backend.set_matrix(n, n, rows.size, rows, cols, vals)
+        self.assemble(grid, fixed_boundaries, epsilon, mixed_boundaries)
+        self._attach(backend_name)
 
 
 class Poisson_solver_2d(_PoissonFrontend):

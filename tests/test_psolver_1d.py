@@ -115,3 +115,44 @@ def test_creators_and_errors():
     # a fixed node covers a mixed condition on it
     _, (rows, _, entries) = P.assemble_poisson_1d(g, [0], [P.Neumann_point(g, "L", 1.0)], 1.0)
     assert len(entries) == 0 and len(rows) == 0
+
+
+def test_frontends_host_path_gives_the_same_system():
+    # assemble + coeff_matrix + make_righthand_item(rho) (the (rho, b)
+    # overload of PSuM's frontends) reproduce the systems built by hand
+    import scipy.sparse as sp
+    g1 = P.simple_grid((0.0,), (1.0,), (50,))
+    rho1 = np.linspace(-1.0, 1.0, 51)
+    fixed1, mixed1 = [P.Dirichlet_point(g1, "R", 1.0)], [P.Robin_point(g1, "L", (1.0, 2.0), 0.5)]
+    ps1 = P.Poisson_solver_1d()
+    ps1.assemble(g1, fixed1, 2.0, mixed1)
+    A_ref, b_ref, _ = system(g1, fixed1, mixed1, rho1, 2.0)
+    r, c, v = ps1.coeff_matrix()
+    A = sp.csr_matrix((v, (r.astype(np.int64), c.astype(np.int64))), shape=A_ref.shape)
+    assert abs(A - A_ref).max() == 0.0
+    assert (ps1.make_righthand_item(rho1) == b_ref).all()
+
+    g3 = P.simple_grid((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), (5, 4, 3))
+    rho3 = np.random.default_rng(8).normal(size=g3.n_nodes)
+    fixed3 = [P.Dirichlet_plane(g3, "Zneg", 0.5)]
+    mixed3 = [P.Neumann_plane(g3, "Zpos", 0.25), P.Robin_plane(g3, "Xneg", (1.0, 1.0), 0.1)]
+    ps3 = P.Poisson_solver_3d()
+    ps3.assemble(g3, "Cartesian", fixed3, 1.5, mixed3)
+    ridx, rval = P.field_solver._merge_fixed(fixed3)
+    (r3, c3, v3), M = P.assemble_poisson_3d(g3, ridx, mixed3, 1.5)
+    assert all((x == y).all() for x, y in zip(ps3.coeff_matrix(), (r3, c3, v3)))
+    ps_ref = P.Poisson_solver_3d()
+    ps_ref.mixed, ps_ref.mixed_M = mixed3, M
+    idx, val = ps_ref.addback()
+    b = rho3.copy()
+    b[idx.astype(np.int64)] += val
+    b[ridx.astype(np.int64)] = rval
+    assert (ps3.make_righthand_item(rho3) == b).all()
+    # the plain Cartesian case goes through the compiled assembly
+    ps2 = P.Poisson_solver_2d()
+    g2 = P.simple_grid((0.0, 0.0), (1.0, 1.0), (6, 6))
+    ps2.assemble(g2, "Cartesian", [P.Dirichlet_line(g2, "N", 0.0)], 3.0)
+    r2, c2, v2 = P.assemble_poisson(g2, P.Dirichlet_line(g2, "N", 0.0)[0], 3.0)
+    assert all((x == y).all() for x, y in zip(ps2.coeff_matrix(), (r2, c2, v2)))
+    with pytest.raises(ValueError):
+        ps3.assemble(g3, "Cylindrical", fixed3)
