@@ -155,3 +155,56 @@ def test_bspline_argument_checks_without_gpu():
     with pytest.raises(ValueError):
         P.add_back_B_spline(7, grid, torch.zeros((2, 3), dtype=torch.float64), 1.0,
                             torch.zeros(25, dtype=torch.float64))
+
+
+def test_frontend_init_and_solve_call_the_backend_in_psum_order(monkeypatch):
+    # Poisson_solver_{1,2,3}d: options cached and replayed before set_matrix
+    # (backend.hpp / field_solver_backend_en.md:125-135), then per solve the
+    # add-back, the replace values and the solve itself
+    from psum_b200 import field_solver as fs
+    calls = []
+
+    class FakeBackend:
+        def __init__(self, kind=None):
+            self.kind = kind
+            calls.append(("create", kind))
+
+        def is_null(self):          # a frontend starts with a null backend, as PSuM's does
+            return self.kind is None
+
+        def set_options(self, o):
+            calls.append(("set_options", o))
+
+        def set_matrix(self, n_row, n_col, nnz, rows, cols, vals):
+            calls.append(("set_matrix", n_row, nnz))
+
+        def set_source_addback(self, idx, val):
+            calls.append(("addback", len(idx)))
+
+        def set_source_replace(self, idx, val):
+            calls.append(("replace", len(idx)))
+
+        def solve(self, b, x):
+            calls.append(("solve",))
+            return 0
+
+    monkeypatch.setattr(fs, "solver_backend", FakeBackend)
+    for ps, args in ((P.Poisson_solver_1d(), lambda g: (g, [P.Dirichlet_point(g, "R", 0.0)], 1.0,
+                                                           [P.Neumann_point(g, "L", 0.0)])),
+                     (P.Poisson_solver_2d(), lambda g: (g, "Cartesian", [P.Dirichlet_line(g, "W", 0.0)], 1.0,
+                                                           [P.Neumann_line(g, "E", 1.0)])),
+                     (P.Poisson_solver_3d(), lambda g: (g, "Cartesian", [P.Dirichlet_plane(g, "Xneg", 0.0)], 1.0,
+                                                           [P.Neumann_plane(g, "Xpos", 1.0)]))):
+        g = P.simple_grid((0.0,) * ps.dim, (1.0,) * ps.dim, (4,) * ps.dim)
+        calls.clear()
+        ps.set_options("I 5 depth 2")
+        ps.init("cuda_multigrid64_gpu", *args(g))
+        assert calls[0] == ("create", "cuda_multigrid64_gpu")
+        assert calls[1] == ("set_options", "I 5 depth 2")
+        assert calls[2][0] == "set_matrix" and calls[2][1] == g.n_nodes and calls[2][2] == ps.coeff_matrix()[0].size
+        calls.clear()
+        assert ps.solve("phi", "rho") == 0
+        assert [c[0] for c in calls] == ["addback", "replace", "solve"]
+        assert calls[0][1] > 0 and calls[1][1] > 0
+        with pytest.raises(P.PsumError):
+            ps.init("native", *args(g))
