@@ -102,3 +102,11 @@ def test_2d_mixed_boundaries(program, tmp_path):
     coo, _ = P.assemble_poisson_2d(g, "Cartesian", P.Dirichlet_line(g, "W", 1.0)[0], mixed,
                                    lambda a, b: 1.0 + 0.5 * b)
     assert compare(program, tmp_path, coo, g.n_nodes, (65, 65, 1), 3) >= 3
+
+
+def test_hall_thruster_operator(program, tmp_path):
+    # the reference's 3-D Hall thruster set-up (Robin planes with coefficient
+    # functions, electrodes, ceramic epsilon) at depth 2 as its test uses
+    from test_psolver_3d import hall_thruster_system
+    ps, A, _ = hall_thruster_system(24, 24, 14)
+    assert compare(program, tmp_path, ps.coeff_matrix(), A.shape[0], (25, 25, 15), 2) == 3

@@ -123,3 +123,61 @@ def test_dirichlet_creators_3d():
     assert idx.tolist() == np.nonzero(sel)[0].tolist()
     with pytest.raises(TypeError):
         P.Dirichlet_box(g, 0.0, 0.0, 1.0, 1.0, 0.0)
+
+
+# ---- test_native_vs_multigrid_3d.cpp:14-159: the Hall thruster case ----
+HALL_Z, HALL_R = 0.080, 0.070
+HALL_BODY_LEN, HALL_UP_TH, HALL_DOWN_TH, HALL_CERAMIC, HALL_METAL = 0.025, 0.016, 0.031, 0.004, 0.003
+
+
+def hall_thruster_system(nx, ny, nz):
+    """The reference case's frontend set-up: Robin planes a = 1, b = |p|^2 / p_n
+    with value -10 on five sides, zero flux on z = 0, the anode annulus at
+    300 on z = 0, two grounded-at--10 electrodes (Dirichlet_box_rz), ceramic
+    rings at 4 eps0 and a charged annulus.  Returns (frontend, A, b)."""
+    g = P.simple_grid((-HALL_R, -HALL_R, 0.0), (HALL_R, HALL_R, HALL_Z), (nx, ny, nz))
+
+    def robin(normal):
+        return lambda x, y, z: (1.0, (x * x + y * y + z * z) / normal(x, y, z))
+
+    mixed = [P.Robin_plane(g, "Xpos", robin(lambda x, y, z: x), -10.0),
+             P.Robin_plane(g, "Xneg", robin(lambda x, y, z: -x), -10.0),
+             P.Robin_plane(g, "Ypos", robin(lambda x, y, z: y), -10.0),
+             P.Robin_plane(g, "Yneg", robin(lambda x, y, z: -y), -10.0),
+             P.Robin_plane(g, "Zpos", robin(lambda x, y, z: z), -10.0),
+             P.Neumann_plane(g, "Zneg", 0.0)]
+    fixed = [P.Dirichlet_plane(g, "Zneg", 300.0,
+                               shape=lambda x, y: HALL_DOWN_TH < math.hypot(x, y) < HALL_R - HALL_UP_TH),
+             P.Dirichlet_box_rz(g, HALL_BODY_LEN - HALL_METAL, 0.0, HALL_BODY_LEN, HALL_DOWN_TH, -10.0),
+             P.Dirichlet_box_rz(g, HALL_BODY_LEN - HALL_METAL, HALL_R - HALL_UP_TH, HALL_BODY_LEN, HALL_R, -10.0)]
+
+    def eps(x, y, z):
+        r = math.hypot(x, y)
+        ceramic = (0 < z < HALL_BODY_LEN and HALL_DOWN_TH < r < HALL_DOWN_TH + HALL_CERAMIC) or \
+                  (0 < z < HALL_BODY_LEN and HALL_R - HALL_UP_TH - HALL_CERAMIC < r < HALL_R - HALL_UP_TH)
+        return (4.0 if ceramic else 1.0) * EPS0
+
+    ps = P.Poisson_solver_3d()
+    ps.assemble(g, "Cartesian", fixed, eps, mixed)
+    x, y, z = node_xyz(g)
+    r = np.hypot(x, y)
+    q = np.where((z > 0.005) & (z < 0.02) & (r > 0.037) & (r < 0.048), 1e-5, 0.0)
+    rows, cols, vals = ps.coeff_matrix()
+    A = sp.csr_matrix((vals, (rows.astype(np.int64), cols.astype(np.int64))), shape=(g.n_nodes, g.n_nodes))
+    return ps, A, ps.make_righthand_item(q)
+
+
+def test_hall_thruster_multigrid_approaches_direct_solution():
+    # FP64 V(2,1) cycles at depth 2 (the reference's eigen_multigrid_cpu
+    # settings) against the direct solution: the relative L2 difference
+    # falls with the cycle count (1, 5, 15, 20 as the reference prints)
+    nx, ny, nz = 32, 32, 20
+    ps, A, b = hall_thruster_system(nx, ny, nz)
+    direct = spl.spsolve(A.tocsc(), b)
+    assert direct.max() == pytest.approx(300.0) and direct.min() >= -10.0 - 1e-6
+    rows, cols, vals = ps.coeff_matrix()
+    mg = O.Multigrid(rows, cols, vals, A.shape[0], nx + 1, ny + 1, nz + 1, 2)
+    errs = [np.linalg.norm(mg.vcycles(b, np.zeros(A.shape[0]), c, 2, 1) - direct) / np.linalg.norm(direct)
+            for c in (1, 5, 15, 20)]
+    assert all(e1 < e0 for e0, e1 in zip(errs, errs[1:])), errs
+    assert errs[-1] < 1e-7, errs        # 0.21, 1.5e-3, 4.7e-7, 1.1e-8
