@@ -110,3 +110,11 @@ def test_hall_thruster_operator(program, tmp_path):
     from test_psolver_3d import hall_thruster_system
     ps, A, _ = hall_thruster_system(24, 24, 14)
     assert compare(program, tmp_path, ps.coeff_matrix(), A.shape[0], (25, 25, 15), 2) == 3
+
+
+@pytest.mark.parametrize("name", ["fixed_zone", "robin_plates", "neumann_lid"])
+def test_native_vs_multigrid_2d_operators(program, tmp_path, name):
+    # the three set-ups of test_native_vs_multigrid_2d.cpp at depth 3
+    import test_multigrid_convergence_2d as T
+    g, ps, _, _ = getattr(T, name)()
+    assert compare(program, tmp_path, ps.coeff_matrix(), g.n_nodes, (g.cells[0] + 1, g.cells[1] + 1, 1), 3) == 4
