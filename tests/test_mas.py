@@ -101,3 +101,46 @@ def test_grid_and_node_field(tmp_path):
     assert (got.view(np.int64) == phi.view(np.int64)).all()
     with pytest.raises(ValueError):
         mas.load_node_field(fp2, "phi", P.simple_grid((0.0, -1.0), (4.0, 1.0), (8, 5)))
+
+
+def test_random_block_sequences_round_trip(tmp_path):
+    # hypothesis: random sequences of blocks of every element type and shape
+    # (empty ones included), written, reopened, partly masked with smash and
+    # read back (mas.hpp:130-330)
+    from hypothesis import HealthCheck, given, settings, strategies as st
+    import hypothesis.extra.numpy as hnp
+
+    dtypes = [np.float64, np.float32, np.int64, np.uint64, np.int32, np.uint32, np.int16, np.uint16, np.int8,
+              np.uint8, np.bool_]
+    block = st.tuples(st.sampled_from(dtypes), hnp.array_shapes(min_dims=1, max_dims=3, min_side=0, max_side=5))
+    counter = iter(range(10 ** 9))
+
+    @settings(max_examples=40, deadline=None, derandomize=True,
+              suppress_health_check=[HealthCheck.function_scoped_fixture])
+    @given(st.lists(block, min_size=1, max_size=8), st.data())
+    def check(blocks, data):
+        path = tmp_path / f"r{next(counter)}.mas"
+        fp = mas.MasFile(path, "replace")
+        written = {}
+        for i, (dt, shape) in enumerate(blocks):
+            arr = data.draw(hnp.arrays(dt, shape, elements=hnp.from_dtype(np.dtype(dt), allow_nan=False)))
+            key = f"b{i}.{np.dtype(dt).name}"
+            fp.write(key, arr, shape)
+            written[key] = arr
+        with pytest.raises(mas.MasDuplicateBlockError):
+            fp.write(next(iter(written)), np.zeros(1))
+        masked = {k for k in written if data.draw(st.booleans())}
+        again = mas.MasFile(path)
+        for k in masked:
+            assert again.smash(k)
+        reread = mas.MasFile(path)
+        assert reread.keys() == [k for k in written if k not in masked]
+        for k, arr in written.items():
+            h, got = reread.read(k)
+            if k in masked:
+                assert h is None
+                continue
+            assert h.shape == tuple(arr.shape) and got.dtype == arr.dtype
+            assert (got == arr).all()
+
+    check()
