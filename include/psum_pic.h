@@ -219,9 +219,14 @@ EXPORT int psum_pic_adjoint_deposit(psum_pic_ctx* ctx, int species, const double
  * file-scope device array (about 12.6 MB) that every GPU loading this
  * library keeps until the process exits; limits: n <= 262,144 particles and
  * at most 1,048,576 grid cells (larger sizes return
- * PSUM_ERR_INVALID_ARGUMENT).  The first call on a device looks the array's
- * address up (cudaGetSymbolAddress); make that first call before any stream
- * capture.  All calls share the one array, so calls that overlap on the GPU
+ * PSUM_ERR_INVALID_ARGUMENT).  The array belongs to the library's device
+ * module: under CUDA's lazy module loading the driver reserves it when that
+ * module is first used on a device, which is this call's first run there
+ * unless another call of this library came first.  A caller with a fixed
+ * device-memory budget should make one warm-up call (any size, e.g. n = 0)
+ * outside the budgeted region.  The first call on a device also looks the
+ * array's address up (cudaGetSymbolAddress); make that first call before any
+ * stream capture.  All calls share the one array, so calls that overlap on the GPU
  * (other host threads, other streams) race; serialise them.  Work runs on
  * `stream` (a cudaStream_t, NULL = legacy default stream) and the call
  * returns after it has finished. */

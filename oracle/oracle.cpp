@@ -952,7 +952,9 @@ long long oracle_bin(const og_grid* gd, long long n, const double* pos, long lon
             continue;
         }
         int c[3];
-        for (int a = 0; a < g.dim; ++a) c[a] = int((p[a] - g.lo[a]) * g.dr[a]);   // nC, :99-104
+        // nC (simple_grid.hpp:99-104), clamped to the last cell: a position just below hi can
+        // truncate to `cells` when dr = 1/dx rounds up; the reference indexes past its counts there
+        for (int a = 0; a < g.dim; ++a) c[a] = std::min(int((p[a] - g.lo[a]) * g.dr[a]), g.cells[a] - 1);
         keys[i] = g.c2i(c);
         counts[keys[i]]++;
     }

@@ -1429,7 +1429,9 @@ __global__ void k_bin_keys64(GridView g, const double* __restrict__ x, const dou
     for (int a = 0; a < g.dim && in; ++a) in = p[a] >= g.lo[a] && p[a] < hi[a];   // inGrid, simple_grid.hpp:168-174
     if (in) {
         int c[3] = {0, 0, 0};
-        for (int a = 0; a < g.dim; ++a) c[a] = (int)((p[a] - g.lo[a]) * g.dr[a]);   // nC: truncation, :99-104
+        // nC: truncation (simple_grid.hpp:99-104), clamped to the last cell: with dr = 1/dx rounded up, a
+        // position just below hi can truncate to `cells`, which has no cell (undefined in the reference)
+        for (int a = 0; a < g.dim; ++a) c[a] = min((int)((p[a] - g.lo[a]) * g.dr[a]), g.cells[a] - 1);
         ref = ((long long)c[0] * g.cells[1] + c[1]) * g.cells[2] + c[2];
     }
     keys_out[i] = ref;
@@ -2778,7 +2780,8 @@ __global__ void k_noalloc_keys(BinKeyArgs a, long long* __restrict__ keys_out, u
     long long ref = -1;
     if (in) {
         int c[3] = {0, 0, 0};
-        for (int d = 0; d < a.g.dim; ++d) c[d] = (int)((p[d] - a.g.lo[d]) * a.g.dr[d]);
+        // nC clamped to the last cell, as in k_bin_keys64
+        for (int d = 0; d < a.g.dim; ++d) c[d] = min((int)((p[d] - a.g.lo[d]) * a.g.dr[d]), a.g.cells[d] - 1);
         ref = ((long long)c[0] * a.g.cells[1] + c[1]) * a.g.cells[2] + c[2];
     }
     keys_out[i] = ref;
@@ -2798,7 +2801,7 @@ extern "C" EXPORT int psum_bin_positions_noalloc(const psum_pic_grid_desc* grid,
         if (!grid || !n_in_grid || !counts_dev || !offsets_dev) throw std::invalid_argument("bin_noalloc: null argument");
         if (n > 0 && (!pos_dev || !keys_dev || !perm_dev)) throw std::invalid_argument("bin_noalloc: null device array");
         if (grid->dim != 2 && grid->dim != 3) throw std::invalid_argument("bin_noalloc: dim must be 2 or 3");
-        if ((long long)n > kNoAllocMaxParticles)
+        if (n > (unsigned long long)kNoAllocMaxParticles)
             throw std::invalid_argument("bin_noalloc: n = " + std::to_string(n) + " exceeds the fixed scratch limit of " +
                                         std::to_string(kNoAllocMaxParticles) + " particles");
         BinKeyArgs a{};
@@ -2807,6 +2810,10 @@ extern "C" EXPORT int psum_bin_positions_noalloc(const psum_pic_grid_desc* grid,
             if (d < grid->dim) {
                 if (grid->cells[d] < 1 || !(grid->lower[d] < grid->upper[d]))
                     throw std::invalid_argument("bin_noalloc: bad grid");
+                // each factor is checked before the product, so the product cannot overflow
+                if (grid->cells[d] > kNoAllocMaxCells || ncell * grid->cells[d] > kNoAllocMaxCells)
+                    throw std::invalid_argument("bin_noalloc: the grid's cells exceed the fixed scratch limit of " +
+                                                std::to_string(kNoAllocMaxCells) + " cells");
                 a.g.cells[d] = grid->cells[d];
                 a.g.lo[d] = grid->lower[d];
                 a.g.dx[d] = (grid->upper[d] - grid->lower[d]) / grid->cells[d];   // simple_grid.hpp:47

@@ -166,6 +166,32 @@ def test_deposit_matches_oracle(precision, kind):
     assert abs(diag["charge"] - n_valid * w) < 1e-6 * n_valid * w
 
 
+@pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
+@pytest.mark.parametrize("kind", ["2d_absorb", "2d_periodic", "3d_periodic"])
+def test_energy_diagnostics_match_oracle(precision, kind):
+    """Kinetic energy per species and field energy (TSI/main.cpp:132-146) against the oracle's FP64 sums of the
+    same state.  Both are FP64 reductions of the same terms in another order: relative tolerance 1e-12.  In mixed
+    mode the oracle sums the exported state (FP32 velocities widened to FP64), so the comparison is exact up to
+    summation order as well."""
+    ctx, g, pos, vel, phi = make_case(kind, precision, seed=16, n=60000)
+    pos = wrap_into(pos, g)
+    pos[0, ::97] = np.nan   # invalid particles carry no kinetic energy
+    species = [(-1.0, 1.0, 0.37), (1.0, 1836.0, 0.37)]
+    ids = []
+    for q, m, w in species:
+        sid = ctx.add_species(q, m, w, pos.shape[1])
+        ctx.load(sid, pos, vel * (1.0 if m == 1.0 else 1.0 / np.sqrt(m)))
+        ids.append(sid)
+    eps = 0.7
+    diag = ctx.diagnostics(dev(phi), eps)
+    for sid, (q, m, w) in zip(ids, species):
+        p0, v0 = ctx.get_state(sid)
+        exp = O.kinetic_energy(p0, v0, m * w)
+        assert abs(diag["kinetic"][sid] - exp) <= 1e-12 * abs(exp)
+    exp_field = O.field_energy(g, phi, eps)
+    assert abs(diag["field"] - exp_field) <= 1e-12 * abs(exp_field)
+
+
 def test_golden_known_answers_fp64():
     ctx = P.ParticleContext((16, 16), (0, 0), (16, 16), (0, 0), P.FP64)
     qm, dt = GOLD["push_qm_dt"]

@@ -124,6 +124,24 @@ def test_binning_golden():
     assert (perm == GOLD["bin_perm"]).all()
 
 
+def test_binning_clamps_truncation_to_the_last_cell():
+    """inGrid admits p = nextafter(hi, lo), but (p - lo) * dr can truncate to `cells` when dr = 1/dx rounds
+    up; the oracle bins such a position into the last cell (the reference's nC would index past the counts)."""
+    cells, lo, hi = (199, 7), (0.0, 0.0), (3.3, 7.0)
+    dr = 1.0 / ((hi[0] - lo[0]) / cells[0])
+    edge = np.nextafter(hi[0], lo[0])
+    assert int((edge - lo[0]) * dr) == cells[0]                    # the case is reached on this grid
+    # how common the case is: (cells, hi) pairs on [0, hi) where the position below hi truncates to cells
+    hits = sum(int(np.nextafter(h, 0.0) * (1.0 / (h / c))) == c for c in range(1, 200) for h in (1.1, 3.3, 0.7))
+    assert hits > 0
+    pos = np.array([[edge, edge, 1.0, edge], [0.5, 6.999999999999999, 3.2, np.nextafter(7.0, 0.0)]])
+    keys, counts, offsets, perm = O.bin_particles(O.make_grid(cells, lo, hi, (0, 0)), pos)
+    last_row = (cells[0] - 1) * cells[1]
+    assert list(keys) == [last_row + 0, last_row + 6, int(1.0 * dr) * 7 + 3, last_row + 6]
+    assert counts.sum() == 4 and counts.size == cells[0] * cells[1]
+    assert list(perm) == [2, 0, 1, 3]
+
+
 # ------------------------------------------------------------- multigrid ---
 def dirichlet_box_2d(N, eps=1.0, lo=0.0, hi=1.0):
     fixed = [i * (N + 1) + j for i in range(N + 1) for j in range(N + 1) if i in (0, N) or j in (0, N)]

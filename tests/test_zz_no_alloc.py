@@ -86,7 +86,56 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     code = P.lib().psum_bin_positions_noalloc(C.byref(g), big.shape[1], big.data_ptr(), out.data_ptr(),
                                               out.data_ptr(), out.data_ptr(), out.data_ptr(), C.byref(m), None)
     assert code == 1 and b"exceeds" in P.lib().psum_last_error()
+    # a count of 2^63 or more must not pass the limit as a negative signed value
+    code = P.lib().psum_bin_positions_noalloc(C.byref(g), (1 << 63) + 5, big.data_ptr(), out.data_ptr(),
+                                              out.data_ptr(), out.data_ptr(), out.data_ptr(), C.byref(m), None)
+    assert code == 1 and b"exceeds" in P.lib().psum_last_error()
     g.cells[0] = g.cells[1] = 2048          # 4,194,304 cells > the 1,048,576-cell limit
     code = P.lib().psum_bin_positions_noalloc(C.byref(g), 10, big.data_ptr(), out.data_ptr(), out.data_ptr(),
                                               out.data_ptr(), out.data_ptr(), C.byref(m), None)
     assert code == 1 and b"exceed" in P.lib().psum_last_error()
+    # factors whose product overflows 64 bits are refused factor by factor
+    g.dim = 3
+    g.cells[0] = g.cells[1] = g.cells[2] = (1 << 31) - 1
+    code = P.lib().psum_bin_positions_noalloc(C.byref(g), 10, big.data_ptr(), out.data_ptr(), out.data_ptr(),
+                                              out.data_ptr(), out.data_ptr(), C.byref(m), None)
+    assert code == 1 and b"exceed" in P.lib().psum_last_error()
+
+
+def test_noalloc_allocates_no_device_memory():
+    """After a warm-up call, further calls leave the device's free memory unchanged."""
+    cells, lo, hi = (300, 200), (0.0, -1.0), (3.0, 1.0)
+    rng = np.random.default_rng(5)
+    pos = torch.tensor(np.stack([rng.uniform(l, h, 100000) for l, h in zip(lo, hi)]), device="cuda")
+    first = noalloc_bin(cells, lo, hi, pos)           # warm-up: module load and symbol look-up
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    reserved0 = torch.cuda.memory_reserved()
+    again = noalloc_bin(cells, lo, hi, pos)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    # the outputs of noalloc_bin are allocated by the test before the call; they come from torch's cache, so
+    # the free memory the driver reports does not change unless the library allocates
+    assert torch.cuda.memory_reserved() == reserved0
+    assert free1 == free0
+    for a, b in zip(first, again):
+        assert np.array_equal(np.asarray(a), np.asarray(b))
+
+
+def test_noalloc_clamps_positions_just_below_the_upper_bound():
+    """A position one ulp below `upper` whose (p - lo) * dr truncates to `cells` bins into the last cell."""
+    from oracle import oracle as O
+    cells, lo, hi = (199, 300), (0.0, 0.0), (3.3, 3.0)
+    n = 1000
+    rng = np.random.default_rng(9)
+    pos = np.stack([rng.uniform(lo[a], hi[a], n) for a in range(2)])
+    edge = [np.nextafter(hi[a], lo[a]) for a in range(2)]
+    pos[0, ::7] = edge[0]
+    pos[1, ::5] = edge[1]
+    dr = [1.0 / ((hi[a] - lo[a]) / cells[a]) for a in range(2)]
+    assert any(int((edge[a] - lo[a]) * dr[a]) == cells[a] for a in range(2))   # the case is reached
+    got = noalloc_bin(cells, lo, hi, torch.tensor(pos, device="cuda"))
+    ek, ec, eo, ep = O.bin_particles(O.make_grid(cells, lo, hi, (0, 0)), pos)
+    assert got[0].max() < cells[0] * cells[1]
+    assert np.array_equal(got[0], ek) and np.array_equal(got[1], ec.astype(np.int64))
+    assert np.array_equal(got[2], eo.astype(np.int64)) and np.array_equal(got[3], ep.astype(np.int64))
