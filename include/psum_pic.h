@@ -172,12 +172,29 @@ EXPORT int psum_pic_join(psum_pic_ctx* ctx);
  * last reset (synchronises the stream). */
 EXPORT int psum_pic_set_timing(psum_pic_ctx* ctx, int enable);
 EXPORT int psum_pic_get_timing(psum_pic_ctx* ctx, double* ms_host, int* count_host, int reset);
+/* The same for the first n_phases phases, including phase 4, the reduction of
+ * the per-step diagnostics (option "diagnostics 1").  No counterpart in the
+ * reference. */
+EXPORT int psum_pic_get_phase_times(psum_pic_ctx* ctx, double* ms_host, int* count_host, int n_phases, int reset);
 
 /* FP64 diagnostics (fixed-order reductions): out_host[s] = kinetic energy of
  * species s (sum 0.5*m*w*|v|^2); out_host[ns] = field energy
  * 0.5*eps*sum over edges (dphi/dx)^2 * cell_volume; out_host[ns+1] = total
  * deposited charge sum_s q_s w_s N_s (exact from the integer accumulators). */
 EXPORT int psum_pic_diagnostics(psum_pic_ctx* ctx, const double* phi_dev, double epsilon, double* out_host);
+
+/* The diagnostics of TSI's step loop (application/benchmark/TSI/main.cpp:132-146)
+ * computed inside every psum_pic_step when the context has option
+ * "diagnostics 1": the push sums the kinetic energy of the pushed particles
+ * (FP64, before absorbed ones leave), the edge kernel sums the field energy of
+ * the step's phi, and the charge density sums the particle charge it holds
+ * (the deposit of the previous step); fixed-order reductions, no extra pass
+ * over the particles.  Returns the last step's values in the layout of
+ * psum_pic_diagnostics: out_host[s] kinetic energy of species s, out_host[ns]
+ * field energy (times epsilon), out_host[ns+1] particle charge.  Errors with
+ * PSUM_ERR_INVALID_ARGUMENT before such a step.  No counterpart in the
+ * reference (its diagnostics are host loops over copies). */
+EXPORT int psum_pic_get_step_diagnostics(psum_pic_ctx* ctx, double epsilon, double* out_host);
 
 /* Error word of the device-side checks since the last call (bit set per
  * psum_status code: non-finite state, overflow, key out of range); resets it. */

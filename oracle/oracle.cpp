@@ -1145,6 +1145,34 @@ int oracle_mg_solve_mixed(void* h, const double* b, double* x, int max_cycles, i
     return batches;
 }
 
+// The same refinement loop with the GPU backends' stopping rule: stop after
+// the first batch whose squared relative residual is at most tol^2 (tol 0:
+// run max_cycles).  Returns the batches run; hist[k] = squared relative
+// residual after batch k.
+int oracle_mg_solve_mixed_tol(void* h, const double* b, double* x, int max_cycles, int correction_interval, int pre,
+                              int post, double tol, double* hist) {
+    MG* mg = static_cast<MG*>(h);
+    const long long n = mg->A.n_row;
+    std::vector<double> bv(b, b + n), xv(x, x + n);
+    const double bn = norm2(bv);
+    int batches = 0;
+    for (int cycle = 0; cycle < max_cycles;) {
+        const int batch = std::min(correction_interval, max_cycles - cycle);
+        std::vector<double> r = residual(mg->A, bv, xv);
+        std::vector<float> r32(n), e32(n, 0.0f);
+        for (long long i = 0; i < n; ++i) r32[i] = (float)r[i];
+        mg_vcycles<float>(*mg, r32, e32, batch, pre, post);
+        for (long long i = 0; i < n; ++i) xv[i] += (double)e32[i];
+        const double rel2 = norm2(residual(mg->A, bv, xv)) / (bn > 0 ? bn : 1.0);
+        if (hist) hist[batches] = rel2;
+        ++batches;
+        cycle += batch;
+        if (tol > 0 && rel2 <= tol * tol) break;
+    }
+    std::copy(xv.begin(), xv.end(), x);
+    return batches;
+}
+
 double oracle_rel_residual(void* h, const double* b, const double* x) {
     MG* mg = static_cast<MG*>(h);
     const long long n = mg->A.n_row;

@@ -62,6 +62,7 @@ def lib():
         L.oracle_mg_level_coo.argtypes = [P, i, P, P, P, P]; L.oracle_mg_level_coo.restype = ll
         L.oracle_mg_vcycles.argtypes = [P, P, P, i, i, i]; L.oracle_mg_vcycles.restype = None
         L.oracle_mg_solve_mixed.argtypes = [P, P, P, i, i, i, i, P]; L.oracle_mg_solve_mixed.restype = i
+        L.oracle_mg_solve_mixed_tol.argtypes = [P, P, P, i, i, i, i, d, P]; L.oracle_mg_solve_mixed_tol.restype = i
         L.oracle_rel_residual.argtypes = [P, P, P]; L.oracle_rel_residual.restype = d
         L.oracle_kinetic_energy.argtypes = [ll, P, P, d]; L.oracle_kinetic_energy.restype = d
         L.oracle_field_energy.argtypes = [P, P, d]; L.oracle_field_energy.restype = d
@@ -216,6 +217,14 @@ class Multigrid:
         hist = np.zeros(max(max_cycles, 1))
         nb = lib().oracle_mg_solve_mixed(self.h, _p(_f64(b)), _p(x), max_cycles, correction_interval, pre, post,
                                          _p(hist))
+        return x, hist[:nb]
+
+    def solve_mixed_tol(self, b, x0, max_cycles, correction_interval, pre, post, tol):
+        """solve_mixed stopping after the first batch with relative residual <= tol (the GPU backends' rule)."""
+        x = _f64(x0).copy()
+        hist = np.zeros(max(max_cycles, 1))
+        nb = lib().oracle_mg_solve_mixed_tol(self.h, _p(_f64(b)), _p(x), max_cycles, correction_interval, pre, post,
+                                             tol, _p(hist))
         return x, hist[:nb]
 
     def rel_residual(self, b, x):

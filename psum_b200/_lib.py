@@ -84,7 +84,9 @@ PROTOTYPES = {
     "psum_pic_step": (I, [P, P, D, P, P, D, I, P]),
     "psum_pic_set_timing": (I, [P, I]),
     "psum_pic_get_timing": (I, [P, P, P, I]),
+    "psum_pic_get_phase_times": (I, [P, P, P, I, I]),
     "psum_pic_diagnostics": (I, [P, P, D, P]),
+    "psum_pic_get_step_diagnostics": (I, [P, D, P]),
     "psum_pic_device_errors": (I, [P, C.POINTER(C.c_uint)]),
     "psum_pic_state_bytes": (I, [P, I, C.POINTER(ULL)]),
     "psum_pic_save_state": (I, [P, I, P]),

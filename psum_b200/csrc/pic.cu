@@ -46,29 +46,41 @@ inline unsigned capped_blocks(long long n_items_per_block_unit, long long n) {
 // (S = 2 in 2-D, 4 in 3-D).  The CIC gradient of PSuM's interp_diff
 // (simple_interpolation.hpp:58-98) is a bilinear/trilinear blend of exactly
 // these differences, so the FP32 gather loses no precision to cancellation.
+// With fe_part set, each block also writes the sum over its nodes of
+// sum_a ((phi(n + e_a) - phi(n)) * dr_a)^2 in FP64 (the field-energy terms of
+// TSI/main.cpp:141-143, periodic edges included) to fe_part[blockIdx.x].
 template <int D>
-__global__ void k_edges(GridView g, const double* __restrict__ phi, float* __restrict__ edges) {
+__global__ void k_edges(GridView g, const double* __restrict__ phi, float* __restrict__ edges,
+                        double* __restrict__ fe_part) {
     const long long node = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (node >= g.n_nodes) return;
-    const int n12 = g.N[1] * g.N[2];
-    const int i = (int)(node / n12);
-    const int rem = (int)(node - (long long)i * n12);
-    const int j = rem / g.N[2];
-    const int k = rem - j * g.N[2];
-    const double p0 = phi[node];
-    float e[4] = {0.f, 0.f, 0.f, 0.f};
-    const int idx[3] = {i, j, k};
-    for (int a = 0; a < D; ++a) {
-        int q[3] = {idx[0], idx[1], idx[2]};
-        q[a] += 1;
-        if (q[a] >= g.N[a]) {
-            if (!g.periodic[a]) continue;
-            q[a] = 0;
+    double fe = 0.0;
+    if (node < g.n_nodes) {
+        const int n12 = g.N[1] * g.N[2];
+        const int i = (int)(node / n12);
+        const int rem = (int)(node - (long long)i * n12);
+        const int j = rem / g.N[2];
+        const int k = rem - j * g.N[2];
+        const double p0 = phi[node];
+        float e[4] = {0.f, 0.f, 0.f, 0.f};
+        const int idx[3] = {i, j, k};
+        for (int a = 0; a < D; ++a) {
+            int q[3] = {idx[0], idx[1], idx[2]};
+            q[a] += 1;
+            if (q[a] >= g.N[a]) {
+                if (!g.periodic[a]) continue;
+                q[a] = 0;
+            }
+            const double dphi = phi[node_index(g, q[0], q[1], q[2])] - p0;
+            e[a] = (float)dphi;
+            const double gr = dphi * g.dr[a];
+            fe += gr * gr;
         }
-        e[a] = (float)(phi[node_index(g, q[0], q[1], q[2])] - p0);
+        if (edges) {
+            if (D == 2) reinterpret_cast<float2*>(edges)[node] = make_float2(e[0], e[1]);
+            else reinterpret_cast<float4*>(edges)[node] = make_float4(e[0], e[1], e[2], 0.f);
+        }
     }
-    if (D == 2) reinterpret_cast<float2*>(edges)[node] = make_float2(e[0], e[1]);
-    else reinterpret_cast<float4*>(edges)[node] = make_float4(e[0], e[1], e[2], 0.f);
+    if (fe_part) block_sum_to(fe, fe_part);
 }
 
 // ------------------------------------------------------------ mixed push --
@@ -88,6 +100,8 @@ struct PushArgs {
     int dep_lsh;        // accumulator units per 2^-26 weight unit: 2^dep_lsh
     unsigned long long* losses;
     unsigned* err;
+    double* kin_part;   // per-block kinetic energy of the pushed particles (null: not summed)
+    double kin_hmw;     // m * w / 2
 };
 
 // Field data of one cell for the CIC gather of the edge differences: the
@@ -238,6 +252,12 @@ __device__ __forceinline__ int push_one(const PushArgs& a, int c[3], float f[3],
     return apply_step<D>(a.g, c, dc);
 }
 
+// |v|^2 of FP32 velocities, summed in FP64 (the terms of TSI/main.cpp:133-136)
+__device__ __forceinline__ double kinetic_v2(const float v[3]) {
+    const double x = v[0], y = v[1], z = v[2];
+    return x * x + y * y + z * z;
+}
+
 // ------------------------------------------------ quantised CIC weights --
 // Every mixed-precision deposit uses integer CIC weights on a 2^-26 grid,
 // built from quantised moments of the in-cell offsets, indexed by axis set m
@@ -300,6 +320,7 @@ __global__ void __launch_bounds__(kPicThreads) k_push_mixed(PushArgs a) {
     unsigned lost_cnt[2 * D];
 #pragma unroll
     for (int q = 0; q < 2 * D; ++q) lost_cnt[q] = 0u;
+    double kin = 0.0;
     for (long long base = ((long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) * 4; base < count;
          base += stride) {
         const long long i0 = base + 4 * lane;
@@ -347,6 +368,7 @@ __global__ void __launch_bounds__(kPicThreads) k_push_mixed(PushArgs a) {
                     for (int q = 0; q < 2 * D; ++q) lost_cnt[q] += (lost == q);
                 }
                 key[j] = lost == -1 ? cell_to_key(a.g, cell[j][0], cell[j][1], cell[j][2]) : -1;
+                if (a.kin_part && key[j] >= 0) kin += a.kin_hmw * kinetic_v2(v[j]);
             }
         }
         if (a.acc) {
@@ -409,6 +431,7 @@ __global__ void __launch_bounds__(kPicThreads) k_push_mixed(PushArgs a) {
             for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
             if (lane == 0 && t) atomicAdd(a.losses + q, (unsigned long long)t);
         }
+        if (a.kin_part) block_sum_to(kin, a.kin_part);
     }
 }
 
@@ -940,7 +963,11 @@ __global__ void __launch_bounds__(kPicThreads, D == 2 ? 5 : 1) k_cls_pass2(ClsAr
     __shared__ float mstage[kClsWarps][NF][kMoverCap];
     __shared__ int mcls[kClsWarps][kMoverCap];
     __shared__ unsigned ccount[kClsWarps][32];
-    if (*a.far) return;   // some particle moved too far: the caller takes the general path
+    if (*a.far) {   // some particle moved too far: the caller takes the general path (and sums its energy)
+        if (a.p.kin_part && threadIdx.x == 0) a.p.kin_part[blockIdx.x] = 0.0;
+        return;
+    }
+    double kin = 0.0;   // kinetic energy of the particles this block writes (option "diagnostics 1")
     const long long ca = a.block_first[blockIdx.x], cb = a.block_first[blockIdx.x + 1];
     const GridView& g = a.p.g;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1010,6 +1037,7 @@ __global__ void __launch_bounds__(kPicThreads, D == 2 ? 5 : 1) k_cls_pass2(ClsAr
             for (int r = 0; r < kClsRounds; ++r) {
                 int cn[3];
                 const int cls = live[r] ? push_classify<D, PUSHER>(a.p, F, co, f[r], v[r], cn, lost_dummy) : -2;
+                if (a.p.kin_part && cls >= 0) kin += a.p.kin_hmw * kinetic_v2(v[r]);
                 const unsigned stay = __ballot_sync(full, cls == STAY);
                 if (cls == STAY) {
                     const unsigned dest = stay_next + (unsigned)__popc(stay & lt);
@@ -1037,6 +1065,7 @@ __global__ void __launch_bounds__(kPicThreads, D == 2 ? 5 : 1) k_cls_pass2(ClsAr
         }
         if (nm) flush(nm);
     }
+    if (a.p.kin_part) block_sum_to(kin, a.p.kin_part);
 }
 
 // Cell offsets of a sorted key array in O(particles + cells): the first and
@@ -1387,14 +1416,24 @@ struct RhoArgs {
     double coef[8];
     int ns;
     double background;
+    unsigned long long* qsum;   // per species: sum of the accumulators (exact integers; null: not summed)
 };
 
 __global__ void k_rho(RhoArgs a, double* __restrict__ rho, long long n) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const bool in = i < n;
     double r = a.background;
-    for (int s = 0; s < a.ns; ++s) r += a.coef[s] * (double)(long long)a.acc[s][i];
-    rho[i] = r;
+    for (int s = 0; s < a.ns; ++s) {
+        const long long v = in ? (long long)a.acc[s][i] : 0;
+        r += a.coef[s] * (double)v;
+        if (a.qsum) {   // the total charge of the density: integer sums, so any order gives the same bits
+            long long t = v;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+            if ((threadIdx.x & 31) == 0 && t) atomicAdd(a.qsum + s, (unsigned long long)t);
+        }
+    }
+    if (in) rho[i] = r;
 }
 
 // ------------------------------------------------------------ binning ---
@@ -1537,11 +1576,67 @@ __global__ void k_acc_sum(const unsigned long long* __restrict__ acc, long long 
 
 constexpr int kDiagBlocks = 296;
 
+// Per-step diagnostics from the partial sums the step's kernels wrote:
+// out[s] = kinetic energy of species s, out[ns] = (1/2) sum |grad phi|^2 * cell
+// volume (the field energy without epsilon), out[ns + 1] = particle charge.
+// One block; every sum runs in a fixed order, so repeats give the same bits.
+struct DiagFinishArgs {
+    const double* fe_part;
+    long long fe_n;
+    double fe_coef;                 // cell volume / 2
+    const double* kin_part[8];
+    long long kin_n[8];
+    const unsigned long long* qsum;
+    double q_coef[8];               // q * w * 2^-dep_shift per species
+    int ns;
+    double* out;
+};
+
+constexpr int kDiagFinishThreads = 256;   // small, so it finds a slot beside a running second pass
+
+__device__ double block_fixed_sum(const double* __restrict__ v, long long n) {
+    __shared__ double red[kDiagFinishThreads];
+    double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+    const long long st = blockDim.x;
+    long long i = threadIdx.x;
+    for (; i + 3 * st < n; i += 4 * st) {
+        t0 += v[i];
+        t1 += v[i + st];
+        t2 += v[i + 2 * st];
+        t3 += v[i + 3 * st];
+    }
+    for (; i < n; i += st) t0 += v[i];
+    const double t = (t0 + t1) + (t2 + t3);
+    __syncthreads();
+    red[threadIdx.x] = t;
+    __syncthreads();
+    for (int h = blockDim.x >> 1; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+        __syncthreads();
+    }
+    return red[0];
+}
+
+__global__ void __launch_bounds__(kDiagFinishThreads) k_diag_finish(DiagFinishArgs a) {
+    for (int s = 0; s < a.ns; ++s) {
+        const double k = a.kin_part[s] ? block_fixed_sum(a.kin_part[s], a.kin_n[s]) : 0.0;
+        if (threadIdx.x == 0) a.out[s] = k;
+    }
+    const double fe = a.fe_part ? block_fixed_sum(a.fe_part, a.fe_n) : 0.0;
+    if (threadIdx.x == 0) {
+        a.out[a.ns] = fe * a.fe_coef;
+        double q = 0.0;
+        for (int s = 0; s < a.ns; ++s) q += a.q_coef[s] * (double)(long long)a.qsum[s];
+        a.out[a.ns + 1] = q;
+    }
+}
+
 }  // namespace
 
 // ============================================================ host side ===
 
 static void finish_cls_step(psum_pic_ctx* c);
+static void finish_diagnostics(psum_pic_ctx* c, int par);
 constexpr int kPhaseContinued = 0x100;   // timing pair that adds time to a phase execution already counted
 
 psum_pic_ctx* ctx_check_nojoin(psum_pic_ctx* c) {
@@ -1698,6 +1793,8 @@ static PushArgs make_push_args(psum_pic_ctx* c, Species& sp, int sidx, double dt
     a.dep_lsh = sp.dep_shift - kCicBits;
     a.losses = c->losses.p + (size_t)sidx * 6;
     a.err = c->err.p;
+    a.kin_part = nullptr;
+    a.kin_hmw = 0.5 * sp.m * sp.w;
     (void)pusher;
     return a;
 }
@@ -1721,6 +1818,28 @@ static void launch_mixed(const PushArgs& a, int dim, int pusher, bool deposit_on
 static void zero_accumulators(psum_pic_ctx* c) {
     for (auto& sp : c->sp)
         cuda_check(cudaMemsetAsync(sp->acc.p, 0, sizeof(unsigned long long) * c->g.n_nodes, c->stream), "memset acc");
+}
+
+// Edge differences of phi for the mixed push, and in a step with
+// diagnostics the field-energy partial sums (FP64 mode: the sums only).
+static void launch_edges(psum_pic_ctx* c, const double* phi, cudaStream_t s) {
+    const bool fe = c->diag_in_step;
+    if (c->precision != PSUM_PIC_MIXED && !fe) return;
+    const unsigned blocks = blocks_for(c->g.n_nodes, 256);
+    float* edges = c->precision == PSUM_PIC_MIXED ? c->edges.p : nullptr;
+    double* part = fe ? c->dbuf[c->diag_par].fe.p : nullptr;
+    if (fe) c->dbuf[c->diag_par].fe_n = blocks;
+    if (c->g.dim == 2) { k_edges<2><<<blocks, 256, 0, s>>>(c->g, phi, edges, part); count_launch(); }
+    else { k_edges<3><<<blocks, 256, 0, s>>>(c->g, phi, edges, part); count_launch(); }
+}
+
+// Kinetic-energy partials of species si for a push launched with `blocks`
+// blocks (in a step with diagnostics; null otherwise).
+static double* kin_slot(psum_pic_ctx* c, int si, long long blocks) {
+    if (!c->diag_in_step || si >= 8) return nullptr;
+    auto& d = c->dbuf[c->diag_par];
+    d.kin_n[si] = blocks;
+    return d.kin.p + d.kin_off[si];
 }
 
 static void deposit_all(psum_pic_ctx* c) {
@@ -1751,10 +1870,7 @@ static void push_all(psum_pic_ctx* c, const double* phi, double dt, int pusher, 
     if (!(std::isfinite(dt))) throw Error(PSUM_ERR_NONFINITE, "push: non-finite dt");
     cudaStream_t s = c->stream;
     zero_accumulators(c);
-    if (c->precision == PSUM_PIC_MIXED) {
-        if (c->g.dim == 2) { k_edges<2><<<blocks_for(c->g.n_nodes, 256), 256, 0, s>>>(c->g, phi, c->edges.p); count_launch(); }
-        else { k_edges<3><<<blocks_for(c->g.n_nodes, 256), 256, 0, s>>>(c->g, phi, c->edges.p); count_launch(); }
-    }
+    launch_edges(c, phi, s);
     for (int si = 0; si < (int)c->sp.size(); ++si) {
         Species& sp = *c->sp[si];
         if (sp.n <= 0) continue;
@@ -1762,6 +1878,7 @@ static void push_all(psum_pic_ctx* c, const double* phi, double dt, int pusher, 
         if (c->precision == PSUM_PIC_MIXED) {
             ensure_keys(c, sp);
             PushArgs a = make_push_args(c, sp, si, dt, pusher, B);
+            a.kin_part = kin_slot(c, si, capped_blocks(4LL * kPicThreads, sp.n));
             launch_mixed(a, c->g.dim, pusher, false, sp.n, s);
         } else {
             Push64Args a{};
@@ -1782,6 +1899,8 @@ static void push_all(psum_pic_ctx* c, const double* phi, double dt, int pusher, 
             a.scale = std::ldexp(1.0, sp.dep_shift);
             a.losses = c->losses.p + (size_t)si * 6;
             a.err = c->err.p;
+            a.kin_part = kin_slot(c, si, push64_blocks(sp.n));
+            a.kin_hmw = 0.5 * sp.m * sp.w;
             launch_push64(a, sp.n, s);
         }
     }
@@ -1904,8 +2023,7 @@ static void cls_step(psum_pic_ctx* c, const double* phi, double dt, int pusher, 
     cudaStream_t s = c->stream;
     ensure_cls_buffers(c);
     zero_accumulators(c);
-    if (c->g.dim == 2) { k_edges<2><<<blocks_for(c->g.n_nodes, 256), 256, 0, s>>>(c->g, phi, c->edges.p); count_launch(); }
-    else { k_edges<3><<<blocks_for(c->g.n_nodes, 256), 256, 0, s>>>(c->g, phi, c->edges.p); count_launch(); }
+    launch_edges(c, phi, s);
     cuda_check(cudaMemsetAsync(c->far_flag.p, 0, sizeof(int) * 8, s), "memset");
     const int ns = (int)c->sp.size();
     const long long nc = c->g.n_cells;
@@ -1950,8 +2068,12 @@ static void cls_step(psum_pic_ctx* c, const double* phi, double dt, int pusher, 
     for (int si = 0; si < ns; ++si) {
         if (c->sp[si]->n <= 0) continue;
         args[si].block_first = c->sp[si]->cls_first2.p;
+        // the second pass sums the kinetic energy of the particles it writes
+        args[si].p.kin_part = kin_slot(c, si, cls_blocks2(c->sp[si]->n, nc, c->g.dim));
         launch_pass(args[si], c->g.dim, pusher, 2, c->sp[si]->n, c->side);
     }
+    c->pend_diag = c->diag_in_step;
+    c->pend_par = c->diag_par;
     if (c->timing) {
         cuda_check(cudaEventRecord(t1, c->side), "cudaEventRecord");
         c->events.push_back({2 | kPhaseContinued, {t0, t1}});   // push phase: the second passes
@@ -1993,12 +2115,23 @@ static void finish_cls_step(psum_pic_ctx* c) {
         PushArgs pa = make_push_args(c, sp, si, c->pend_dt, c->pend_pusher, c->pend_has_B ? c->pend_B : nullptr);
         pa.acc = nullptr;
         pa.losses = c->losses.p + 6 * 8;   // discard slot: pass 1 already counted this step's losses
+        if (c->pend_diag && si < 8) {      // the second pass wrote nothing: the move in place sums the energy
+            auto& d = c->dbuf[c->pend_par];
+            d.kin_n[si] = capped_blocks(4LL * kPicThreads, sp.n);
+            pa.kin_part = d.kin.p + d.kin_off[si];
+        }
         launch_mixed(pa, c->g.dim, c->pend_pusher, false, sp.n, s);
         sort_species(c, sp, si);
         cuda_check(cudaMemsetAsync(sp.acc.p, 0, sizeof(unsigned long long) * c->g.n_nodes, s), "memset acc");
         ensure_keys(c, sp);
         PushArgs da = make_push_args(c, sp, si, 0.0, 0, nullptr);
         launch_mixed(da, c->g.dim, 0, true, sp.n, s);
+        t.stop();
+    }
+    if (c->pend_diag) {
+        c->pend_diag = false;
+        PhaseTimer t(c, 4);
+        finish_diagnostics(c, c->pend_par);
         t.stop();
     }
     cuda_check(cudaGetLastError(), "fused step finish");
@@ -2018,8 +2151,54 @@ static void rho_into(psum_pic_ctx* c, double background, double* rho, int only_s
         a.coef[a.ns] = (with_charge ? sp.q : 1.0) * sp.w / vol * std::ldexp(1.0, -sp.dep_shift);
         a.ns++;
     }
+    // in a step with diagnostics the density also sums the charge it holds
+    if (c->diag_in_step && only_species < 0 && with_charge) {
+        a.qsum = c->dbuf[c->diag_par].qsum.p;
+        cuda_check(cudaMemsetAsync(a.qsum, 0, sizeof(unsigned long long) * 8, c->stream), "memset qsum");
+    }
     { k_rho<<<blocks_for(c->g.n_nodes, 256), 256, 0, c->stream>>>(a, rho, c->g.n_nodes); count_launch(); }
     cuda_check(cudaGetLastError(), "rho launch");
+}
+
+// Buffers of the per-step diagnostics, sized for the largest push grid of
+// every species (fused first pass, general mixed push, FP64 push).
+static void ensure_diag_buffers(psum_pic_ctx* c) {
+    auto& d = c->dbuf[c->diag_par];
+    grow(d.fe, (size_t)blocks_for(c->g.n_nodes, 256));
+    long long off = 0;
+    for (int s = 0; s < (int)c->sp.size() && s < 8; ++s) {
+        const long long n = std::max<long long>(c->sp[s]->n, 1);
+        d.kin_off[s] = off;
+        d.kin_n[s] = 0;
+        off += std::max({cls_blocks2(n, c->g.n_cells, c->g.dim), (long long)capped_blocks(4LL * kPicThreads, n),
+                         push64_blocks(n)});
+    }
+    grow(d.kin, (size_t)std::max<long long>(off, 1));
+    grow(d.qsum, 8);
+    grow(c->diag_out, 16);
+    d.fe_n = 0;
+}
+
+// Reduces the step's partial sums into diag_out (context stream, after the push).
+static void finish_diagnostics(psum_pic_ctx* c, int par) {
+    const auto& d = c->dbuf[par];
+    DiagFinishArgs a{};
+    a.fe_part = d.fe_n ? d.fe.p : nullptr;
+    a.fe_n = d.fe_n;
+    double vol = 1.0;
+    for (int d = 0; d < c->g.dim; ++d) vol *= c->g.dx[d];
+    a.fe_coef = 0.5 * vol;
+    a.ns = std::min<int>((int)c->sp.size(), 8);
+    for (int s = 0; s < a.ns; ++s) {
+        Species& sp = *c->sp[s];
+        a.kin_part[s] = d.kin_n[s] ? d.kin.p + d.kin_off[s] : nullptr;
+        a.kin_n[s] = d.kin_n[s];
+        a.q_coef[s] = sp.q * sp.w * std::ldexp(1.0, -sp.dep_shift);
+    }
+    a.qsum = d.qsum.p;
+    a.out = c->diag_out.p;
+    { k_diag_finish<<<1, kDiagFinishThreads, 0, c->stream>>>(a); count_launch(); }
+    cuda_check(cudaGetLastError(), "diagnostics launch");
 }
 
 }  // namespace psum_b200
@@ -2117,6 +2296,9 @@ EXPORT int psum_pic_set_options(psum_pic_ctx* ctx, const char* options) {
             if (key == "sort_interval") {
                 if (v < 0) throw std::invalid_argument("sort_interval must be >= 0");
                 ctx->sort_interval = v;
+            } else if (key == "diagnostics") {
+                if (v != 0 && v != 1) throw std::invalid_argument("diagnostics must be 0 or 1");
+                ctx->diag = v != 0;
             } else {
                 throw std::invalid_argument("set_options: unknown particle option '" + key + "'");
             }
@@ -2575,6 +2757,16 @@ EXPORT int psum_pic_step(psum_pic_ctx* ctx, psum_field_solver_handle solver, dou
             if (far) finish_cls_step(ctx);
         }
         cudaStream_t user = ctx->stream;
+        if (ctx->diag) {
+            if (ctx->sp.size() > 8) throw std::invalid_argument("step diagnostics: more than 8 species");
+            ctx->diag_par ^= 1;   // the pending step (if any) keeps the other buffers until it is joined
+            ensure_diag_buffers(ctx);
+        }
+        ctx->diag_in_step = ctx->diag;
+        struct DiagOff {
+            psum_pic_ctx* c;
+            ~DiagOff() { c->diag_in_step = false; }
+        } diag_off{ctx};
         cuda_check(cudaEventRecord(ctx->ev_in, user), "cudaEventRecord");
         cuda_check(cudaStreamWaitEvent(ctx->prio, ctx->ev_in, 0), "cudaStreamWaitEvent");
         ctx->stream = ctx->prio;
@@ -2619,6 +2811,13 @@ EXPORT int psum_pic_step(psum_pic_ctx* ctx, psum_field_solver_handle solver, dou
                 t.stop();
             }
         }
+        // a fused step reduces its sums when it is joined; the general path has none pending
+        if (ctx->diag && !ctx->pending) {
+            PhaseTimer t(ctx, 4);
+            finish_diagnostics(ctx, ctx->diag_par);
+            t.stop();
+        }
+        ctx->diag_valid = ctx->diag;
     });
 }
 
@@ -2639,13 +2838,52 @@ EXPORT int psum_pic_get_timing(psum_pic_ctx* ctx, double* ms_host, int* count_ho
             if (count_host) count_host[p] = 0;
         }
         for (auto& e : ctx->events) {
+            const int p = e.first & 0xff;
+            if (p >= 4) continue;   // the diagnostics phase is reported by psum_pic_get_phase_times
             float ms = 0.f;
             cuda_check(cudaEventElapsedTime(&ms, e.second.first, e.second.second), "cudaEventElapsedTime");
-            const int p = e.first & 0xff;
             ms_host[p] += ms;
             if (count_host && !(e.first & kPhaseContinued)) count_host[p] += 1;
         }
         if (reset) ctx->drop_events();
+    });
+}
+
+EXPORT int psum_pic_get_phase_times(psum_pic_ctx* ctx, double* ms_host, int* count_host, int n_phases, int reset) {
+    return guarded([&] {
+        ctx_check(ctx);
+        if (!ms_host || n_phases < 1) throw std::invalid_argument("get_phase_times: null output or no phases");
+        cuda_check(cudaStreamSynchronize(ctx->stream), "timing sync");
+        for (int p = 0; p < n_phases; ++p) {
+            ms_host[p] = 0.0;
+            if (count_host) count_host[p] = 0;
+        }
+        for (auto& e : ctx->events) {
+            const int p = e.first & 0xff;
+            if (p >= n_phases) continue;
+            float ms = 0.f;
+            cuda_check(cudaEventElapsedTime(&ms, e.second.first, e.second.second), "cudaEventElapsedTime");
+            ms_host[p] += ms;
+            if (count_host && !(e.first & kPhaseContinued)) count_host[p] += 1;
+        }
+        if (reset) ctx->drop_events();
+    });
+}
+
+EXPORT int psum_pic_get_step_diagnostics(psum_pic_ctx* ctx, double epsilon, double* out_host) {
+    return guarded([&] {
+        ctx_check(ctx);
+        if (!out_host) throw std::invalid_argument("get_step_diagnostics: null output");
+        if (!ctx->diag_valid)
+            throw std::invalid_argument("get_step_diagnostics: no step with option 'diagnostics 1' has run");
+        const int ns = (int)ctx->sp.size();
+        double v[16];
+        cuda_check(cudaMemcpyAsync(v, ctx->diag_out.p, sizeof(double) * (ns + 2), cudaMemcpyDeviceToHost, ctx->stream),
+                   "D2H");
+        cuda_check(cudaStreamSynchronize(ctx->stream), "diag sync");
+        for (int s = 0; s < ns; ++s) out_host[s] = v[s];
+        out_host[ns] = epsilon * v[ns];
+        out_host[ns + 1] = v[ns + 1];
     });
 }
 

@@ -83,6 +83,26 @@ struct psum_pic_ctx {
     bool pend_has_B = false;
     double pend_B[3] = {0, 0, 0};
     int sort_interval = 1;
+    // per-step diagnostics (option "diagnostics 1"): partial sums written by the
+    // step's own kernels (field energy by k_edges, kinetic energy by the push,
+    // charge by k_rho), reduced by k_diag_finish into diag_out
+    // The partial sums are double buffered by step parity: a fused step's sums
+    // are reduced when it is joined, after the next step's density has begun.
+    struct DiagBufs {
+        psum_b200::DevBuf<double> fe, kin;
+        psum_b200::DevBuf<unsigned long long> qsum;
+        long long fe_n = 0;
+        long long kin_n[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        long long kin_off[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    };
+    bool diag = false;
+    bool diag_in_step = false;                // set while psum_pic_step launches its kernels
+    DiagBufs dbuf[2];
+    int diag_par = 0;                         // parity of the current step's buffers
+    bool pend_diag = false;                   // the pending fused step's sums await their reduction
+    int pend_par = 0;
+    psum_b200::DevBuf<double> diag_out;
+    bool diag_valid = false;
     long long steps = 0;
     bool timing = false;
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> events;   // (phase, start/stop)

@@ -90,6 +90,23 @@ __device__ __forceinline__ void warp_deposit(unsigned long long* __restrict__ ac
     if (tail && node >= 0 && val != 0) atomicAdd(acc + node, (unsigned long long)val);
 }
 
+// Block sum of one FP64 value per thread in a fixed order (warp butterflies,
+// then the warp totals in warp order), written by thread 0 to out[blockIdx.x].
+// Every thread of the block calls it; blockDim.x is a multiple of 32, at most 1024.
+__device__ __forceinline__ void block_sum_to(double v, double* __restrict__ out) {
+    __shared__ double warp_tot[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncthreads();   // warp_tot may still be read by an earlier call
+    if ((threadIdx.x & 31) == 0) warp_tot[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += warp_tot[w];
+        out[blockIdx.x] = s;
+    }
+}
+
 // Count per (axis, side) losses of a warp with one atomic per nonzero counter.
 __device__ __forceinline__ void warp_count_losses(unsigned long long* losses, int dim, int lost_code) {
     // lost_code: -1 none, else axis*2+side

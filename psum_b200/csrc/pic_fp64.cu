@@ -111,6 +111,7 @@ __global__ void __launch_bounds__(kPicThreads) k_push64(Push64Args a) {
     const long long count = *a.count;
     const int D = g.dim;
     const int lane = threadIdx.x & 31;
+    double kin = 0.0;
     for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < count;
          base += (long long)gridDim.x * blockDim.x) {
         const long long i = base + lane;
@@ -185,12 +186,14 @@ __global__ void __launch_bounds__(kPicThreads) k_push64(Push64Args a) {
             for (int d = 0; d < D; ++d) a.pos[d][i] = p[d];
             if (!alive) a.pos[0][i] = __longlong_as_double(0x7ff8000000000000LL);   // NaN x: invalid
             a.key[i] = alive ? key64(g, p) : -1;
+            if (a.kin_part && alive) kin += a.kin_hmw * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
         } else if (i < count) {
             a.key[i] = -1;
         }
         warp_count_losses(a.losses, D, lost);
         if (a.acc) deposit64(g, p, alive, a.acc, a.scale);
     }
+    if (a.kin_part) block_sum_to(kin, a.kin_part);
 }
 
 __global__ void __launch_bounds__(kPicThreads) k_deposit64(Deposit64Args a) {
@@ -221,11 +224,14 @@ __global__ void k_keys64(GridView g, const double* __restrict__ x, const double*
 
 }  // namespace
 
+long long push64_blocks(long long n_upper) {
+    const long long warps = (std::max<long long>(n_upper, 1) + 31) / 32;
+    return std::min<long long>((warps + 7) / 8, 148LL * 16);
+}
+
 void launch_push64(const Push64Args& a, long long n_upper, cudaStream_t s) {
     if (n_upper <= 0) return;
-    const long long warps = (n_upper + 31) / 32;
-    const unsigned blocks = (unsigned)std::min<long long>((warps + 7) / 8, 148LL * 16);
-    { k_push64<<<blocks, kPicThreads, 0, s>>>(a); count_launch(); }
+    { k_push64<<<(unsigned)push64_blocks(n_upper), kPicThreads, 0, s>>>(a); count_launch(); }
 }
 
 void launch_deposit64(const Deposit64Args& a, long long n_upper, cudaStream_t s) {

@@ -24,6 +24,8 @@ struct Push64Args {
     double scale;
     unsigned long long* losses;
     unsigned* err;
+    double* kin_part;   // per-block kinetic energy of the surviving particles (null: not summed)
+    double kin_hmw;     // m * w / 2
 };
 
 struct Deposit64Args {
@@ -35,6 +37,7 @@ struct Deposit64Args {
 };
 
 void launch_push64(const Push64Args& a, long long n_upper, cudaStream_t s);
+long long push64_blocks(long long n_upper);   // grid size of launch_push64
 void launch_deposit64(const Deposit64Args& a, long long n_upper, cudaStream_t s);
 void launch_keys64(const GridView& g, double* const pos[3], int* key, const long long* count, long long n_upper,
                    cudaStream_t s);

@@ -170,16 +170,25 @@ class ParticleContext:
         check(lib().psum_pic_set_timing(self.handle, int(bool(enable))))
 
     def get_timing(self, reset=True):
-        """Accumulated ms and counts per step phase: rho, solve, push, sort."""
-        ms = np.zeros(4)
-        cnt = np.zeros(4, np.int32)
-        check(lib().psum_pic_get_timing(self.handle, _ptr(ms), _ptr(cnt), int(reset)))
-        return dict(zip(("rho", "solve", "push", "sort"), zip(ms.tolist(), cnt.tolist())))
+        """Accumulated ms and counts per step phase: rho, solve, push, sort, diag (the reduction of the
+        per-step diagnostics of option 'diagnostics 1')."""
+        names = ("rho", "solve", "push", "sort", "diag")
+        ms = np.zeros(len(names))
+        cnt = np.zeros(len(names), np.int32)
+        check(lib().psum_pic_get_phase_times(self.handle, _ptr(ms), _ptr(cnt), len(names), int(reset)))
+        return dict(zip(names, zip(ms.tolist(), cnt.tolist())))
 
     def diagnostics(self, phi, epsilon):
         out = np.zeros(len(self.species) + 2)
         self._order(phi)
         check(lib().psum_pic_diagnostics(self.handle, _ptr(phi), float(epsilon), _ptr(out)))
+        return {"kinetic": out[:len(self.species)].copy(), "field": out[-2], "charge": out[-1]}
+
+    def step_diagnostics(self, epsilon):
+        """The diagnostics the last psum_pic_step computed (option 'diagnostics 1'): kinetic energy per
+        species after the push, field energy of the step's phi, charge of the step's density."""
+        out = np.zeros(len(self.species) + 2)
+        check(lib().psum_pic_get_step_diagnostics(self.handle, float(epsilon), _ptr(out)))
         return {"kinetic": out[:len(self.species)].copy(), "field": out[-2], "charge": out[-1]}
 
     def device_errors(self):

@@ -733,3 +733,41 @@ def test_append_after_step_equals_load_of_concatenation(precision, kind):
     # from device arrays
     ctx.append(sp, dev(pos[:, :10]), dev(vel[:, :10]))
     assert ctx.count(sp)[0] == ns0 + 10
+
+
+@pytest.mark.parametrize("path", ["fused", "general", "fp64"])
+@pytest.mark.parametrize("kind", ["2d_absorb", "3d_periodic"])
+def test_step_diagnostics_equal_separate_diagnostics(path, kind):
+    """Option 'diagnostics 1': the kinetic energy summed by the push, the field energy summed by the edge kernel
+    and the charge summed by the density equal psum_pic_diagnostics of the same state (kinetic after the step,
+    field of the step's phi, charge of the density the step solved for).  FP64 sums of the same terms in another
+    order: relative 1e-12; the charge is an integer sum, so it is exact."""
+    precision = P.FP64 if path == "fp64" else P.MIXED
+    ctx, g, pos, vel, phi = make_case(kind, precision, seed=41, n=50000)
+    pos = wrap_into(pos, g)
+    ctx.set_options(f"sort_interval {0 if path == 'general' else 1} diagnostics 1")
+    sps = []
+    for s in range(2):
+        sp = ctx.add_species(-1.0 if s == 0 else 1.0, 1.0 if s == 0 else 4.0, 0.5, pos.shape[1])
+        ctx.load(sp, pos, vel * (1.0 if s == 0 else 0.5))
+        sps.append(sp)
+    ctx.sort()
+    ctx.deposit()
+    nn = ctx.n_nodes
+    solver = _identity_solver(g, nn)   # max_cycles 0: phi stays the case's field
+    rho = dev(np.zeros(nn))
+    phi_t = dev(phi)
+    eps = 0.7
+    with pytest.raises(P.PsumError):
+        ctx.step_diagnostics(eps)      # no step with diagnostics yet
+    ctx.set_timing(True)
+    for _ in range(3):
+        before = ctx.diagnostics(None, 1.0)
+        ctx.step(solver, 0.0, rho, phi_t, 0.12)
+        got = ctx.step_diagnostics(eps)
+        exp = ctx.diagnostics(phi_t, eps)
+        np.testing.assert_allclose(got["kinetic"], exp["kinetic"], rtol=1e-12, atol=0)
+        assert abs(got["field"] - exp["field"]) <= 1e-12 * abs(exp["field"])
+        assert got["charge"] == before["charge"]
+    phases = ctx.get_timing(reset=True)
+    assert phases["diag"][1] == 3 and phases["push"][1] == 3
