@@ -1146,8 +1146,8 @@ int oracle_mg_solve_mixed(void* h, const double* b, double* x, int max_cycles, i
 }
 
 // The same refinement loop with the GPU backends' stopping rule: stop after
-// the first batch whose squared relative residual is at most tol^2 (tol 0:
-// run max_cycles).  Returns the batches run; hist[k] = squared relative
+// the first batch whose relative residual ||b - A x|| / ||b|| is at most tol
+// (tol 0: run max_cycles).  Returns the batches run; hist[k] = relative
 // residual after batch k.
 int oracle_mg_solve_mixed_tol(void* h, const double* b, double* x, int max_cycles, int correction_interval, int pre,
                               int post, double tol, double* hist) {
@@ -1163,11 +1163,11 @@ int oracle_mg_solve_mixed_tol(void* h, const double* b, double* x, int max_cycle
         for (long long i = 0; i < n; ++i) r32[i] = (float)r[i];
         mg_vcycles<float>(*mg, r32, e32, batch, pre, post);
         for (long long i = 0; i < n; ++i) xv[i] += (double)e32[i];
-        const double rel2 = norm2(residual(mg->A, bv, xv)) / (bn > 0 ? bn : 1.0);
-        if (hist) hist[batches] = rel2;
+        const double rel = norm2(residual(mg->A, bv, xv)) / (bn > 0 ? bn : 1.0);
+        if (hist) hist[batches] = rel;
         ++batches;
         cycle += batch;
-        if (tol > 0 && rel2 <= tol * tol) break;
+        if (tol > 0 && rel <= tol) break;
     }
     std::copy(xv.begin(), xv.end(), x);
     return batches;

@@ -110,9 +110,63 @@ struct DevAxis {
 
 // Launches of the stencil kernels with the operator's tap count as a
 // compile-time constant where it is one of the common ones.
+// Levels of at least this many rows take the TMA-staged sweep (when the
+// solver's option `tma` is on and the box is 2-D or 3-D).
+constexpr long long kTmaMinRows = 1LL << 16;
+
+template <class T, int Mode, int NS>
+void launch_tma_ns(const StencilDev<T>& A, const TmaTile& V, size_t smem, unsigned blocks, const T* x, const T* b,
+                   T* out, T omega, const MGState* st, int* stall, cudaStream_t s) {
+    static bool attr = false;
+    if (!attr) {
+        cuda_check(cudaFuncSetAttribute(k_level_op_tma<T, Mode, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)(96 * 1024)),
+                   "cudaFuncSetAttribute");
+        attr = true;
+    }
+    k_level_op_tma<T, Mode, NS><<<blocks, kTmaThreads, smem, s>>>(A, V, x, b, out, omega, st, stall);
+}
+
+// TMA-staged sweep of a level (k_level_op_tma); false when the level does
+// not qualify (small, or a 1-D box).
+template <class T, int Mode>
+bool launch_level_op_tma(const StencilDev<T>& A, const T* x, const T* b, T* out, T omega, const MGState* st,
+                         int* stall, cudaStream_t s) {
+    using S = TmaShape<T>;
+    if (Mode == kSmoothFromZero || A.n < kTmaMinRows) return false;
+    TmaTile V{};
+    int TR;
+    if (A.n0 > 1 && A.n1 > 1 && A.n2 > 1) {
+        V.P = A.n0; V.R = A.n1; V.C = A.n2;
+        TR = S::TR3;
+        V.chunk = 16;
+    } else if (A.n2 == 1 && A.n0 > 1 && A.n1 > 1) {
+        V.P = 1; V.R = A.n0; V.C = A.n1;
+        TR = S::TR2;
+        V.chunk = 1;
+    } else {
+        return false;
+    }
+    V.tiles_c = (V.C + S::TC - 1) / S::TC;
+    V.tiles_r = (V.R + TR - 1) / TR;
+    V.chunks = (V.P + V.chunk - 1) / V.chunk;
+    V.lrow = S::lrow();
+    const int nslots = V.P > 1 ? kTmaSlots : 1;
+    const size_t smem = sizeof(T) * (size_t)nslots * (TR + 2) * V.lrow + sizeof(int) * (size_t)nslots * (TR + 2);
+    const unsigned blocks = (unsigned)((long long)V.tiles_c * V.tiles_r * V.chunks);
+    if (A.ns == 5) launch_tma_ns<T, Mode, 5>(A, V, smem, blocks, x, b, out, omega, st, stall, s);
+    else if (A.ns == 7) launch_tma_ns<T, Mode, 7>(A, V, smem, blocks, x, b, out, omega, st, stall, s);
+    else if (A.ns == 9) launch_tma_ns<T, Mode, 9>(A, V, smem, blocks, x, b, out, omega, st, stall, s);
+    else if (A.ns == 27) launch_tma_ns<T, Mode, 27>(A, V, smem, blocks, x, b, out, omega, st, stall, s);
+    else launch_tma_ns<T, Mode, 0>(A, V, smem, blocks, x, b, out, omega, st, stall, s);
+    count_launch();
+    return true;
+}
+
 template <class T, int Mode>
 void launch_level_op(const StencilDev<T>& A, const T* x, const T* b, T* out, T omega, const MGState* st,
-                     cudaStream_t s) {
+                     cudaStream_t s, int* stall = nullptr) {
+    if (stall && launch_level_op_tma<T, Mode>(A, x, b, out, omega, st, stall, s)) return;
     const unsigned g = grid_for(A.n);
     if (Mode == kSmoothFromZero) k_level_op<T, Mode, 0><<<g, kThreads, 0, s>>>(A, x, b, out, omega, st);
     else if (A.ns == 5) k_level_op<T, Mode, 5><<<g, kThreads, 0, s>>>(A, x, b, out, omega, st);
@@ -161,6 +215,7 @@ struct SolverBase {
     int null_space = 0;                     // option `null_space 0|1` (read by set_matrix)
     bool ns_built = false;                  // the hierarchy was built for a singular operator
     int use_graph = 1;                      // option `graph 0|1`: replay the solve as one CUDA graph
+    int use_tma = 1;                        // option `tma 0|1`: TMA-staged sweeps on large levels
     unsigned long long n_row = 0;
     bool ready = false;
     cudaStream_t own_stream = nullptr;
@@ -224,9 +279,10 @@ struct Solver : SolverBase {
             if (l < host.L) L->op.upload(host.ahat[l], s);
             std::vector<T> d(host.dinv[l].begin(), host.dinv[l].end());
             L->dinv.upload(d.data(), d.size(), s);
-            L->bufA.alloc(L->n);
-            L->bufB.alloc(L->n);
-            L->b.alloc(L->n);
+            // +16 elements: the TMA-staged sweep's 16-byte-aligned copies may read past a vector's last element
+            L->bufA.alloc(L->n + 16);
+            L->bufB.alloc(L->n + 16);
+            L->b.alloc(L->n + 16);
             if (l < host.L) {
                 for (int a = 0; a < 3; ++a) L->axes[a].upload(host.xfer[l][a], s, L->xfer.ax[a]);
                 const AxisDev<T>* ax = L->xfer.ax;
@@ -238,11 +294,14 @@ struct Solver : SolverBase {
             lv.push_back(std::move(L));
         }
         coarse_inv.upload(host.coarse_inv.data(), host.coarse_inv.size(), s);
-        if (precision == 64) x64.alloc(n_row);
+        if (precision == 64) x64.alloc(n_row + 16);
         cuda_check(cudaStreamSynchronize(s), "build_device");
         levels = host.L + 1;
         coarse_rows = (unsigned long long)lv.back()->n;
     }
+
+    // the stall word of the TMA-staged sweeps, or null when option `tma` is off
+    int* tma_stall() { return use_tma ? &state.p->stall : nullptr; }
 
     // Enqueue `cycles` V(pre,post) cycles on level-0 (x0 in/out, b0 = scaled rhs).
     // `x_is_zero`: the level-0 iterate starts at zero (first sweep simplified).
@@ -268,7 +327,7 @@ struct Solver : SolverBase {
                 launch_level_op<T, kSmoothFromZero>(V.op.view, xcur[l], bl[l], xoth[l], omega, st, s);
                 zero[l] = false;
             } else {
-                launch_level_op<T, kSmooth>(V.op.view, xcur[l], bl[l], xoth[l], omega, st, s);
+                launch_level_op<T, kSmooth>(V.op.view, xcur[l], bl[l], xoth[l], omega, st, s, tma_stall());
             }
             std::swap(xcur[l], xoth[l]);
         };
@@ -281,7 +340,7 @@ struct Solver : SolverBase {
                     { k_restrict<T><<<grid_for(lv[l + 1]->n), kThreads, 0, s>>>(V.xfer, bl[l], bl[l + 1], xcur[l + 1],
                                                                              lv[l + 1]->dinv.p, st); count_launch(); }
                 } else {
-                    launch_level_op<T, kResidual>(V.op.view, xcur[l], bl[l], xoth[l], omega, st, s);
+                    launch_level_op<T, kResidual>(V.op.view, xcur[l], bl[l], xoth[l], omega, st, s, tma_stall());
                     { k_restrict<T><<<grid_for(lv[l + 1]->n), kThreads, 0, s>>>(V.xfer, xoth[l], bl[l + 1],
                                                                              xcur[l + 1], lv[l + 1]->dinv.p, st); count_launch(); }
                 }
@@ -481,6 +540,7 @@ void solver_set_options(SolverBase* s, const char* options) {
         else if (key == "periodic_J") s->periodic[1] = parse_int(iss, key) != 0;
         else if (key == "periodic_K") s->periodic[2] = parse_int(iss, key) != 0;
         else if (key == "graph") s->use_graph = parse_int(iss, key) != 0;
+        else if (key == "tma") s->use_tma = parse_int(iss, key) != 0;
         else if (key == "null_space") s->null_space = parse_int(iss, key) != 0;
         else if (key == "correction_interval") {
             int v = 0;
@@ -637,6 +697,7 @@ void ft_solve(psum_field_solver_handle h, double* b, double* x) {
     cuda_check(cudaStreamSynchronize(s->own_stream), "solve sync");
     MGState st = solver_read_state(s, s->own_stream);
     if (st.status == PSUM_ERR_DIVERGED) throw Error(PSUM_ERR_DIVERGED, "multigrid: residual diverged");
+    if (st.stall) throw Error(PSUM_ERR_INTERNAL, "multigrid: a TMA-staged sweep stopped waiting for its copies");
 }
 
 void ft_set_options(psum_field_solver_handle h, const char* o) { solver_set_options(solver_from_handle(h), o); }
@@ -706,11 +767,12 @@ EXPORT int psum_mg_solve(psum_field_solver_handle h, double* b_dev, double* x_de
         SolverBase* s = solver_from_handle(h);
         solver_solve_async(s, b_dev, x_dev, s->own_stream);
         MGState st = solver_read_state(s, s->own_stream);
-        status = st.status;
+        status = st.stall ? PSUM_ERR_INTERNAL : st.status;
     });
     if (rc != PSUM_OK) return rc;
     if (status == PSUM_ERR_NOT_CONVERGED) set_last_error("multigrid: tol not reached within max_cycles");
     if (status == PSUM_ERR_DIVERGED) set_last_error("multigrid: residual diverged");
+    if (status == PSUM_ERR_INTERNAL) set_last_error("multigrid: a TMA-staged sweep stopped waiting for its copies");
     return status;
 }
 

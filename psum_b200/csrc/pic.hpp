@@ -71,6 +71,7 @@ struct psum_pic_ctx {
     // moved more than one cell, with the step's dt, pusher and B kept here).
     cudaStream_t side = nullptr;              // least priority
     cudaEvent_t ev_pass1 = nullptr, ev_pass2 = nullptr;
+    cudaEvent_t ev_sp[8] = {};                // per species: its first pass, offsets and scan are done
     // A step's charge density and solve run on `prio` (greatest priority),
     // ordered after the context stream (ev_in) and before it (ev_out), so
     // that their blocks are scheduled ahead of a pending second pass.
@@ -83,6 +84,7 @@ struct psum_pic_ctx {
     bool pend_has_B = false;
     double pend_B[3] = {0, 0, 0};
     int sort_interval = 1;
+    bool fp64_fma = false;                    // FP64 mode: the contracted kernel build (not bit-exact)
     // per-step diagnostics (option "diagnostics 1"): partial sums written by the
     // step's own kernels (field energy by k_edges, kinetic energy by the push,
     // charge by k_rho), reduced by k_diag_finish into diag_out
@@ -122,6 +124,8 @@ struct psum_pic_ctx {
         drop_events();
         if (ev_pass1) cudaEventDestroy(ev_pass1);
         if (ev_pass2) cudaEventDestroy(ev_pass2);
+        for (auto e : ev_sp)
+            if (e) cudaEventDestroy(e);
         if (ev_in) cudaEventDestroy(ev_in);
         if (ev_out) cudaEventDestroy(ev_out);
         if (prio) {

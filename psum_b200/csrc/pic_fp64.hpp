@@ -36,10 +36,20 @@ struct Deposit64Args {
     double scale;
 };
 
-void launch_push64(const Push64Args& a, long long n_upper, cudaStream_t s);
-long long push64_blocks(long long n_upper);   // grid size of launch_push64
-void launch_deposit64(const Deposit64Args& a, long long n_upper, cudaStream_t s);
-void launch_keys64(const GridView& g, double* const pos[3], int* key, const long long* count, long long n_upper,
-                   cudaStream_t s);
+// Launchers of the two builds of pic_fp64_kernels.cuh: fp64_exact (no
+// contraction, bit-exact with the oracle) and fp64_fma (contracted).
+#define PSUM_FP64_LAUNCHERS                                                                                      \
+    void launch_push64(const Push64Args& a, long long n_upper, cudaStream_t s);                                   \
+    long long push64_blocks(long long n_upper); /* grid size of launch_push64 */                                  \
+    void launch_deposit64(const Deposit64Args& a, long long n_upper, cudaStream_t s);                             \
+    void launch_keys64(const GridView& g, double* const pos[3], int* key, const long long* count, long long n_upper, \
+                       cudaStream_t s);
+namespace fp64_exact {
+PSUM_FP64_LAUNCHERS
+}
+namespace fp64_fma {
+PSUM_FP64_LAUNCHERS
+}
+#undef PSUM_FP64_LAUNCHERS
 
 }  // namespace psum_b200

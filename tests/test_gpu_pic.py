@@ -41,6 +41,12 @@ def make_case(kind, precision, seed=0, n=20000):
     elif kind == "2d_mixed_bc":
         cells, lo, hi, per = (20, 16), (0.0, -2.0), (5.0, 2.0), (0, 1)
         plo, phi_ = (0.0, -2.0), (5.0, 2.0 + 4.0 / 16)
+    elif kind == "1d_periodic":   # TSI idiom: lower bound dx/2, 63 cells, 64 wrapping nodes
+        cells, lo, hi, per = (63,), (0.5,), (63.5,), (1,)
+        plo, phi_ = (0.0,), (64.0,)
+    elif kind == "1d_absorb":
+        cells, lo, hi, per = (64,), (0.0,), (64.0,), (0,)
+        plo, phi_ = lo, hi
     elif kind == "3d_large":   # 172^3 wrapping cells: more than 4M cells
         cells, lo, hi, per = (171, 171, 171), (0.5,) * 3, (171.5,) * 3, (1, 1, 1)
         plo, phi_ = (0.0,) * 3, (172.0,) * 3
@@ -771,3 +777,93 @@ def test_step_diagnostics_equal_separate_diagnostics(path, kind):
         assert got["charge"] == before["charge"]
     phases = ctx.get_timing(reset=True)
     assert phases["diag"][1] == 3 and phases["push"][1] == 3
+
+
+
+@pytest.mark.parametrize("kind", ["1d_periodic", "1d_absorb"])
+@pytest.mark.parametrize("pusher", [P.LEAPFROG, P.BORIS])
+def test_1d_fp64_push_bit_exact(kind, pusher):
+    """1-D runs (TSI and sheath are 1-D: application/benchmark/TSI/main.cpp:94): the FP64 push is bit-exact with
+    the oracle, with the same loss counts."""
+    ctx, g, pos, vel, phi = make_case(kind, P.FP64, seed=61)
+    pos = wrap_into(pos, g)
+    B = (0.3, -0.2, 0.5)
+    sp = ctx.add_species(-1.0, 1.0, 1.0, pos.shape[1])
+    ctx.load(sp, pos, vel)
+    ctx.push(dev(phi), 0.2, pusher, B)
+    got_pos, got_vel = ctx.get_state(sp)
+    exp_pos, exp_vel, exp_loss = O.push(g, pos, vel, phi, -1.0, 0.2, pusher, B)
+    assert np.array_equal(np.isnan(got_pos[0]), np.isnan(exp_pos[0]))
+    alive = ~np.isnan(exp_pos[0])
+    assert (got_pos[:, alive].view(np.int64) == exp_pos[:, alive].view(np.int64)).all()
+    assert (got_vel.view(np.int64) == exp_vel.view(np.int64)).all()
+    assert (ctx.losses()[0] == exp_loss).all()
+
+
+@pytest.mark.parametrize("kind", ["1d_periodic", "1d_absorb"])
+def test_1d_mixed_push_and_deposit_within_tolerance(kind):
+    """1-D mixed precision: one push from the same state within 2e-6 cells / 2e-5 in velocity of the FP64
+    oracle, and the exact integer deposit within 2e-6 of the oracle's."""
+    ctx, g, pos, vel, phi = make_case(kind, P.MIXED, seed=62)
+    pos = wrap_into(pos, g)
+    sp = ctx.add_species(-1.0, 1.0, 1.0, pos.shape[1])
+    ctx.load(sp, pos, vel)
+    pos0, vel0 = ctx.get_state(sp)
+    ctx.deposit()
+    dens = dev(np.zeros(ctx.n_nodes))
+    ctx.density(sp, dens)
+    exp_rho = O.deposit(g, pos0, 1.0, ctx.n_nodes)
+    assert np.abs(dens.cpu().numpy() - exp_rho).max() <= 2e-6 * np.abs(exp_rho).max()
+    ctx.push(dev(phi), 0.2)
+    got_pos, got_vel = ctx.get_state(sp)
+    exp_pos, exp_vel, _ = O.push(g, pos0, vel0, phi, -1.0, 0.2)
+    ok = ~np.isnan(exp_pos[0]) & ~np.isnan(got_pos[0])
+    d = got_pos[0, ok] - exp_pos[0, ok]
+    if g.periodic[0]:
+        L = (g.cells[0] + 1) * (g.upper[0] - g.lower[0]) / g.cells[0]
+        d = (d + L / 2) % L - L / 2
+    assert np.abs(d).max() < 2e-6
+    assert np.abs(got_vel[:, ok] - exp_vel[:, ok]).max() < 2e-5
+    amb = (np.abs(exp_pos[0] - g.lower[0]) < 1e-5) | (np.abs(exp_pos[0] - g.upper[0]) < 1e-5)
+    assert (np.isnan(exp_pos[0])[~amb] == np.isnan(got_pos[0])[~amb]).all()
+
+
+def test_1d_two_stream_steps_through_the_1d_solver():
+    """A 1-D two-stream run as TSI sets it up (grounded node, uniform background, two counter-streaming beams),
+    stepped through psum_pic_step with the 1-D frontend's multigrid backend: the mixed run's potential stays
+    within 1e-5 (relative L2) of the FP64 run's over 10 steps, and the state stays sorted by cell."""
+    cells = 255
+    grid = P.simple_grid((0.5,), (cells + 0.5,), (cells,))
+    n = 64 * (cells + 1)
+    rng = np.random.default_rng(63)
+    L = cells + 1.0
+    pos = np.mod(rng.uniform(0.0, L, (1, n)), L) + 0.5
+    vel = rng.normal(0.0, 0.05, (3, n))
+    vel[0] += np.where(np.arange(n) % 2 == 0, 0.4, -0.4)
+    phis = {}
+    for prec in (P.MIXED, P.FP64):
+        ctx = P.ParticleContext((cells,), (0.5,), (cells + 0.5,), (1,), prec)
+        ctx.set_options("diagnostics 1")
+        e = ctx.add_species(-1.0, 1.0, L / n, n)
+        ctx.load(e, pos, vel)
+        ctx.sort()
+        ctx.deposit()
+        ps = P.Poisson_solver_1d()
+        ps.set_options(f"I {cells + 1} J 1 K 1 depth 5 pre_relax 2 post_relax 2 max_cycles 200 correction_interval 4 "
+                       f"tol 1e-12 periodic_I 1")
+        backend = "cuda_multigrid32f_gpu" if prec == P.MIXED else "cuda_multigrid64_gpu"
+        ps.init(backend, grid, [P.Dirichlet_point(grid, "L", 0.0)], 1.0)
+        ps.make_righthand_item()
+        rho = dev(np.zeros(cells + 1))
+        phi = dev(np.zeros(cells + 1))
+        for _ in range(10):
+            ctx.step(ps.backend, 1.0, rho, phi, 0.1)
+        k = torch.zeros(ctx.count(e)[0], dtype=torch.int32, device="cuda")
+        ctx.sort()
+        ctx.get_keys(e, k)
+        assert (np.diff(k.cpu().numpy()) >= 0).all()
+        diag = ctx.step_diagnostics(1.0)
+        assert np.isfinite(diag["kinetic"]).all() and diag["field"] > 0
+        phis[prec] = phi.cpu().numpy()
+    err = np.linalg.norm(phis[P.MIXED] - phis[P.FP64]) / np.linalg.norm(phis[P.FP64])
+    assert err < 1e-5, err

@@ -351,3 +351,111 @@ def test_mixed_boundaries_multigrid_matches_direct(kind):
         ref = direct_solve(g, domain, fixed, mixed, rho, eps)
         got = phi.cpu().numpy()
         assert np.linalg.norm(got - ref) <= 1e-7 * np.linalg.norm(ref), ps.backend.last_stats()
+
+
+@pytest.mark.parametrize("kind", ["cuda_multigrid64_gpu", "cuda_multigrid32f_gpu"])
+def test_mixed_boundaries_3d_multigrid_matches_direct(kind):
+    """The 3-D frontend with Neumann and Robin planes (Poisson_solver_3d.hpp:178-349) and with an epsilon function:
+    both multigrid backends reach the host direct solution of the same system on the GPU."""
+    from test_mixed_boundaries_3d import direct_solve, exact, grad, laplacian, node_xyz
+    N = 24
+    g = P.simple_grid((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), (N, N, N))
+    x, y, z = node_xyz(g)
+    a, bcoef = 1.5, 0.75
+    mixed = [P.Neumann_plane(g, "Xpos", lambda x, y, z: grad(x, y, z)[0]),
+             P.Neumann_plane(g, "Yneg", lambda x, y, z: -grad(x, y, z)[1]),
+             P.Neumann_plane(g, "Ypos", lambda x, y, z: grad(x, y, z)[1]),
+             P.Neumann_plane(g, "Zneg", lambda x, y, z: -grad(x, y, z)[2]),
+             P.Robin_plane(g, "Zpos", (a, bcoef), lambda x, y, z: a * exact(x, y, z) + bcoef * grad(x, y, z)[2])]
+    fx = P.Dirichlet_plane(g, "Xneg", 0.0)[0]
+    fi = fx.astype(np.int64)
+    cases = [(1.0, [(fx, exact(x[fi], y[fi], z[fi]))], mixed),
+             (lambda x, y, z: 1 + 0.5 * x + 0.25 * y * z, [(fx, exact(x[fi], y[fi], z[fi]))], mixed[1:])]
+    for eps, fixed, mb in cases:
+        rho = -laplacian(x, y, z)
+        ps = P.Poisson_solver_3d()
+        ps.set_options(f"I {N + 1} J {N + 1} K {N + 1} depth 3 pre_relax 2 post_relax 2 max_cycles 400 "
+                       f"correction_interval 4 tol 1e-10")
+        ps.init(kind, g, ps.Cartesian, fixed, eps, mixed_boundaries=mb)
+        phi, b = dev(np.zeros(g.n_nodes)), dev(rho)
+        code = ps.solve(phi, b)
+        assert code == 0, ps.backend.last_stats()
+        ref = direct_solve(g, fixed, mb, rho, eps=eps)
+        got = phi.cpu().numpy()
+        assert np.linalg.norm(got - ref) <= 1e-8 * np.linalg.norm(ref), ps.backend.last_stats()
+
+
+@pytest.mark.parametrize("kind", ["cuda_multigrid64_gpu", "cuda_multigrid32f_gpu"])
+def test_1d_operators_multigrid_match_direct(kind):
+    """PSuM's 1-D frontend (Poisson_solver_1d.hpp:126-222): grounded ends, a Neumann end and a Robin end with a
+    variable epsilon, solved by both multigrid backends on the GPU (I = cells + 1, J = K = 1) against the host
+    direct solution of the same system."""
+    from test_psolver_1d import EPS0, system, xs
+    g = P.simple_grid((0.0,), (1.0,), (256,))
+    x = xs(g)
+    rho = -EPS0 * (-np.pi ** 2 * np.sin(np.pi * x))
+    setups = [([P.Dirichlet_point(g, "L", 0.0), P.Dirichlet_point(g, "R", 0.0)], [], EPS0),
+              ([P.Dirichlet_point(g, "L", 0.5)], [P.Neumann_point(g, "R", 0.3)], EPS0),
+              ([P.Dirichlet_point(g, "L", 0.0)], [P.Robin_point(g, "R", (2.0, 0.5), 1.0)],
+               lambda x: EPS0 * (1.0 + 0.5 * x))]
+    for fixed, mixed, eps in setups:
+        A, b, _ = system(g, fixed, mixed, rho, eps)
+        ref = spl.spsolve(A.tocsc(), b)
+        ps = P.Poisson_solver_1d()
+        # the FP64 V-cycles level off near a relative residual of 4e-11 on these systems: stop at 1e-9
+        ps.set_options(f"I {g.n_nodes} J 1 K 1 depth 4 pre_relax 2 post_relax 2 max_cycles 1000 "
+                       f"correction_interval 4 tol 1e-9")
+        ps.init(kind, g, fixed, eps, mixed_boundaries=mixed)
+        phi, bd = dev(np.zeros(g.n_nodes)), dev(rho)
+        code = ps.solve(phi, bd)
+        assert code == 0, ps.backend.last_stats()
+        got = phi.cpu().numpy()
+        assert np.abs(got - ref).max() <= 1e-7 * np.abs(ref).max(), ps.backend.last_stats()
+
+
+@pytest.mark.parametrize("kind", ["cuda_multigrid64_gpu", "cuda_multigrid32f_gpu"])
+@pytest.mark.parametrize("case", ["2d_1025", "2d_257", "3d_periodic_128", "3d_odd_65x70x90"])
+def test_tma_staged_sweeps_equal_per_row_sweeps(kind, case):
+    """Levels of 2^16 rows and more are swept by the TMA-staged kernel (row segments by cp.async.bulk into shared
+    memory); option `tma 0` keeps the per-row kernel.  Same taps in the same order: the iterates are identical."""
+    if case.startswith("2d"):
+        N = 1024 if case == "2d_1025" else 256
+        g, fixed, r, c, v, n, b = dirichlet_case(N, seed=7)
+        opts = f"I {N + 1} J {N + 1} K 1 depth 4 pre_relax 2 post_relax 2 max_cycles 6 correction_interval 2"
+    elif case == "3d_periodic_128":
+        g, r, c, v, n, b = periodic_case(3, 128, seed=8)
+        opts = ("I 128 J 128 K 128 depth 4 pre_relax 2 post_relax 2 max_cycles 4 correction_interval 2 "
+                "periodic_I 1 periodic_J 1 periodic_K 1")
+    else:   # an odd box with Dirichlet faces: exception rows, rows of any pitch, partial tiles
+        g = P.simple_grid((0, 0, 0), (1, 1.1, 1.3), (64, 69, 89))
+        fixed = np.unique(np.concatenate([P.Dirichlet_plane(g, d, 0)[0] for d in ("Xneg", "Ypos", "Zneg")]))
+        r, c, v = P.assemble_poisson(g, fixed, 1.0)
+        n = g.n_nodes
+        b = np.random.default_rng(9).normal(size=n)
+        b[fixed.astype(np.int64)] = 0.0
+        opts = "I 65 J 70 K 90 depth 3 pre_relax 2 post_relax 1 max_cycles 4 correction_interval 2"
+    x0 = np.random.default_rng(10).normal(size=n) * 0.1
+    outs = []
+    for tma in (1, 0):
+        s = P.solver_backend(kind)
+        s.set_options(f"{opts} tma {tma}")
+        s.set_matrix(n, n, r.size, r, c, v)
+        bd, xd = dev(b), dev(x0)
+        assert s.solve(bd, xd) in (0, 4)   # fixed cycle count, no tol: never a stall
+        outs.append(xd.cpu().numpy())
+    assert (outs[0].view(np.int64) == outs[1].view(np.int64)).all()
+
+
+def test_tma_staged_fp64_vcycles_match_oracle():
+    """The FP64 V-cycles on a 257^2 box (TMA-staged sweeps on the finest level) still equal the oracle's."""
+    N, depth, cycles = 256, 4, 3
+    g, fixed, r, c, v, n, b = dirichlet_case(N, seed=11)
+    s = P.solver_backend("cuda_multigrid64_gpu")
+    s.set_options(f"I {N + 1} J {N + 1} K 1 depth {depth} pre_relax 2 post_relax 2 max_cycles {cycles}")
+    s.set_matrix(n, n, r.size, r, c, v)
+    x0 = np.random.default_rng(12).normal(size=n) * 0.1
+    bd, xd = dev(b), dev(x0)
+    s.solve(bd, xd)
+    mg = O.Multigrid(r, c, v, n, N + 1, N + 1, 1, depth)
+    ref = mg.vcycles(b, x0, cycles, 2, 2)
+    assert np.linalg.norm(xd.cpu().numpy() - ref) / np.linalg.norm(ref) < 1e-12
