@@ -17,6 +17,7 @@
 #include <string>
 #include <vector>
 
+#include "../../include/psum_interp.h"
 #include "../../include/psum_pic.h"
 #include "common.hpp"
 #include "mg_backend.hpp"
@@ -1157,6 +1158,90 @@ __global__ void k_fill_keys(const unsigned* __restrict__ starts, long long n_cel
     for (unsigned i = starts[c] + (threadIdx.x & 31); i < e; i += 32) key[i] = (int)c;
 }
 
+// ------------------------------------------ B-spline step (interp_order) --
+// FP64 positions pos[d*n_upper + i] of the stored particles (NaN x for
+// invalid entries and for i >= the device count), from the mixed state
+// (cell + offset) or the FP64 state: the input of the B-spline deposit and
+// gather of a step with interp_order 2-4.
+__global__ void k_state_positions(GridView g, int mixed, const int* __restrict__ key, const float* __restrict__ o0,
+                                  const float* __restrict__ o1, const float* __restrict__ o2,
+                                  const double* __restrict__ q0, const double* __restrict__ q1,
+                                  const double* __restrict__ q2, const long long* __restrict__ count,
+                                  long long n_upper, double* __restrict__ out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_upper) return;
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    double p[3] = {nan, 0.0, 0.0};
+    if (i < *count) {
+        if (mixed) {
+            const int k = key[i];
+            if (k >= 0) {
+                int c[3];
+                key_to_cell(g, k, c[0], c[1], c[2]);
+                const float* off[3] = {o0, o1, o2};
+                for (int a = 0; a < g.dim; ++a) p[a] = g.lo[a] + ((double)c[a] + (double)off[a][i]) * g.dx[a];
+            }
+        } else {
+            const double* q[3] = {q0, q1, q2};
+            for (int a = 0; a < g.dim; ++a) p[a] = q[a][i];
+        }
+    }
+    for (int a = 0; a < g.dim; ++a) out[(long long)a * n_upper + i] = p[a];
+}
+
+// Mixed push with the field's gradient gathered by the caller (grad[d*n_upper + i],
+// per unit length): the scaled gradient of the kick is gs_a * grad_a * dx_a, then
+// the same kick, move and boundary as every mixed push; no deposit (the next
+// step's charge density is the B-spline deposit of the new positions).
+template <int D, int PUSHER>
+__global__ void __launch_bounds__(kPicThreads) k_push_grad_mixed(PushArgs a, const double* __restrict__ grad,
+                                                                 long long n_upper) {
+    const long long count = *a.count;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int lost = -1;
+    double kin = 0.0;
+    if (i < count && i < n_upper) {
+        const int k = a.key[i];
+        if (k >= 0) {
+            int c[3];
+            key_to_cell(a.g, k, c[0], c[1], c[2]);
+            float f[3] = {0.f, 0.f, 0.f}, v[3];
+            for (int d = 0; d < D; ++d) f[d] = a.off[d][i];
+            for (int q = 0; q < 3; ++q) v[q] = a.vel[q][i];
+            float G[3] = {0.f, 0.f, 0.f};
+            for (int d = 0; d < D; ++d) G[d] = (float)((double)a.gs[d] * grad[(long long)d * n_upper + i] * a.g.dx[d]);
+            kick<D, PUSHER>(a, G, v);
+            int dc[3] = {0, 0, 0};
+            int nk = -1;
+            if (!move<D>(a, v, f, dc)) {
+                atomicOr(a.err, kErrNonFinite);
+            } else {
+                lost = apply_step<D>(a.g, c, dc);
+                if (lost < 0) nk = cell_to_key(a.g, c[0], c[1], c[2]);
+            }
+            a.key[i] = nk;
+            for (int d = 0; d < D; ++d) a.off[d][i] = nk >= 0 ? f[d] : 0.f;
+            for (int q = 0; q < 3; ++q) a.vel[q][i] = v[q];
+            if (a.kin_part && nk >= 0) kin += a.kin_hmw * kinetic_v2(v);
+        }
+    }
+    warp_count_losses(a.losses, D, lost);
+    if (a.kin_part) block_sum_to(kin, a.kin_part);
+}
+
+// rho = background before the B-spline deposits add to it
+__global__ void k_fill(double* __restrict__ v, long long n, double value) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = value;
+}
+
+// per-block sums of rho - background (the charge of a B-spline step's density)
+__global__ void __launch_bounds__(256) k_rho_charge(const double* __restrict__ rho, long long n, double background,
+                                                   double* __restrict__ part) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    block_sum_to(i < n ? rho[i] - background : 0.0, part);
+}
+
 // ------------------------------------------------------- load / export --
 __global__ void k_load_mixed(GridView g, long long n, const double* __restrict__ pos, const double* __restrict__ vel,
                              int* __restrict__ key, float* __restrict__ o0, float* __restrict__ o1,
@@ -1645,6 +1730,9 @@ struct DiagFinishArgs {
     long long kin_n[8];
     const unsigned long long* qsum;
     double q_coef[8];               // q * w * 2^-dep_shift per species
+    const double* rho_part;         // B-spline steps: per-block sums of rho - background (else null)
+    long long rho_n;
+    double rho_coef;                // cell volume
     int ns;
     double* out;
 };
@@ -1685,6 +1773,10 @@ __global__ void __launch_bounds__(kDiagFinishThreads) k_diag_finish(DiagFinishAr
         double q = 0.0;
         for (int s = 0; s < a.ns; ++s) q += a.q_coef[s] * (double)(long long)a.qsum[s];
         a.out[a.ns + 1] = q;
+    }
+    if (a.rho_part) {
+        const double q = block_fixed_sum(a.rho_part, a.rho_n);
+        if (threadIdx.x == 0) a.out[a.ns + 1] = q * a.rho_coef;
     }
 }
 
@@ -2270,12 +2362,14 @@ static void ensure_diag_buffers(psum_pic_ctx* c) {
         d.kin_off[s] = off;
         d.kin_n[s] = 0;
         off += std::max({cls_blocks2(n, c->g.n_cells, c->g.dim), (long long)capped_blocks(4LL * kPicThreads, n),
-                         fp64_exact::push64_blocks(n)});
+                         fp64_exact::push64_blocks(n), (long long)blocks_for(n, kPicThreads)});
     }
     grow(d.kin, (size_t)std::max<long long>(off, 1));
     grow(d.qsum, 8);
     grow(c->diag_out, 16);
     d.fe_n = 0;
+    d.rho_n = 0;
+    cuda_check(cudaMemsetAsync(d.qsum.p, 0, sizeof(unsigned long long) * 8, c->stream), "memset qsum");
 }
 
 // Reduces the step's partial sums into diag_out (context stream, after the push).
@@ -2295,9 +2389,106 @@ static void finish_diagnostics(psum_pic_ctx* c, int par) {
         a.q_coef[s] = sp.q * sp.w * std::ldexp(1.0, -sp.dep_shift);
     }
     a.qsum = d.qsum.p;
+    a.rho_part = d.rho_n ? d.rho_part.p : nullptr;
+    a.rho_n = d.rho_n;
+    a.rho_coef = vol;
     a.out = c->diag_out.p;
     { k_diag_finish<<<1, kDiagFinishThreads, 0, c->stream>>>(a); count_launch(); }
     cuda_check(cudaGetLastError(), "diagnostics launch");
+}
+
+// Charge density of a step with interp_order > 1: rho = background plus the
+// B-spline deposit (add_back_B_spline, higher_order_interp.hpp:196-247) of
+// every species' current positions, exported to bs_pos (kept for the push).
+static void rho_bspline(psum_pic_ctx* c, double background, double* rho) {
+    cudaStream_t s = c->stream;
+    const long long nn = c->g.n_nodes;
+    { k_fill<<<blocks_for(nn, 256), 256, 0, s>>>(rho, nn, background); count_launch(); }
+    grow(c->bs_acc, (size_t)nn);
+    double vol = 1.0;
+    for (int d = 0; d < c->g.dim; ++d) vol *= c->g.dx[d];
+    for (int si = 0; si < (int)c->sp.size(); ++si) {
+        Species& sp = *c->sp[si];
+        if (sp.n <= 0) continue;
+        if (si >= 8) throw Error(PSUM_ERR_INVALID_ARGUMENT, "interp_order: more than 8 species");
+        if (c->precision == PSUM_PIC_MIXED) ensure_keys(c, sp);
+        grow(c->bs_pos[si], (size_t)sp.n * c->g.dim);
+        const int cur = sp.cur;
+        const bool mixed = c->precision == PSUM_PIC_MIXED;
+        { k_state_positions<<<blocks_for(sp.n, 256), 256, 0, s>>>(
+              c->g, mixed ? 1 : 0, mixed ? sp.key[cur].p : nullptr, mixed ? sp.off[0][cur].p : nullptr,
+              mixed && c->g.dim > 1 ? sp.off[1][cur].p : nullptr, mixed && c->g.dim > 2 ? sp.off[2][cur].p : nullptr,
+              mixed ? nullptr : sp.pos64[0][cur].p, !mixed && c->g.dim > 1 ? sp.pos64[1][cur].p : nullptr,
+              !mixed && c->g.dim > 2 ? sp.pos64[2][cur].p : nullptr, c->count.p + si, sp.n, c->bs_pos[si].p); count_launch(); }
+        const int st = psum_add_back_bspline(&c->desc, c->interp_order, (unsigned long long)sp.n, c->bs_pos[si].p,
+                                             sp.q * sp.w / vol, rho, c->bs_acc.p, nullptr, s);
+        if (st != PSUM_OK) throw Error(st, "interp_order: B-spline deposit failed");
+    }
+    if (c->diag_in_step) {   // the charge of this density, for the step's diagnostics
+        auto& d = c->dbuf[c->diag_par];
+        const long long nb = blocks_for(nn, 256);
+        grow(d.rho_part, (size_t)nb);
+        d.rho_n = nb;
+        { k_rho_charge<<<(unsigned)nb, 256, 0, s>>>(rho, nn, background, d.rho_part.p); count_launch(); }
+    }
+    cuda_check(cudaGetLastError(), "rho_bspline launch");
+}
+
+// Push of a step with interp_order > 1: the B-spline gradient gather
+// (interp_diff_B_spline) of phi at the positions rho_bspline exported, then
+// the push with that field (no CIC gather, no deposit) in place.
+static void push_bspline(psum_pic_ctx* c, const double* phi, double dt, int pusher, const double* B) {
+    if (!(std::isfinite(dt))) throw Error(PSUM_ERR_NONFINITE, "push: non-finite dt");
+    cudaStream_t s = c->stream;
+    launch_edges(c, phi, s);   // field-energy sums of a step with diagnostics
+    for (int si = 0; si < (int)c->sp.size(); ++si) {
+        Species& sp = *c->sp[si];
+        if (sp.n <= 0) continue;
+        sp.sorted = false;
+        grow(c->bs_grad, (size_t)sp.n * c->g.dim);
+        const int st = psum_interp_diff_bspline(&c->desc, c->interp_order, (unsigned long long)sp.n,
+                                                c->bs_pos[si].p, phi, c->bs_grad.p, nullptr, s);
+        if (st != PSUM_OK) throw Error(st, "interp_order: B-spline gather failed");
+        if (c->precision == PSUM_PIC_MIXED) {
+            PushArgs a = make_push_args(c, sp, si, dt, pusher, B);
+            a.acc = nullptr;
+            const unsigned nb = blocks_for(sp.n, kPicThreads);
+            a.kin_part = kin_slot(c, si, nb);
+            const int D = c->g.dim;
+            const bool boris = pusher == PSUM_PIC_BORIS;
+#define PSUM_PG(DD, PP) k_push_grad_mixed<DD, PP><<<nb, kPicThreads, 0, s>>>(a, c->bs_grad.p, sp.n)
+            if (D == 1) { if (boris) PSUM_PG(1, PSUM_PIC_BORIS); else PSUM_PG(1, PSUM_PIC_LEAPFROG); }
+            else if (D == 2) { if (boris) PSUM_PG(2, PSUM_PIC_BORIS); else PSUM_PG(2, PSUM_PIC_LEAPFROG); }
+            else { if (boris) PSUM_PG(3, PSUM_PIC_BORIS); else PSUM_PG(3, PSUM_PIC_LEAPFROG); }
+#undef PSUM_PG
+            count_launch();
+        } else {
+            Push64Args a{};
+            a.g = c->g;
+            for (int d = 0; d < 3; ++d) {
+                a.hi[d] = c->g.lo[d] + c->g.cells[d] * c->g.dx[d];
+                a.pos[d] = d < c->g.dim ? sp.pos64[d][sp.cur].p : nullptr;
+                a.vel[d] = sp.vel64[d][sp.cur].p;
+                a.B[d] = B ? B[d] : 0.0;
+            }
+            a.key = sp.key[sp.cur].p;
+            a.count = c->count.p + si;
+            a.phi = phi;
+            a.q_m = sp.q / sp.m;
+            a.dt = dt;
+            a.pusher = pusher;
+            a.acc = nullptr;
+            a.scale = 0.0;
+            a.losses = c->losses.p + (size_t)si * 6;
+            a.err = c->err.p;
+            a.kin_part = kin_slot(c, si, fp64_exact::push64_blocks(sp.n));
+            a.kin_hmw = 0.5 * sp.m * sp.w;
+            a.grad = c->bs_grad.p;
+            a.grad_stride = sp.n;
+            push64(c, a, sp.n, s);
+        }
+    }
+    cuda_check(cudaGetLastError(), "push_bspline launch");
 }
 
 }  // namespace psum_b200
@@ -2315,6 +2506,7 @@ EXPORT int psum_pic_create(const psum_pic_grid_desc* gd, int precision, psum_pic
         if (precision != PSUM_PIC_MIXED && precision != PSUM_PIC_FP64)
             throw std::invalid_argument("psum_pic_create: unknown precision");
         auto c = std::make_unique<psum_pic_ctx>();
+        c->desc = *gd;
         GridView& g = c->g;
         g.dim = gd->dim;
         long long nn = 1, nc = 1;
@@ -2395,6 +2587,9 @@ EXPORT int psum_pic_set_options(psum_pic_ctx* ctx, const char* options) {
             if (key == "sort_interval") {
                 if (v < 0) throw std::invalid_argument("sort_interval must be >= 0");
                 ctx->sort_interval = v;
+            } else if (key == "interp_order") {
+                if (v < 1 || v > 4) throw std::invalid_argument("interp_order must be 1, 2, 3 or 4");
+                ctx->interp_order = v;
             } else if (key == "fp64_fma") {
                 if (v != 0 && v != 1) throw std::invalid_argument("fp64_fma must be 0 or 1");
                 ctx->fp64_fma = v != 0;
@@ -2875,7 +3070,8 @@ EXPORT int psum_pic_step(psum_pic_ctx* ctx, psum_field_solver_handle solver, dou
         try {
             {
                 PhaseTimer t(ctx, 0);
-                rho_into(ctx, background, rho_dev, -1, true);
+                if (ctx->interp_order > 1) rho_bspline(ctx, background, rho_dev);
+                else rho_into(ctx, background, rho_dev, -1, true);
                 t.stop();
             }
             {
@@ -2891,7 +3087,8 @@ EXPORT int psum_pic_step(psum_pic_ctx* ctx, psum_field_solver_handle solver, dou
         cuda_check(cudaEventRecord(ctx->ev_out, ctx->prio), "cudaEventRecord");
         cuda_check(cudaStreamWaitEvent(user, ctx->ev_out, 0), "cudaStreamWaitEvent");
         finish_cls_step(ctx);
-        bool fused = ctx->precision == PSUM_PIC_MIXED && ctx->sort_interval == 1 && cls_step_applies(ctx);
+        bool fused = ctx->precision == PSUM_PIC_MIXED && ctx->sort_interval == 1 && cls_step_applies(ctx) &&
+                     ctx->interp_order == 1;
         for (auto& sp : ctx->sp) fused = fused && (sp->sorted || sp->n == 0);
         if (pusher != PSUM_PIC_LEAPFROG && pusher != PSUM_PIC_BORIS) throw std::invalid_argument("step: unknown pusher");
         if (fused) {
@@ -2901,7 +3098,8 @@ EXPORT int psum_pic_step(psum_pic_ctx* ctx, psum_field_solver_handle solver, dou
         } else {
             {
                 PhaseTimer t(ctx, 2);
-                push_all(ctx, phi_dev, dt, pusher, B);
+                if (ctx->interp_order > 1) push_bspline(ctx, phi_dev, dt, pusher, B);
+                else push_all(ctx, phi_dev, dt, pusher, B);
                 t.stop();
             }
             ctx->steps++;

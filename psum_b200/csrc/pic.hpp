@@ -50,6 +50,7 @@ struct SortScratch {
 struct psum_pic_ctx {
     uint32_t magic = psum_b200::kPicMagic;
     psum_b200::GridView g{};
+    psum_pic_grid_desc desc{};           // the grid as created (for the B-spline entry points)
     int precision = 0;
     cudaStream_t stream = nullptr;       // active stream
     cudaStream_t own_stream = nullptr;
@@ -85,6 +86,12 @@ struct psum_pic_ctx {
     double pend_B[3] = {0, 0, 0};
     int sort_interval = 1;
     bool fp64_fma = false;                    // FP64 mode: the contracted kernel build (not bit-exact)
+    // option "interp_order k" (2-4): the step deposits and gathers with PSuM's B-spline weights of order k
+    // (positions exported to bs_pos per species, the gathered gradient in bs_grad, deposit scratch bs_acc)
+    int interp_order = 1;
+    psum_b200::DevBuf<double> bs_pos[8];
+    psum_b200::DevBuf<double> bs_grad;
+    psum_b200::DevBuf<unsigned long long> bs_acc;
     // per-step diagnostics (option "diagnostics 1"): partial sums written by the
     // step's own kernels (field energy by k_edges, kinetic energy by the push,
     // charge by k_rho), reduced by k_diag_finish into diag_out
@@ -93,6 +100,8 @@ struct psum_pic_ctx {
     struct DiagBufs {
         psum_b200::DevBuf<double> fe, kin;
         psum_b200::DevBuf<unsigned long long> qsum;
+        psum_b200::DevBuf<double> rho_part;   // B-spline steps: per-block sums of rho - background
+        long long rho_n = 0;
         long long fe_n = 0;
         long long kin_n[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         long long kin_off[8] = {0, 0, 0, 0, 0, 0, 0, 0};

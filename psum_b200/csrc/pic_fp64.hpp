@@ -26,6 +26,9 @@ struct Push64Args {
     unsigned* err;
     double* kin_part;   // per-block kinetic energy of the surviving particles (null: not summed)
     double kin_hmw;     // m * w / 2
+    const double* grad; // non-null: the field's gradient at each particle, grad[d*n_upper + i] (the B-spline
+                        // gather of a step with interp_order > 1), used instead of the CIC gather of phi
+    long long grad_stride;
 };
 
 struct Deposit64Args {

@@ -127,16 +127,20 @@ __global__ void __launch_bounds__(kPicThreads) k_push64(Push64Args a) {
         int lost = -1;
         if (alive) {
             for (int d = 1; d < D; ++d) p[d] = a.pos[d][i];
-            long long idx[8];
-            double dcoef[3][8];
-            cic64(g, p, idx, nullptr, dcoef);
             double E[3] = {0, 0, 0};
-            const int cnt = 1 << D;
-            for (int d = 0; d < D; ++d) {
-                double res = 0;
-                for (int k = 0; k < cnt; ++k)
-                    if (fabs(dcoef[d][k]) > 1e-10) res += a.phi[idx[k]] * dcoef[d][k];
-                E[d] = -res;
+            if (a.grad) {   // gathered by the caller (B-spline orders 2-4)
+                for (int d = 0; d < D; ++d) E[d] = -a.grad[d * a.grad_stride + i];
+            } else {
+                long long idx[8];
+                double dcoef[3][8];
+                cic64(g, p, idx, nullptr, dcoef);
+                const int cnt = 1 << D;
+                for (int d = 0; d < D; ++d) {
+                    double res = 0;
+                    for (int k = 0; k < cnt; ++k)
+                        if (fabs(dcoef[d][k]) > 1e-10) res += a.phi[idx[k]] * dcoef[d][k];
+                    E[d] = -res;
+                }
             }
             double v[3] = {a.vel[0][i], a.vel[1][i], a.vel[2][i]};
             if (a.pusher == 0) {

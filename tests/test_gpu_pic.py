@@ -867,3 +867,62 @@ def test_1d_two_stream_steps_through_the_1d_solver():
         phis[prec] = phi.cpu().numpy()
     err = np.linalg.norm(phis[P.MIXED] - phis[P.FP64]) / np.linalg.norm(phis[P.FP64])
     assert err < 1e-5, err
+
+
+def _bspline_step_expected(g, order, pos0, vel0, phi, qm, dt, w_vol, background, nn):
+    """One step with B-spline order `order`: rho = background + add_back_B_spline of the current positions,
+    then E = -interp_diff_B_spline(phi) at them, leapfrog v += (q/m) E dt, x += v dt, periodic wrap (the oracle's
+    B-spline restatement, simple_interpolation.hpp:105-184, and numpy for the push)."""
+    rho, _ = O.bspline_deposit(g, order, pos0, w_vol, nn)
+    grad = O.bspline_gather(g, order, pos0, phi, grad=True, tol=0.0)
+    v = vel0.copy()
+    for a in range(g.dim):
+        v[a] = v[a] + qm * dt * (-grad[a])
+    p = pos0 + v[:g.dim] * dt
+    for a in range(g.dim):
+        if g.periodic[a]:
+            dx = (g.upper[a] - g.lower[a]) / g.cells[a]
+            L = (g.cells[a] + 1) * dx
+            p[a] = g.lower[a] + np.mod(p[a] - g.lower[a], L)
+    return background + rho, p, v
+
+
+@pytest.mark.parametrize("order", [2, 3, 4])
+@pytest.mark.parametrize("kind", ["1d_periodic", "2d_periodic", "3d_periodic"])
+@pytest.mark.parametrize("precision", [P.FP64, P.MIXED])
+def test_interp_order_step_matches_oracle(order, kind, precision):
+    """Option interp_order (TSI's interp_order for push and deposit, TSI/main.cpp:28-29,
+    higher_order_interp.hpp:196-247): the step's charge density is the B-spline deposit and its push gathers
+    the B-spline gradient.  FP64: density within the deposit's fixed-point bound of the oracle's (per node at
+    most (contributions) * 2^-(F+1) * weight, bounded here by 1e-9 of the density scale), positions and
+    velocities within 1e-12 of the oracle's gather pushed in numpy.  Mixed: within 2e-6 cells and 2e-5 in
+    velocity (the FP32 state)."""
+    ctx, g, pos, vel, phi = make_case(kind, precision, seed=70 + order, n=20000)
+    pos = wrap_into(pos, g)
+    ctx.set_options(f"interp_order {order} sort_interval 0 diagnostics 1")
+    w = 0.37
+    sp = ctx.add_species(-1.0, 1.0, w, pos.shape[1])
+    ctx.load(sp, pos, vel)
+    pos0, vel0 = ctx.get_state(sp)
+    nn = ctx.n_nodes
+    solver = _identity_solver(g, nn)   # max_cycles 0: phi stays the case's field
+    rho = dev(np.zeros(nn))
+    phi_t = dev(phi)
+    vol = np.prod([(g.upper[a] - g.lower[a]) / g.cells[a] for a in range(g.dim)])
+    ctx.step(solver, 0.25, rho, phi_t, 0.1)
+    exp_rho, exp_pos, exp_vel = _bspline_step_expected(g, order, pos0, vel0, phi, -1.0, 0.1, -w / vol, 0.25, nn)
+    got_rho = rho.cpu().numpy()
+    assert np.abs(got_rho - exp_rho).max() <= 1e-9 * np.abs(exp_rho).max()
+    got_pos, got_vel = ctx.get_state(sp)
+    d = got_pos - exp_pos
+    for a in range(g.dim):
+        dx = (g.upper[a] - g.lower[a]) / g.cells[a]
+        L = (g.cells[a] + 1) * dx
+        d[a] = (d[a] + L / 2) % L - L / 2
+    if precision == P.FP64:
+        assert np.abs(d).max() < 1e-12 and np.abs(got_vel - exp_vel).max() < 1e-12
+    else:
+        assert np.abs(d).max() < 2e-6 and np.abs(got_vel - exp_vel).max() < 2e-5
+    diag = ctx.step_diagnostics(1.0)
+    # the density's charge: sum (rho - background) * cell volume = charge of the deposited particles
+    assert abs(diag["charge"] - (-w) * pos.shape[1]) < 1e-6 * w * pos.shape[1]
