@@ -50,7 +50,7 @@ extern "C" {
 #endif
 
 typedef struct psum_pic_grid_desc {
-    int dim;            /* 2 or 3 */
+    int dim;            /* 1, 2 or 3 (1-D runs take the step's general path) */
     int cells[3];       /* simple_grid<D>::cell_num */
     double lower[3];    /* simple_grid<D>::lower_bounds */
     double upper[3];    /* simple_grid<D>::upper_bounds */
@@ -74,7 +74,13 @@ EXPORT int psum_pic_destroy(psum_pic_ctx* ctx);
  * cudaStreamLegacy or a user stream; NULL = the context's own stream). */
 EXPORT int psum_pic_set_stream(psum_pic_ctx* ctx, void* stream);
 /* Options as whitespace `key value` pairs (the solver option grammar):
- *   sort_interval N   re-sort by cell every N steps (default 1; 0 = never) */
+ *   sort_interval N   re-sort by cell every N steps (default 1; 0 = never)
+ *   diagnostics 0|1   sum the energy and charge diagnostics inside every step
+ *                     (psum_pic_get_step_diagnostics; default 0)
+ *   interp_order K    B-spline order of the step's deposit and gather (1 = CIC,
+ *                     the default; 2-4 run the general path, TSI/main.cpp:28-29)
+ *   fp64_fma 0|1      FP64 contexts: the kernel build with fused multiply-adds
+ *                     (faster, not bit-exact with the oracle; default 0) */
 EXPORT int psum_pic_set_options(psum_pic_ctx* ctx, const char* options);
 
 /* Adds a species able to hold `capacity` particles; *id receives its index. */
