@@ -135,24 +135,16 @@ bool launch_level_op_tma(const StencilDev<T>& A, const T* x, const T* b, T* out,
     using S = TmaShape<T>;
     if (Mode == kSmoothFromZero || A.n < kTmaMinRows) return false;
     TmaTile V{};
-    int TR;
-    if (A.n0 > 1 && A.n1 > 1 && A.n2 > 1) {
-        V.P = A.n0; V.R = A.n1; V.C = A.n2;
-        TR = S::TR3;
-        V.chunk = 16;
-    } else if (A.n2 == 1 && A.n0 > 1 && A.n1 > 1) {
-        V.P = 1; V.R = A.n0; V.C = A.n1;
-        TR = S::TR2;
-        V.chunk = 1;
-    } else {
-        return false;
-    }
+    if (!(A.n0 > 2 && A.n1 > 1 && A.n2 > 1)) return false;   // 3-D boxes only (2-D levels stay in L2)
+    V.P = A.n0;
+    V.R = A.n1;
+    V.C = A.n2;
+    V.chunk = 32;
     V.tiles_c = (V.C + S::TC - 1) / S::TC;
-    V.tiles_r = (V.R + TR - 1) / TR;
+    V.tiles_r = (V.R + S::TR - 1) / S::TR;
     V.chunks = (V.P + V.chunk - 1) / V.chunk;
     V.lrow = S::lrow();
-    const int nslots = V.P > 1 ? kTmaSlots : 1;
-    const size_t smem = sizeof(T) * (size_t)nslots * (TR + 2) * V.lrow + sizeof(int) * (size_t)nslots * (TR + 2);
+    const size_t smem = S::smem();
     const unsigned blocks = (unsigned)((long long)V.tiles_c * V.tiles_r * V.chunks);
     if (A.ns == 5) launch_tma_ns<T, Mode, 5>(A, V, smem, blocks, x, b, out, omega, st, stall, s);
     else if (A.ns == 7) launch_tma_ns<T, Mode, 7>(A, V, smem, blocks, x, b, out, omega, st, stall, s);

@@ -149,39 +149,44 @@ __global__ void __launch_bounds__(kThreads) k_level_op(StencilDev<T> A, const T*
 
 // ------------------------------------------------------ TMA-staged sweeps --
 // k_level_op_tma: the same smooth / residual sweep as k_level_op for large
-// levels, with x staged in shared memory by the TMA bulk-copy engine.  The
-// level's node box is viewed as planes x rows x columns (3-D: i, j, k; 2-D:
-// one plane of rows i and columns j).  A block owns a tile of TR rows x TC
-// columns over a chunk of planes and marches along the planes: every row
-// segment of a plane (with one halo row and column on each side) arrives by
-// cp.async.bulk into a ring of four plane slots, completing on the slot's
-// mbarrier; the copy's start is rounded down to 16 bytes, so any row pitch
-// works.  Halo cells across a box face are wrapped like the stencil's own
-// wrap (PSuM's cyclic neighbour rule) and patched from global memory after
-// the plane lands.  Taps are summed in the same order as stencil_row, and
-// exception rows take the same CSR path, so the results are bit-identical
-// to k_level_op.  b is read and out written directly (each once, coalesced).
-// Every mbarrier wait is bounded: after ~2^22 polls the block records a
-// stall in *stall and goes on, so a wrong byte count cannot hang the GPU.
+// 3-D levels, with x staged in shared memory by the TMA bulk-copy engine.
+// The level's node box is viewed as planes (i) x rows (j) x columns (k).  A
+// block owns a tile of TR rows x TC columns over a chunk of planes and
+// marches along the planes: the row segments of a plane (one halo row and
+// column on each side) arrive by cp.async.bulk into a ring of five plane
+// slots, completing on the slot's mbarrier; the copy's start is rounded down
+// to 16 bytes, so any row pitch works, and each row records where its
+// columns begin.  Halo cells across a box face are wrapped like the
+// stencil's own wrap (PSuM's cyclic neighbour rule) and patched from global
+// memory after the plane lands.  Planes p-1, p, p+1 are resident while p is
+// computed and p+2, p+3 are in flight; one block barrier per plane orders
+// the refill of the slot of p-2.  Taps are summed in the same order as
+// stencil_row, and exception rows take the same CSR path, so the results are
+// bit-identical to k_level_op.  b is read and out written directly (each
+// once, coalesced).  Every mbarrier wait is bounded: after 2^16 suspended
+// polls the block records a stall in *stall, and once a stall is recorded
+// later waits return at once, so a wrong byte count cannot hang the GPU.
 struct TmaTile {
-    int P, R, C;          // planes, rows, columns of the view (3-D: n0, n1, n2; 2-D: 1, n0, n1)
+    int P, R, C;          // planes, rows, columns of the view (n0, n1, n2)
     int tiles_c, tiles_r;
     int chunk, chunks;    // planes per block, blocks along the planes
     int lrow;             // shared-memory row stride in elements
 };
 
 constexpr int kTmaThreads = 256;
-constexpr int kTmaSlots = 4;
+constexpr int kTmaSlots = 5;
 
 template <class T>
 struct TmaShape {
     static constexpr int TC = sizeof(T) == 4 ? 128 : 64;   // columns per tile (one 512-byte segment)
-    static constexpr int TR3 = 8;                           // rows per tile, 3-D (marching)
-    static constexpr int TR2 = 32;                          // rows per tile, 2-D (one plane)
+    static constexpr int TR = 16;                           // rows per tile
     static constexpr int kAlign = 16 / (int)sizeof(T);      // elements per 16 bytes
     // row stride: one aligned lead unit, the segment (TC + 2 halo) and the
     // alignment slack of its end, rounded to 16 bytes
     static constexpr int lrow() { return ((kAlign + TC + 2 + 2 * kAlign) + kAlign - 1) / kAlign * kAlign; }
+    static constexpr size_t smem() {
+        return sizeof(T) * (size_t)kTmaSlots * (TR + 2) * lrow() + sizeof(int) * (size_t)kTmaSlots * (TR + 2);
+    }
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -197,28 +202,26 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned
                  : "memory");
 }
 
-// Non-blocking test of phase `parity` of bar.
-__device__ __forceinline__ bool mbar_test_wait(unsigned long long* bar, unsigned parity) {
+// Suspended test of phase `parity` of bar (returns after the phase completes
+// or a hardware time limit).
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
     unsigned ok;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(ok)
         : "r"(smem_u32(bar)), "r"(parity)
         : "memory");
     return ok != 0;
 }
 
-// Bounded wait for phase `parity` of bar: polls with a short sleep for about
-// 2^18 * (poll + 64 ns), a few tens of milliseconds, far above a copy's
-// microseconds.  On expiry it records a stall in *stall and returns; once a
-// stall is recorded (by this block or another) later waits return at once,
-// so a wrong byte count costs one expiry per block, never a hang.
+// Bounded wait for phase `parity` of bar: at most 2^16 suspended polls; on
+// expiry it records a stall in *stall and returns; once a stall is recorded
+// (by this block or another) later waits return at once.
 __device__ __forceinline__ void mbar_wait_bounded(unsigned long long* bar, unsigned parity, int* stall) {
+    if (mbar_try_wait(bar, parity)) return;
     if (*(volatile int*)stall) return;
-    for (int it = 0; it < (1 << 18); ++it) {
-        if (mbar_test_wait(bar, parity)) return;
-        __nanosleep(64);
-    }
+    for (int it = 0; it < (1 << 16); ++it)
+        if (mbar_try_wait(bar, parity)) return;
     atomicExch(stall, 1);
 }
 
@@ -257,17 +260,16 @@ __global__ void __launch_bounds__(kTmaThreads) k_level_op_tma(StencilDev<T> A, T
                                                               const MGState* __restrict__ st, int* stall) {
     using S = TmaShape<T>;
     constexpr int TC = S::TC;
+    constexpr int TR = S::TR;
     constexpr int KA = S::kAlign;
+    constexpr int NSL = kTmaSlots;
     if (st && st->done) return;   // st == nullptr: ungated (inside the device-side loop)
     extern __shared__ __align__(128) unsigned char tma_smem[];
-    __shared__ __align__(8) unsigned long long bar[kTmaSlots];
-    const bool three = V.P > 1;
-    const int TR = three ? S::TR3 : S::TR2;
-    const int nslots = three ? kTmaSlots : 1;
+    __shared__ __align__(8) unsigned long long bar[NSL];
     const int lrow = V.lrow;
     T* const ring = reinterpret_cast<T*>(tma_smem);   // [slot][TR + 2][lrow]
-    int* const leadv = reinterpret_cast<int*>(tma_smem + sizeof(T) * (size_t)nslots * (TR + 2) * lrow);   // [slot][TR + 2]
-    // tile and plane chunk of this block
+    // per slot row: element offset of column c in the slot's row buffer is rowoff + c
+    int* const rowoff = reinterpret_cast<int*>(tma_smem + sizeof(T) * (size_t)NSL * (TR + 2) * lrow);   // [slot][TR + 2]
     int bid = blockIdx.x;
     const int tc = bid % V.tiles_c;
     bid /= V.tiles_c;
@@ -276,17 +278,19 @@ __global__ void __launch_bounds__(kTmaThreads) k_level_op_tma(StencilDev<T> A, T
     const int c0 = tc * TC, r0 = tr * TR;
     const int pa = ch * V.chunk, pb = min(pa + V.chunk, V.P);
     const int c_lo = max(c0 - 1, 0), c_hi = min(c0 + TC + 1, V.C);
-    // local planes: 3-D: pa - 1 .. pb (wrapped), 2-D: the one plane
-    const int nlocal = three ? (pb - pa + 2) : 1;
+    const int nlocal = pb - pa + 2;   // local planes pa - 1 .. pb (wrapped)
     if (threadIdx.x == 0) {
-        for (int q = 0; q < kTmaSlots; ++q) mbar_init(&bar[q], 1);
+        for (int q = 0; q < NSL; ++q) mbar_init(&bar[q], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    auto issue = [&](int L) {   // thread 0: copy local plane L into slot L % 4
-        const int slot = L % kTmaSlots;
-        int p = three ? pa - 1 + L : 0;
-        p = p < 0 ? p + V.P : (p >= V.P ? p - V.P : p);
+    auto plane_of = [&](int L) {
+        int p = pa - 1 + L;
+        return p < 0 ? p + V.P : (p >= V.P ? p - V.P : p);
+    };
+    auto issue = [&](int L) {   // thread 0: copy local plane L into slot L % NSL
+        const int slot = L % NSL;
+        const int p = plane_of(L);
         T* dst = ring + (size_t)slot * (TR + 2) * lrow;
         unsigned total = 0;
         for (int lr = 0; lr < TR + 2; ++lr) {
@@ -295,7 +299,7 @@ __global__ void __launch_bounds__(kTmaThreads) k_level_op_tma(StencilDev<T> A, T
             const int rw = r < 0 ? r + V.R : (r == V.R ? 0 : r);
             const RowCopy rc = row_copy<T>(((long long)p * V.R + rw) * V.C, c_lo, c_hi);
             total += rc.bytes;
-            leadv[slot * (TR + 2) + lr] = rc.lead;
+            rowoff[slot * (TR + 2) + lr] = (int)((size_t)(slot * (TR + 2) + lr) * lrow) + KA + rc.lead - c_lo;
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         mbar_expect_tx(&bar[slot], total);
@@ -308,41 +312,36 @@ __global__ void __launch_bounds__(kTmaThreads) k_level_op_tma(StencilDev<T> A, T
                      &bar[slot]);
         }
     };
-    // element (local row lr, column c) of a slot: the copy of columns [c_lo, c_hi)
-    // starts KA elements into the row, `lead` elements before column c_lo
-    auto at = [&](int slot, int lr, int c) -> T {
-        return ring[((size_t)slot * (TR + 2) + lr) * lrow + KA + leadv[slot * (TR + 2) + lr] + (c - c_lo)];
-    };
-    if (threadIdx.x == 0)
-        for (int L = 0; L < min(nslots, nlocal); ++L) issue(L);
     // wrapped halo columns: column -1 (when c0 == 0) and column C (when the tile reaches the last column)
     auto patch = [&](int L) {
-        const int slot = L % kTmaSlots;
-        int p = three ? pa - 1 + L : 0;
-        p = p < 0 ? p + V.P : (p >= V.P ? p - V.P : p);
         const bool left = c0 == 0, right = c0 + TC >= V.C;
         if (!left && !right) return;
+        const int slot = L % NSL;
+        const int p = plane_of(L);
         for (int lr = threadIdx.x; lr < TR + 2; lr += blockDim.x) {
             const int r = r0 - 1 + lr;
             if (r > V.R) continue;
             const int rw = r < 0 ? r + V.R : (r == V.R ? 0 : r);
             const long long base = ((long long)p * V.R + rw) * V.C;
-            T* row = ring + ((size_t)slot * (TR + 2) + lr) * lrow + KA + leadv[slot * (TR + 2) + lr];
-            if (left) row[-1 - c_lo] = x[base + V.C - 1];        // column -1
-            if (right) row[V.C - c_lo] = x[base];                // column C
+            T* row = ring + rowoff[slot * (TR + 2) + lr];
+            if (left) row[-1] = x[base + V.C - 1];     // column -1
+            if (right) row[V.C] = x[base];             // column C
         }
     };
-    const int planes = three ? (pb - pa) : 1;
+    if (threadIdx.x == 0)
+        for (int L = 0; L < min(NSL - 1, nlocal); ++L) issue(L);
+    __syncthreads();   // the row offsets thread 0 wrote are seen by the patches below
+    const int planes = pb - pa;
     for (int j = 0; j < planes; ++j) {
-        // planes j .. j + 2 (3-D) or plane 0 (2-D) must have landed
-        const int Lhi = three ? j + 2 : 0;
-        for (int L = three ? (j == 0 ? 0 : j + 2) : 0; L <= Lhi; ++L) {
-            mbar_wait_bounded(&bar[L % kTmaSlots], (unsigned)((L / kTmaSlots) & 1), stall);
+        // local planes j, j + 1, j + 2 (planes p - 1, p, p + 1) must have landed
+        for (int L = j == 0 ? 0 : j + 2; L <= j + 2; ++L) {
+            mbar_wait_bounded(&bar[L % NSL], (unsigned)((L / NSL) & 1), stall);
             patch(L);
         }
-        __syncthreads();
-        const int p = three ? pa + j : 0;
-        const int sm = three ? j % kTmaSlots : 0, s0 = three ? (j + 1) % kTmaSlots : 0, sp = three ? (j + 2) % kTmaSlots : 0;
+        __syncthreads();   // every thread is done with plane j - 1's slot and sees the patches
+        if (threadIdx.x == 0 && j + NSL - 1 < nlocal) issue(j + NSL - 1);   // refills the slot of local j - 1
+        const int p = pa + j;
+        const int sm = j % NSL, s0 = (j + 1) % NSL, sp = (j + 2) % NSL;
         for (int e = threadIdx.x; e < TR * TC; e += blockDim.x) {
             const int lr = e / TC + 1, cc = e % TC;
             const int rr = r0 + lr - 1, c = c0 + cc;
@@ -353,18 +352,8 @@ __global__ void __launch_bounds__(kTmaThreads) k_level_op_tma(StencilDev<T> A, T
 #pragma unroll
             for (int t = 0; t < NT; ++t) {
                 if (NS > 0 || t < A.ns) {
-                    int dp, dr, dc;
-                    if (three) {
-                        dp = A.di[t];
-                        dr = A.dj[t];
-                        dc = A.dk[t];
-                    } else {
-                        dp = 0;
-                        dr = A.di[t];
-                        dc = A.dj[t];
-                    }
-                    const int slot = dp < 0 ? sm : (dp > 0 ? sp : s0);
-                    s += A.c[t] * at(slot, lr + dr, c + dc);
+                    const int slot = A.di[t] < 0 ? sm : (A.di[t] > 0 ? sp : s0);
+                    s += A.c[t] * ring[rowoff[slot * (TR + 2) + lr + A.dj[t]] + c + A.dk[t]];
                 }
             }
             const int r32 = (int)row;
@@ -376,13 +365,11 @@ __global__ void __launch_bounds__(kTmaThreads) k_level_op_tma(StencilDev<T> A, T
                 s = T(0);
                 for (int t = b0; t < e0; ++t) s += __ldg(A.exc_val + t) * __ldg(x + __ldg(A.exc_col + t));
             }
-            if (Mode == kSmooth) out[row] = at(s0, lr, c) + omega * (__ldg(b + row) - s);
+            if (Mode == kSmooth) out[row] = ring[rowoff[s0 * (TR + 2) + lr] + c] + omega * (__ldg(b + row) - s);
             else out[row] = __ldg(b + row) - s;
         }
-        __syncthreads();   // slot j is free: refill it with local plane j + 4
-        if (three && threadIdx.x == 0 && j + kTmaSlots < nlocal) issue(j + kTmaSlots);
     }
-    // 2-D: nothing outstanding; 3-D: every issued plane was waited on
+    // every issued plane was waited on: nothing is in flight at exit
 }
 
 // b_c = dinv_c * (R r_f), x_c = 0 at coarse row c

@@ -146,6 +146,10 @@ def test_mixed_push_within_tolerance(kind):
         u = (exp_pos[a, ok] - g.lower[a]) / dx
         near |= np.abs(u - np.round(u)) < 1e-5
     assert (kg[ok][~near] == ke[~near]).all()
+    # the excluded particles: those within FP32 reach (1e-5 cells) of a face, about 2e-5 * 2 * dim of them
+    print(f"{kind}: keys compared for {int((~near).sum())} particles, {int(near.sum())} within 1e-5 cells of a "
+          f"face excluded; {int(ambiguous.sum())} within 1e-5 of an absorbing wall excluded from the loss check")
+    assert near.sum() <= max(3, 1e-3 * near.size) and ambiguous.sum() <= max(3, 1e-3 * ambiguous.size)
 
 
 @pytest.mark.parametrize("precision", [P.FP64, P.MIXED])

@@ -414,14 +414,20 @@ def test_1d_operators_multigrid_match_direct(kind):
 
 
 @pytest.mark.parametrize("kind", ["cuda_multigrid64_gpu", "cuda_multigrid32f_gpu"])
-@pytest.mark.parametrize("case", ["2d_1025", "2d_257", "3d_periodic_128", "3d_odd_65x70x90"])
+@pytest.mark.parametrize("case", ["3d_dirichlet_129", "3d_periodic_128", "3d_odd_65x70x90"])
 def test_tma_staged_sweeps_equal_per_row_sweeps(kind, case):
-    """Levels of 2^16 rows and more are swept by the TMA-staged kernel (row segments by cp.async.bulk into shared
-    memory); option `tma 0` keeps the per-row kernel.  Same taps in the same order: the iterates are identical."""
-    if case.startswith("2d"):
-        N = 1024 if case == "2d_1025" else 256
-        g, fixed, r, c, v, n, b = dirichlet_case(N, seed=7)
-        opts = f"I {N + 1} J {N + 1} K 1 depth 4 pre_relax 2 post_relax 2 max_cycles 6 correction_interval 2"
+    """3-D levels of 2^16 rows and more are swept by the TMA-staged kernel (row segments by cp.async.bulk into a
+    shared-memory plane ring); option `tma 0` keeps the per-row kernel.  Same taps in the same order: the
+    iterates are identical."""
+    if case == "3d_dirichlet_129":
+        g = P.simple_grid((0, 0, 0), (1, 1, 1), (128, 128, 128))
+        fixed = np.unique(np.concatenate([P.Dirichlet_plane(g, d, 0)[0]
+                                          for d in ("Xneg", "Xpos", "Yneg", "Ypos", "Zneg", "Zpos")]))
+        r, c, v = P.assemble_poisson(g, fixed, 1.0)
+        n = g.n_nodes
+        b = np.random.default_rng(7).normal(size=n)
+        b[fixed.astype(np.int64)] = 0.0
+        opts = "I 129 J 129 K 129 depth 4 pre_relax 2 post_relax 2 max_cycles 4 correction_interval 2"
     elif case == "3d_periodic_128":
         g, r, c, v, n, b = periodic_case(3, 128, seed=8)
         opts = ("I 128 J 128 K 128 depth 4 pre_relax 2 post_relax 2 max_cycles 4 correction_interval 2 "
@@ -447,15 +453,14 @@ def test_tma_staged_sweeps_equal_per_row_sweeps(kind, case):
 
 
 def test_tma_staged_fp64_vcycles_match_oracle():
-    """The FP64 V-cycles on a 257^2 box (TMA-staged sweeps on the finest level) still equal the oracle's."""
-    N, depth, cycles = 256, 4, 3
-    g, fixed, r, c, v, n, b = dirichlet_case(N, seed=11)
+    """The FP64 V-cycles on a 48^3-node periodic box (TMA-staged sweeps on the finest level) equal the oracle's."""
+    g, r, c, v, n, b = periodic_case(3, 48, seed=11)
     s = P.solver_backend("cuda_multigrid64_gpu")
-    s.set_options(f"I {N + 1} J {N + 1} K 1 depth {depth} pre_relax 2 post_relax 2 max_cycles {cycles}")
+    s.set_options("I 48 J 48 K 48 depth 3 pre_relax 2 post_relax 1 max_cycles 3 periodic_I 1 periodic_J 1 periodic_K 1")
     s.set_matrix(n, n, r.size, r, c, v)
     x0 = np.random.default_rng(12).normal(size=n) * 0.1
     bd, xd = dev(b), dev(x0)
     s.solve(bd, xd)
-    mg = O.Multigrid(r, c, v, n, N + 1, N + 1, 1, depth)
-    ref = mg.vcycles(b, x0, cycles, 2, 2)
+    mg = O.Multigrid(r, c, v, n, 48, 48, 48, 3, periodic=(1, 1, 1))
+    ref = mg.vcycles(b, x0, 3, 2, 1)
     assert np.linalg.norm(xd.cpu().numpy() - ref) / np.linalg.norm(ref) < 1e-12
