@@ -759,7 +759,7 @@ def run_bspline(args, torch, P):
     if not args.no_cpu_baseline:
         # the oracle's FP64 restatement on the host cores, on a bounded sample
         from oracle import oracle as O
-        m = min(args.cpu_sample, n)
+        m = min(1 << 21, n)   # about ten seconds of the oracle on the host cores
         sample = pos[:, :m].cpu().numpy()
         phi_h = phi.cpu().numpy()
         g = O.make_grid((cells, cells), (0.5, 0.5), (cells + 0.5, cells + 0.5), (0, 0))

@@ -104,6 +104,10 @@ EXPORT int psum_mg_last_stats(psum_field_solver_handle h, int* cycles, int* refi
 /* Number of levels actually built and the coarsest level's size. */
 EXPORT int psum_mg_hierarchy_info(psum_field_solver_handle h, int* levels, unsigned long long* coarse_rows,
                                   unsigned long long* exception_rows_level0);
+/* Level vectors the TMA-staged sweep kernel has read so far (one tensor map
+ * each): 0 with option `tma 0`, before the first solve, or when no level
+ * qualifies (3-D, at least 2^16 rows, rows a multiple of 16 bytes long). */
+EXPORT int psum_mg_tma_sweeps(psum_field_solver_handle h, int* level_vectors);
 EXPORT int psum_mg_destroy(psum_field_solver_handle h);
 
 /* ---- block 3: host-side FD operator assembly (the Poisson frontends) ----

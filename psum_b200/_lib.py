@@ -56,6 +56,7 @@ PROTOTYPES = {
     "psum_mg_solve_async": (I, [P, P, P, P]),
     "psum_mg_last_stats": (I, [P, C.POINTER(I), C.POINTER(I), C.POINTER(D), C.POINTER(D)]),
     "psum_mg_hierarchy_info": (I, [P, C.POINTER(I), C.POINTER(ULL), C.POINTER(ULL)]),
+    "psum_mg_tma_sweeps": (I, [P, C.POINTER(I)]),
     "psum_mg_destroy": (I, [P]),
     # block 3: FD operator assembly
     "psum_poisson_assemble": (I, [I, P, P, P, D, ULL, P, C.POINTER(ULL), P, P, P]),

@@ -28,6 +28,8 @@
 #include <string>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "common.hpp"
 #include "mg_backend.hpp"
 #include "mg_host.hpp"
@@ -110,32 +112,84 @@ struct DevAxis {
 
 // Launches of the stencil kernels with the operator's tap count as a
 // compile-time constant where it is one of the common ones.
-// Levels of at least this many rows take the TMA-staged sweep (when the
-// solver's option `tma` is on and the box is 2-D or 3-D).
+// 3-D levels of at least this many rows whose rows are a multiple of 16
+// bytes long take the TMA-staged sweep (when the solver's option `tma` is on).
 constexpr long long kTmaMinRows = 1LL << 16;
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library).
+inline PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        cuda_check(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q),
+                   "cudaGetDriverEntryPoint");
+        if (q != cudaDriverEntryPointSuccess || !p) throw Error(PSUM_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// The tensor map of a level vector viewed as (planes, rows, columns) with the
+// sweep's box; the vector is one of the solver's own buffers on this GPU.
+template <class T>
+CUtensorMap make_level_map(const T* x, int P, int R, int C) {
+    using S = TmaShape<T>;
+    CUtensorMap m;
+    const cuuint64_t dims[3] = {(cuuint64_t)C, (cuuint64_t)R, (cuuint64_t)P};
+    const cuuint64_t strides[2] = {(cuuint64_t)C * sizeof(T), (cuuint64_t)R * C * sizeof(T)};
+    const cuuint32_t box[3] = {(cuuint32_t)S::W, (cuuint32_t)S::H, 1u};
+    const cuuint32_t estr[3] = {1u, 1u, 1u};
+    const CUresult r = tmap_encoder()(&m, sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                                      3, const_cast<T*>(x), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw Error(PSUM_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    return m;
+}
+
+// Tensor maps of the level vectors the sweeps read, by pointer and view.
+struct TmapCache {
+    struct Entry {
+        const void* p;
+        int P, R, C;
+        CUtensorMap m;
+    };
+    std::vector<Entry> e;
+    template <class T>
+    const CUtensorMap& get(const T* x, int P, int R, int C) {
+        for (auto& q : e)
+            if (q.p == x && q.P == P && q.R == R && q.C == C) return q.m;
+        e.push_back({x, P, R, C, make_level_map<T>(x, P, R, C)});
+        return e.back().m;
+    }
+};
+
 template <class T, int Mode, int NS>
-void launch_tma_ns(const StencilDev<T>& A, const TmaTile& V, size_t smem, unsigned blocks, const T* x, const T* b,
-                   T* out, T omega, const MGState* st, int* stall, cudaStream_t s) {
+void launch_tma_ns(const CUtensorMap& map, const StencilDev<T>& A, const TmaTile& V, unsigned blocks, const T* x,
+                   const T* b, T* out, T omega, const MGState* st, int* stall, cudaStream_t s) {
     static bool attr = false;
     if (!attr) {
         cuda_check(cudaFuncSetAttribute(k_level_op_tma<T, Mode, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)(96 * 1024)),
+                                        (int)TmaShape<T>::smem()),
                    "cudaFuncSetAttribute");
         attr = true;
     }
-    k_level_op_tma<T, Mode, NS><<<blocks, kTmaThreads, smem, s>>>(A, V, x, b, out, omega, st, stall);
+    k_level_op_tma<T, Mode, NS><<<blocks, kTmaThreads, TmaShape<T>::smem(), s>>>(map, A, V, x, b, out, omega, st, stall);
 }
 
 // TMA-staged sweep of a level (k_level_op_tma); false when the level does
-// not qualify (small, or a 1-D box).
+// not qualify (small, not 3-D, or rows not a multiple of 16 bytes).
 template <class T, int Mode>
-bool launch_level_op_tma(const StencilDev<T>& A, const T* x, const T* b, T* out, T omega, const MGState* st,
-                         int* stall, cudaStream_t s) {
+bool launch_level_op_tma(TmapCache& cache, const StencilDev<T>& A, const T* x, const T* b, T* out, T omega,
+                         const MGState* st, int* stall, cudaStream_t s) {
     using S = TmaShape<T>;
     if (Mode == kSmoothFromZero || A.n < kTmaMinRows) return false;
+    if (!(A.n0 > 2 && A.n1 > 1 && A.n2 > 1)) return false;          // 3-D boxes only (2-D levels stay in L2)
+    if ((A.n2 * (int)sizeof(T)) % 16 != 0) return false;             // tensor-map row pitch: 16-byte multiple
+    if ((reinterpret_cast<uintptr_t>(x) & 15) != 0) return false;
     TmaTile V{};
-    if (!(A.n0 > 2 && A.n1 > 1 && A.n2 > 1)) return false;   // 3-D boxes only (2-D levels stay in L2)
     V.P = A.n0;
     V.R = A.n1;
     V.C = A.n2;
@@ -143,22 +197,21 @@ bool launch_level_op_tma(const StencilDev<T>& A, const T* x, const T* b, T* out,
     V.tiles_c = (V.C + S::TC - 1) / S::TC;
     V.tiles_r = (V.R + S::TR - 1) / S::TR;
     V.chunks = (V.P + V.chunk - 1) / V.chunk;
-    V.lrow = S::lrow();
-    const size_t smem = S::smem();
+    const CUtensorMap& map = cache.get<T>(x, V.P, V.R, V.C);
     const unsigned blocks = (unsigned)((long long)V.tiles_c * V.tiles_r * V.chunks);
-    if (A.ns == 5) launch_tma_ns<T, Mode, 5>(A, V, smem, blocks, x, b, out, omega, st, stall, s);
-    else if (A.ns == 7) launch_tma_ns<T, Mode, 7>(A, V, smem, blocks, x, b, out, omega, st, stall, s);
-    else if (A.ns == 9) launch_tma_ns<T, Mode, 9>(A, V, smem, blocks, x, b, out, omega, st, stall, s);
-    else if (A.ns == 27) launch_tma_ns<T, Mode, 27>(A, V, smem, blocks, x, b, out, omega, st, stall, s);
-    else launch_tma_ns<T, Mode, 0>(A, V, smem, blocks, x, b, out, omega, st, stall, s);
+    if (A.ns == 5) launch_tma_ns<T, Mode, 5>(map, A, V, blocks, x, b, out, omega, st, stall, s);
+    else if (A.ns == 7) launch_tma_ns<T, Mode, 7>(map, A, V, blocks, x, b, out, omega, st, stall, s);
+    else if (A.ns == 9) launch_tma_ns<T, Mode, 9>(map, A, V, blocks, x, b, out, omega, st, stall, s);
+    else if (A.ns == 27) launch_tma_ns<T, Mode, 27>(map, A, V, blocks, x, b, out, omega, st, stall, s);
+    else launch_tma_ns<T, Mode, 0>(map, A, V, blocks, x, b, out, omega, st, stall, s);
     count_launch();
     return true;
 }
 
 template <class T, int Mode>
 void launch_level_op(const StencilDev<T>& A, const T* x, const T* b, T* out, T omega, const MGState* st,
-                     cudaStream_t s, int* stall = nullptr) {
-    if (stall && launch_level_op_tma<T, Mode>(A, x, b, out, omega, st, stall, s)) return;
+                     cudaStream_t s, int* stall = nullptr, TmapCache* cache = nullptr) {
+    if (stall && cache && launch_level_op_tma<T, Mode>(*cache, A, x, b, out, omega, st, stall, s)) return;
     const unsigned g = grid_for(A.n);
     if (Mode == kSmoothFromZero) k_level_op<T, Mode, 0><<<g, kThreads, 0, s>>>(A, x, b, out, omega, st);
     else if (A.ns == 5) k_level_op<T, Mode, 5><<<g, kThreads, 0, s>>>(A, x, b, out, omega, st);
@@ -237,6 +290,7 @@ struct SolverBase {
     int levels = 0;
     unsigned long long coarse_rows = 0;
 
+    virtual int tma_level_vectors() const { return 0; }   // level vectors swept by the TMA-staged kernel so far
     virtual ~SolverBase() {
         drop_graph();
         if (aux_stream) cudaStreamDestroy(aux_stream);
@@ -260,6 +314,7 @@ struct Solver : SolverBase {
     DevBuf<double> coarse_inv;   // FP64 in both backends (see k_dense_mv)
     DevBuf<double> x64;   // FP64 level-0 iterate for the FP64 backend
     void build_device(cudaStream_t s) override {
+        tmaps.e.clear();
         a0.upload(host.a0, s);
         dinv0.upload(host.dinv[0].data(), host.dinv[0].size(), s);
         partials.alloc(kNormBlocks);
@@ -294,6 +349,8 @@ struct Solver : SolverBase {
 
     // the stall word of the TMA-staged sweeps, or null when option `tma` is off
     int* tma_stall() { return use_tma ? &state.p->stall : nullptr; }
+    TmapCache tmaps;   // tensor maps of the level vectors (rebuilt with the hierarchy)
+    int tma_level_vectors() const override { return (int)tmaps.e.size(); }
 
     // Enqueue `cycles` V(pre,post) cycles on level-0 (x0 in/out, b0 = scaled rhs).
     // `x_is_zero`: the level-0 iterate starts at zero (first sweep simplified).
@@ -319,7 +376,7 @@ struct Solver : SolverBase {
                 launch_level_op<T, kSmoothFromZero>(V.op.view, xcur[l], bl[l], xoth[l], omega, st, s);
                 zero[l] = false;
             } else {
-                launch_level_op<T, kSmooth>(V.op.view, xcur[l], bl[l], xoth[l], omega, st, s, tma_stall());
+                launch_level_op<T, kSmooth>(V.op.view, xcur[l], bl[l], xoth[l], omega, st, s, tma_stall(), &tmaps);
             }
             std::swap(xcur[l], xoth[l]);
         };
@@ -332,7 +389,7 @@ struct Solver : SolverBase {
                     { k_restrict<T><<<grid_for(lv[l + 1]->n), kThreads, 0, s>>>(V.xfer, bl[l], bl[l + 1], xcur[l + 1],
                                                                              lv[l + 1]->dinv.p, st); count_launch(); }
                 } else {
-                    launch_level_op<T, kResidual>(V.op.view, xcur[l], bl[l], xoth[l], omega, st, s, tma_stall());
+                    launch_level_op<T, kResidual>(V.op.view, xcur[l], bl[l], xoth[l], omega, st, s, tma_stall(), &tmaps);
                     { k_restrict<T><<<grid_for(lv[l + 1]->n), kThreads, 0, s>>>(V.xfer, xoth[l], bl[l + 1],
                                                                              xcur[l + 1], lv[l + 1]->dinv.p, st); count_launch(); }
                 }
@@ -798,6 +855,13 @@ EXPORT int psum_mg_hierarchy_info(psum_field_solver_handle h, int* levels, unsig
         if (levels) *levels = s->levels;
         if (coarse_rows) *coarse_rows = s->coarse_rows;
         if (exception_rows_level0) *exception_rows_level0 = s->host.ahat[0].exc_rows.size();
+    });
+}
+
+EXPORT int psum_mg_tma_sweeps(psum_field_solver_handle h, int* level_vectors) {
+    return guarded([&] {
+        SolverBase* s = solver_from_handle(h);
+        if (level_vectors) *level_vectors = s->tma_level_vectors();
     });
 }
 

@@ -13,6 +13,7 @@
 // body of the device-side refinement loop get no flag and skip that load.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -149,28 +150,30 @@ __global__ void __launch_bounds__(kThreads) k_level_op(StencilDev<T> A, const T*
 
 // ------------------------------------------------------ TMA-staged sweeps --
 // k_level_op_tma: the same smooth / residual sweep as k_level_op for large
-// 3-D levels, with x staged in shared memory by the TMA bulk-copy engine.
-// The level's node box is viewed as planes (i) x rows (j) x columns (k).  A
-// block owns a tile of TR rows x TC columns over a chunk of planes and
-// marches along the planes: the row segments of a plane (one halo row and
-// column on each side) arrive by cp.async.bulk into a ring of five plane
-// slots, completing on the slot's mbarrier; the copy's start is rounded down
-// to 16 bytes, so any row pitch works, and each row records where its
-// columns begin.  Halo cells across a box face are wrapped like the
-// stencil's own wrap (PSuM's cyclic neighbour rule) and patched from global
-// memory after the plane lands.  Planes p-1, p, p+1 are resident while p is
-// computed and p+2, p+3 are in flight; one block barrier per plane orders
-// the refill of the slot of p-2.  Taps are summed in the same order as
-// stencil_row, and exception rows take the same CSR path, so the results are
-// bit-identical to k_level_op.  b is read and out written directly (each
-// once, coalesced).  Every mbarrier wait is bounded: after 2^16 suspended
-// polls the block records a stall in *stall, and once a stall is recorded
-// later waits return at once, so a wrong byte count cannot hang the GPU.
+// 3-D levels whose rows are a multiple of 16 bytes long, with x staged in
+// shared memory by the TMA engine.  The level's node box is viewed as planes
+// (i) x rows (j) x columns (k), described by a tensor map.  A block owns a
+// tile of TR rows x TC columns over a chunk of planes and marches along the
+// planes: each plane's tile plus a halo (one row each side; the columns from
+// 16 bytes before the tile to 16 bytes after it, so the box starts on a
+// 16-byte boundary) arrives with one cp.async.bulk.tensor.3d into a ring of
+// five plane slots, completing on the slot's mbarrier.  The plane index is
+// wrapped in the copy's coordinate; halo rows and columns beyond the box
+// (zero-filled by the copy) are patched from global memory with the
+// stencil's own wrap (PSuM's cyclic neighbour rule), corners included.
+// Planes p-1, p, p+1 are resident while p is computed and p+2, p+3 are in
+// flight; one block barrier per plane orders the refill of the slot of p-2.
+// Taps are summed in the same order as stencil_row, and exception rows take
+// the same CSR path, so the results are bit-identical to k_level_op.  b is
+// read and out written directly (each once, coalesced).  Every mbarrier wait
+// is bounded: after 2^16 suspended polls the block records a stall in
+// *stall, and once a stall is recorded later waits return at once, so a
+// wrong byte count cannot hang the GPU.  The tensor map covers only the
+// solver's own level vector on this GPU; no multicast.
 struct TmaTile {
     int P, R, C;          // planes, rows, columns of the view (n0, n1, n2)
     int tiles_c, tiles_r;
     int chunk, chunks;    // planes per block, blocks along the planes
-    int lrow;             // shared-memory row stride in elements
 };
 
 constexpr int kTmaThreads = 256;
@@ -178,15 +181,14 @@ constexpr int kTmaSlots = 5;
 
 template <class T>
 struct TmaShape {
-    static constexpr int TC = sizeof(T) == 4 ? 128 : 64;   // columns per tile (one 512-byte segment)
+    static constexpr int TC = sizeof(T) == 4 ? 128 : 64;   // columns per tile (512 bytes)
     static constexpr int TR = 16;                           // rows per tile
-    static constexpr int kAlign = 16 / (int)sizeof(T);      // elements per 16 bytes
-    // row stride: one aligned lead unit, the segment (TC + 2 halo) and the
-    // alignment slack of its end, rounded to 16 bytes
-    static constexpr int lrow() { return ((kAlign + TC + 2 + 2 * kAlign) + kAlign - 1) / kAlign * kAlign; }
-    static constexpr size_t smem() {
-        return sizeof(T) * (size_t)kTmaSlots * (TR + 2) * lrow() + sizeof(int) * (size_t)kTmaSlots * (TR + 2);
-    }
+    static constexpr int KA = 16 / (int)sizeof(T);          // elements per 16 bytes: the column halo of the box
+    static constexpr int W = TC + 2 * KA;                   // box columns (multiple of 16 bytes)
+    static constexpr int H = TR + 2;                        // box rows
+    static constexpr size_t box_bytes() { return sizeof(T) * (size_t)W * H; }
+    static constexpr size_t slot_bytes() { return (box_bytes() + 127) / 128 * 128; }   // 128-byte aligned slots
+    static constexpr size_t smem() { return slot_bytes() * kTmaSlots + 8 * kTmaSlots; }   // slots, then mbarriers
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -225,51 +227,29 @@ __device__ __forceinline__ void mbar_wait_bounded(unsigned long long* bar, unsig
     atomicExch(stall, 1);
 }
 
-// One bulk copy global -> shared (both 16-byte aligned, size a multiple of
-// 16), completing `bytes` on bar.  Reads only this GPU's own memory.
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+// One tiled TMA load of the box at (x, y, z) of the tensor map into shared
+// memory, completing its bytes on bar.  x is a multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_3d(void* dst, const void* tmap, int x, int y, int z, unsigned long long* bar) {
     asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_u32(dst)),
+        "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
         : "memory");
 }
 
-// Byte extent of the 16-byte-aligned copy of columns [c_lo, c_hi) of view
-// row `row` (global element offset base = row * C).
-struct RowCopy {
-    long long g0;      // aligned global byte offset
-    unsigned bytes;    // multiple of 16
-    int lead;          // elements between the copy start and column c_lo
-};
-
-template <class T>
-__device__ __forceinline__ RowCopy row_copy(long long base, int c_lo, int c_hi) {
-    const long long b0 = (base + c_lo) * (long long)sizeof(T);
-    const long long b1 = (base + c_hi) * (long long)sizeof(T);
-    RowCopy rc;
-    rc.g0 = b0 & ~15LL;
-    rc.bytes = (unsigned)(((b1 + 15) & ~15LL) - rc.g0);
-    rc.lead = (int)((b0 - rc.g0) / (long long)sizeof(T));
-    return rc;
-}
-
 template <class T, int Mode, int NS>
-__global__ void __launch_bounds__(kTmaThreads) k_level_op_tma(StencilDev<T> A, TmaTile V, const T* __restrict__ x,
+__global__ void __launch_bounds__(kTmaThreads) k_level_op_tma(const __grid_constant__ CUtensorMap xmap, StencilDev<T> A,
+                                                              TmaTile V, const T* __restrict__ x,
                                                               const T* __restrict__ b, T* __restrict__ out, T omega,
                                                               const MGState* __restrict__ st, int* stall) {
     using S = TmaShape<T>;
-    constexpr int TC = S::TC;
-    constexpr int TR = S::TR;
-    constexpr int KA = S::kAlign;
+    constexpr int TC = S::TC, TR = S::TR, KA = S::KA, W = S::W, H = S::H;
     constexpr int NSL = kTmaSlots;
+    constexpr int SLOT = (int)(S::slot_bytes() / sizeof(T));   // slot stride in elements
     if (st && st->done) return;   // st == nullptr: ungated (inside the device-side loop)
     extern __shared__ __align__(128) unsigned char tma_smem[];
-    __shared__ __align__(8) unsigned long long bar[NSL];
-    const int lrow = V.lrow;
-    T* const ring = reinterpret_cast<T*>(tma_smem);   // [slot][TR + 2][lrow]
-    // per slot row: element offset of column c in the slot's row buffer is rowoff + c
-    int* const rowoff = reinterpret_cast<int*>(tma_smem + sizeof(T) * (size_t)NSL * (TR + 2) * lrow);   // [slot][TR + 2]
+    T* const ring = reinterpret_cast<T*>(tma_smem);   // [slot][H][W]; column c at index c - (c0 - KA)
+    unsigned long long* const bar = reinterpret_cast<unsigned long long*>(tma_smem + S::slot_bytes() * NSL);
     int bid = blockIdx.x;
     const int tc = bid % V.tiles_c;
     bid /= V.tiles_c;
@@ -277,8 +257,8 @@ __global__ void __launch_bounds__(kTmaThreads) k_level_op_tma(StencilDev<T> A, T
     const int ch = bid / V.tiles_r;
     const int c0 = tc * TC, r0 = tr * TR;
     const int pa = ch * V.chunk, pb = min(pa + V.chunk, V.P);
-    const int c_lo = max(c0 - 1, 0), c_hi = min(c0 + TC + 1, V.C);
     const int nlocal = pb - pa + 2;   // local planes pa - 1 .. pb (wrapped)
+    const bool edge = r0 == 0 || r0 + TR >= V.R || c0 == 0 || c0 + TC >= V.C;
     if (threadIdx.x == 0) {
         for (int q = 0; q < NSL; ++q) mbar_init(&bar[q], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -288,49 +268,28 @@ __global__ void __launch_bounds__(kTmaThreads) k_level_op_tma(StencilDev<T> A, T
         int p = pa - 1 + L;
         return p < 0 ? p + V.P : (p >= V.P ? p - V.P : p);
     };
-    auto issue = [&](int L) {   // thread 0: copy local plane L into slot L % NSL
+    auto issue = [&](int L) {   // thread 0: local plane L into slot L % NSL
         const int slot = L % NSL;
-        const int p = plane_of(L);
-        T* dst = ring + (size_t)slot * (TR + 2) * lrow;
-        unsigned total = 0;
-        for (int lr = 0; lr < TR + 2; ++lr) {
-            const int r = r0 - 1 + lr;
-            if (r > V.R) break;                       // below the row after the last: not needed
-            const int rw = r < 0 ? r + V.R : (r == V.R ? 0 : r);
-            const RowCopy rc = row_copy<T>(((long long)p * V.R + rw) * V.C, c_lo, c_hi);
-            total += rc.bytes;
-            rowoff[slot * (TR + 2) + lr] = (int)((size_t)(slot * (TR + 2) + lr) * lrow) + KA + rc.lead - c_lo;
-        }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_expect_tx(&bar[slot], total);
-        for (int lr = 0; lr < TR + 2; ++lr) {
-            const int r = r0 - 1 + lr;
-            if (r > V.R) break;
-            const int rw = r < 0 ? r + V.R : (r == V.R ? 0 : r);
-            const RowCopy rc = row_copy<T>(((long long)p * V.R + rw) * V.C, c_lo, c_hi);
-            bulk_g2s(dst + (size_t)lr * lrow + KA, reinterpret_cast<const unsigned char*>(x) + rc.g0, rc.bytes,
-                     &bar[slot]);
-        }
+        mbar_expect_tx(&bar[slot], (unsigned)S::box_bytes());
+        tma_load_3d(ring + (size_t)slot * SLOT, &xmap, c0 - KA, r0 - 1, plane_of(L), &bar[slot]);
     };
-    // wrapped halo columns: column -1 (when c0 == 0) and column C (when the tile reaches the last column)
+    auto wrapi = [](int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); };
+    // halo cells the box could not read: row -1 / row R and column -1 / column C, wrapped
     auto patch = [&](int L) {
-        const bool left = c0 == 0, right = c0 + TC >= V.C;
-        if (!left && !right) return;
-        const int slot = L % NSL;
-        const int p = plane_of(L);
-        for (int lr = threadIdx.x; lr < TR + 2; lr += blockDim.x) {
-            const int r = r0 - 1 + lr;
-            if (r > V.R) continue;
-            const int rw = r < 0 ? r + V.R : (r == V.R ? 0 : r);
-            const long long base = ((long long)p * V.R + rw) * V.C;
-            T* row = ring + rowoff[slot * (TR + 2) + lr];
-            if (left) row[-1] = x[base + V.C - 1];     // column -1
-            if (right) row[V.C] = x[base];             // column C
+        if (!edge) return;
+        T* slot = ring + (size_t)(L % NSL) * SLOT;
+        const long long pbase = (long long)plane_of(L) * V.R;
+        for (int e = threadIdx.x; e < H * (TC + 2); e += blockDim.x) {
+            const int lr = e / (TC + 2), k = e % (TC + 2);
+            const int r = r0 - 1 + lr, c = c0 - 1 + k;
+            if (r > V.R || c > V.C) continue;                               // beyond the halo: never read
+            if (r >= 0 && r < V.R && c >= 0 && c < V.C) continue;           // inside the box: the copy read it
+            slot[lr * W + (c - (c0 - KA))] = x[(pbase + wrapi(r, V.R)) * V.C + wrapi(c, V.C)];
         }
     };
     if (threadIdx.x == 0)
         for (int L = 0; L < min(NSL - 1, nlocal); ++L) issue(L);
-    __syncthreads();   // the row offsets thread 0 wrote are seen by the patches below
     const int planes = pb - pa;
     for (int j = 0; j < planes; ++j) {
         // local planes j, j + 1, j + 2 (planes p - 1, p, p + 1) must have landed
@@ -341,19 +300,22 @@ __global__ void __launch_bounds__(kTmaThreads) k_level_op_tma(StencilDev<T> A, T
         __syncthreads();   // every thread is done with plane j - 1's slot and sees the patches
         if (threadIdx.x == 0 && j + NSL - 1 < nlocal) issue(j + NSL - 1);   // refills the slot of local j - 1
         const int p = pa + j;
-        const int sm = j % NSL, s0 = (j + 1) % NSL, sp = (j + 2) % NSL;
+        const T* const sm = ring + (size_t)(j % NSL) * SLOT;
+        const T* const s0 = ring + (size_t)((j + 1) % NSL) * SLOT;
+        const T* const sp = ring + (size_t)((j + 2) % NSL) * SLOT;
         for (int e = threadIdx.x; e < TR * TC; e += blockDim.x) {
             const int lr = e / TC + 1, cc = e % TC;
             const int rr = r0 + lr - 1, c = c0 + cc;
             if (rr >= V.R || c >= V.C) continue;
             const long long row = ((long long)p * V.R + rr) * V.C + c;   // global row index of the level
+            const int at = lr * W + cc + KA;                                 // (lr, c) in a slot
             constexpr int NT = NS > 0 ? NS : kMaxTaps;
             T s = T(0);
 #pragma unroll
             for (int t = 0; t < NT; ++t) {
                 if (NS > 0 || t < A.ns) {
-                    const int slot = A.di[t] < 0 ? sm : (A.di[t] > 0 ? sp : s0);
-                    s += A.c[t] * ring[rowoff[slot * (TR + 2) + lr + A.dj[t]] + c + A.dk[t]];
+                    const T* pl = A.di[t] < 0 ? sm : (A.di[t] > 0 ? sp : s0);
+                    s += A.c[t] * pl[at + A.dj[t] * W + A.dk[t]];
                 }
             }
             const int r32 = (int)row;
@@ -365,7 +327,7 @@ __global__ void __launch_bounds__(kTmaThreads) k_level_op_tma(StencilDev<T> A, T
                 s = T(0);
                 for (int t = b0; t < e0; ++t) s += __ldg(A.exc_val + t) * __ldg(x + __ldg(A.exc_col + t));
             }
-            if (Mode == kSmooth) out[row] = ring[rowoff[s0 * (TR + 2) + lr] + c] + omega * (__ldg(b + row) - s);
+            if (Mode == kSmooth) out[row] = s0[at] + omega * (__ldg(b + row) - s);
             else out[row] = __ldg(b + row) - s;
         }
     }

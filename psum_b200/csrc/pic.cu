@@ -92,9 +92,11 @@ struct PushArgs {
     float* vel[3];
     const long long* count;
     const float* edges;
-    float gs[3];        // gradient scale: -(q/m) dt dr_a (leapfrog) or -dr_a (q/m) dt / 2 (Boris)
+    float kE[3];        // q/m * dt * dr_a  (velocity kick per unit edge difference)
     float dtdr[3];      // dt * dr_a        (offset change per unit velocity)
+    float qmdt_half;    // q/m * dt / 2 (Boris)
     float Bt[3];        // B * q/m * dt / 2 (Boris t vector)
+    float dr[3];
     unsigned long long* acc;
     int dep_lsh;        // accumulator units per 2^-26 weight unit: 2^dep_lsh
     unsigned long long* losses;
@@ -103,40 +105,32 @@ struct PushArgs {
     double kin_hmw;     // m * w / 2
 };
 
-// Gradient data of one cell, pre-scaled for the species' kick.  The CIC
-// gradient of PSuM's interp_diff (simple_interpolation.hpp:58-98) is a
-// bilinear (3D) or linear (2D) blend of the edge differences G_a, which live
-// on the edges along axis a and so vary with the other axes' offsets only.
-// Stored per axis as (base, slope) pairs of the scaled differences
-// s_a * G_a, where s_a = -(q/m) dt dr_a (leapfrog: the kick itself) or
-// -dr_a (q/m) dt / 2 (Boris: E dt q/2m), so that a gather is one FMA per
-// axis in 2D and four in 3D.  Every kernel that moves particles uses these
-// same operations, so they all move a particle bit-identically.
+// Field data of one cell for the CIC gather of the edge differences: the
+// components that interpolate G_a over the cell (G_a lives on the edges along
+// axis a, so it varies with the other axes' offsets only).
 template <int D>
-struct CellCoef {
-    float k[D == 1 ? 2 : (D == 2 ? 4 : 12)];
+struct CellField {
+    float e[D == 1 ? 1 : (D == 2 ? 4 : 12)];
 };
 
 template <int D>
-__device__ __forceinline__ void cell_coef(const PushArgs& a, int c0, int c1, int c2, CellCoef<D>& K) {
+__device__ __forceinline__ void load_cell_field(const PushArgs& a, int c0, int c1, int c2, CellField<D>& F) {
     const GridView& g = a.g;
-    if (D == 1) {
+    if constexpr (D == 1) {
         // 1-D: the CIC gradient is the cell's one edge difference (constant in the cell)
-        const float2* E = reinterpret_cast<const float2*>(a.edges);
-        K.k[0] = __fmul_rn(a.gs[0], __ldg(E + c0).x);
-        K.k[1] = 0.f;
+        F.e[0] = __ldg(reinterpret_cast<const float2*>(a.edges) + c0).x;
         (void)c1;
         (void)c2;
-    } else if (D == 2) {
+    } else if constexpr (D == 2) {
         const float2* E = reinterpret_cast<const float2*>(a.edges);
         const int n0p = next_node(g, 0, c0), n1p = next_node(g, 1, c1);
         const float2 e00 = __ldg(E + node_index(g, c0, c1, 0));
         const float2 e01 = __ldg(E + node_index(g, c0, n1p, 0));
         const float2 e10 = __ldg(E + node_index(g, n0p, c1, 0));
-        K.k[0] = __fmul_rn(a.gs[0], e00.x);                        // axis 0 at f1 = 0
-        K.k[1] = __fmul_rn(a.gs[0], __fsub_rn(e01.x, e00.x));      // its slope in f1
-        K.k[2] = __fmul_rn(a.gs[1], e00.y);                        // axis 1 at f0 = 0
-        K.k[3] = __fmul_rn(a.gs[1], __fsub_rn(e10.y, e00.y));      // its slope in f0
+        F.e[0] = e00.x;
+        F.e[1] = e01.x;
+        F.e[2] = e00.y;
+        F.e[3] = e10.y;
     } else {
         const float4* E = reinterpret_cast<const float4*>(a.edges);
         const int n0p = next_node(g, 0, c0), n1p = next_node(g, 1, c1), n2p = next_node(g, 2, c2);
@@ -147,50 +141,52 @@ __device__ __forceinline__ void cell_coef(const PushArgs& a, int c0, int c1, int
         const float4 e100 = __ldg(E + node_index(g, n0p, c1, c2));
         const float4 e101 = __ldg(E + node_index(g, n0p, c1, n2p));
         const float4 e110 = __ldg(E + node_index(g, n0p, n1p, c2));
-        // per axis: (lo base, lo slope, hi base, hi slope) along the inner blend axis
-        const float s0 = a.gs[0], s1 = a.gs[1], s2 = a.gs[2];
-        K.k[0] = __fmul_rn(s0, e000.x); K.k[1] = __fmul_rn(s0, __fsub_rn(e001.x, e000.x));   // f2 at f1 = 0
-        K.k[2] = __fmul_rn(s0, e010.x); K.k[3] = __fmul_rn(s0, __fsub_rn(e011.x, e010.x));   // f2 at f1 = 1
-        K.k[4] = __fmul_rn(s1, e000.y); K.k[5] = __fmul_rn(s1, __fsub_rn(e001.y, e000.y));   // f2 at f0 = 0
-        K.k[6] = __fmul_rn(s1, e100.y); K.k[7] = __fmul_rn(s1, __fsub_rn(e101.y, e100.y));   // f2 at f0 = 1
-        K.k[8] = __fmul_rn(s2, e000.z); K.k[9] = __fmul_rn(s2, __fsub_rn(e010.z, e000.z));   // f1 at f0 = 0
-        K.k[10] = __fmul_rn(s2, e100.z); K.k[11] = __fmul_rn(s2, __fsub_rn(e110.z, e100.z)); // f1 at f0 = 1
+        F.e[0] = e000.x; F.e[1] = e001.x; F.e[2] = e010.x; F.e[3] = e011.x;
+        F.e[4] = e000.y; F.e[5] = e001.y; F.e[6] = e100.y; F.e[7] = e101.y;
+        F.e[8] = e000.z; F.e[9] = e010.z; F.e[10] = e100.z; F.e[11] = e110.z;
     }
 }
 
-// Scaled gradient s_a G_a at in-cell offsets f.
 template <int D>
-__device__ __forceinline__ void grad_scaled(const CellCoef<D>& K, const float f[3], float G[3]) {
-    if (D == 1) {
-        G[0] = K.k[0];
+__device__ __forceinline__ void interp_grad(const CellField<D>& F, const float f[3], float G[3]) {
+#define PSUM_LERP(a_, wa_, b_, wb_) __fmaf_rn((b_), (wb_), __fmul_rn((a_), (wa_)))
+    if constexpr (D == 1) {
+        G[0] = F.e[0];
         G[1] = G[2] = 0.f;
-    } else if (D == 2) {
-        G[0] = __fmaf_rn(f[1], K.k[1], K.k[0]);
-        G[1] = __fmaf_rn(f[0], K.k[3], K.k[2]);
+        (void)f;
+    } else if constexpr (D == 2) {
+        G[0] = PSUM_LERP(F.e[0], __fsub_rn(1.f, f[1]), F.e[1], f[1]);
+        G[1] = PSUM_LERP(F.e[2], __fsub_rn(1.f, f[0]), F.e[3], f[0]);
         G[2] = 0.f;
     } else {
-        float lo = __fmaf_rn(f[2], K.k[1], K.k[0]), hi = __fmaf_rn(f[2], K.k[3], K.k[2]);
-        G[0] = __fmaf_rn(f[1], __fsub_rn(hi, lo), lo);
-        lo = __fmaf_rn(f[2], K.k[5], K.k[4]);
-        hi = __fmaf_rn(f[2], K.k[7], K.k[6]);
-        G[1] = __fmaf_rn(f[0], __fsub_rn(hi, lo), lo);
-        lo = __fmaf_rn(f[1], K.k[9], K.k[8]);
-        hi = __fmaf_rn(f[1], K.k[11], K.k[10]);
-        G[2] = __fmaf_rn(f[0], __fsub_rn(hi, lo), lo);
+        const float g0 = __fsub_rn(1.f, f[0]), g1 = __fsub_rn(1.f, f[1]), g2 = __fsub_rn(1.f, f[2]);
+        G[0] = PSUM_LERP(PSUM_LERP(F.e[0], g2, F.e[1], f[2]), g1, PSUM_LERP(F.e[2], g2, F.e[3], f[2]), f[1]);
+        G[1] = PSUM_LERP(PSUM_LERP(F.e[4], g2, F.e[5], f[2]), g0, PSUM_LERP(F.e[6], g2, F.e[7], f[2]), f[0]);
+        G[2] = PSUM_LERP(PSUM_LERP(F.e[8], g1, F.e[9], f[1]), g0, PSUM_LERP(F.e[10], g1, F.e[11], f[1]), f[0]);
     }
+#undef PSUM_LERP
 }
 
-// Velocity update from the scaled gradient G (leapfrog: v += G; Boris: half
-// kick, rotation, half kick, with E q dt / 2m = G).
+// Velocity update from the gathered edge differences G, then the move in
+// cell units.  f holds the new in-cell offsets and dc the cell steps per axis
+// on exit (offset carry rule: an offset that rounds to 1.0f moves to the next
+// cell with offset 0).  Every operation is an explicit round-to-nearest
+// intrinsic (fused multiply-adds where written), so every kernel that calls
+// this function moves the same particle bit-identically.  False when the
+// state became non-finite (kick_move flags the error word; kick_move_core
+// leaves that to its caller).
 template <int D, int PUSHER>
-__device__ __forceinline__ void kick(const PushArgs& a, const float G[3], float v[3]) {
+__device__ __forceinline__ bool kick_move_core(const PushArgs& a, const float G[3], float f[3], float v[3], int dc[3]) {
     if (PUSHER == PSUM_PIC_LEAPFROG) {
 #pragma unroll
-        for (int d = 0; d < D; ++d) v[d] = __fadd_rn(v[d], G[d]);
+        for (int d = 0; d < D; ++d) v[d] = __fmaf_rn(-a.kE[d], G[d], v[d]);   // v += (q/m) E dt, E = -dr G
     } else {
+        float E[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int d = 0; d < D; ++d) E[d] = -__fmul_rn(a.dr[d], G[d]);
         float vm[3], vp[3], vq[3], s[3];
 #pragma unroll
-        for (int q = 0; q < 3; ++q) vm[q] = __fadd_rn(v[q], G[q]);
+        for (int q = 0; q < 3; ++q) vm[q] = __fadd_rn(v[q], __fmul_rn(E[q], a.qmdt_half));
         const float t2 = __fadd_rn(__fadd_rn(__fmul_rn(a.Bt[0], a.Bt[0]), __fmul_rn(a.Bt[1], a.Bt[1])),
                                    __fmul_rn(a.Bt[2], a.Bt[2]));
 #pragma unroll
@@ -204,26 +200,15 @@ __device__ __forceinline__ void kick(const PushArgs& a, const float G[3], float 
         vp[2] = __fadd_rn(vm[2], PSUM_CROSS(vq[0], s[1], vq[1], s[0]));
 #undef PSUM_CROSS
 #pragma unroll
-        for (int q = 0; q < 3; ++q) v[q] = __fadd_rn(vp[q], G[q]);
+        for (int q = 0; q < 3; ++q) v[q] = __fadd_rn(vp[q], __fmul_rn(E[q], a.qmdt_half));
     }
-}
-
-// The move in cell units: new offsets f and cell steps dc from
-// sd_a = f_a + v_a dt dr_a, f = sd - floor(sd), dc = floor(sd), with the
-// carry rule (an offset that rounds to 1.0f moves to the next cell with
-// offset 0).  Returns false when the state is non-finite (or beyond 1e9
-// cells).
-template <int D>
-__device__ __forceinline__ bool move(const PushArgs& a, const float v[3], float f[3], int dc[3]) {
-    float sd[3];
-#pragma unroll
-    for (int d = 0; d < D; ++d) sd[d] = __fmaf_rn(v[d], a.dtdr[d], f[d]);
     bool ok = true;
 #pragma unroll
     for (int d = 0; d < D; ++d) {
-        ok = ok && fabsf(sd[d]) < 1.0e9f;   // false for NaN and infinities too
-        const float fl = floorf(sd[d]);
-        float nf = __fsub_rn(sd[d], fl);
+        const float sd = __fmaf_rn(v[d], a.dtdr[d], f[d]);
+        ok = ok && fabsf(sd) < 1.0e9f;   // false for NaN and infinities too
+        const float fl = floorf(sd);
+        float nf = __fsub_rn(sd, fl);
         int step = (int)fl;
         if (nf >= 1.0f) {
             nf = 0.0f;
@@ -232,6 +217,13 @@ __device__ __forceinline__ bool move(const PushArgs& a, const float v[3], float 
         f[d] = nf;
         dc[d] = step;
     }
+    return ok;
+}
+
+template <int D, int PUSHER>
+__device__ __forceinline__ bool kick_move(const PushArgs& a, const float G[3], float f[3], float v[3], int dc[3]) {
+    const bool ok = kick_move_core<D, PUSHER>(a, G, f, v, dc);
+    if (!ok) atomicOr(a.err, kErrNonFinite);
     return ok;
 }
 
@@ -258,19 +250,15 @@ __device__ __forceinline__ int apply_step(const GridView& g, int c[3], const int
 
 // One particle: gather, push, boundary.  c[] holds the cell on entry and the
 // new cell on exit.  Returns the loss code (axis*2+side), -1 when the
-// particle stays, or -2 when its state became non-finite (error word set).
+// particle stays, or -2 when its state became non-finite.
 template <int D, int PUSHER>
 __device__ __forceinline__ int push_one(const PushArgs& a, int c[3], float f[3], float v[3]) {
-    CellCoef<D> K;
-    cell_coef<D>(a, c[0], c[1], c[2], K);
+    CellField<D> F;
+    load_cell_field<D>(a, c[0], c[1], c[2], F);
     float G[3];
-    grad_scaled<D>(K, f, G);
-    kick<D, PUSHER>(a, G, v);
+    interp_grad<D>(F, f, G);
     int dc[3] = {0, 0, 0};
-    if (!move<D>(a, v, f, dc)) {
-        atomicOr(a.err, kErrNonFinite);
-        return -2;
-    }
+    if (!kick_move<D, PUSHER>(a, G, f, v, dc)) return -2;
     return apply_step<D>(a.g, c, dc);
 }
 
@@ -490,16 +478,7 @@ constexpr int kClsTileMax = 3072;   // int64 node accumulators in shared memory 
 // Rounds of 32 particles per warp iteration (all loads issued first): 4, or
 // 1 for species with few particles per cell (empty rounds cost a cell's
 // whole iteration there).
-#ifndef PSUM_V_ROUNDS
-#define PSUM_V_ROUNDS 4
-#endif
-#ifndef PSUM_V_P2B
-#define PSUM_V_P2B 5
-#endif
-#ifndef PSUM_V_P1B
-#define PSUM_V_P1B 1
-#endif
-constexpr int kClsRoundsMax = PSUM_V_ROUNDS;
+constexpr int kClsRoundsMax = 4;
 constexpr int cls_rounds(double particles_per_cell) { return particles_per_cell < 64.0 ? 1 : kClsRoundsMax; }
 
 // Particles per block: 2D blocks cover a few tens of cells of one row; 3D
@@ -647,21 +626,42 @@ __device__ __forceinline__ void deposit_direct(const PushArgs& a, const int c[3]
     }
 }
 
-// Push of one particle of cell co with the warp's cell coefficients: move
-// class (>= 0), -1 far (more than one cell on some axis), -3 absorbed or
-// non-finite (loss counted).  `edge` is false for cells whose one-cell
-// neighbours all lie inside the cell lattice without a wrap (the common
-// case): a one-cell move from such a cell needs no boundary test.  Wrapping,
-// losses, far moves and non-finite states take a rare path that follows
-// push_one exactly.
+// Push of one particle of cell co with the warp's cell field: move class
+// (>= 0), -1 far (more than one cell on some axis), -3 absorbed or
+// non-finite (loss counted).  cn is the new cell for far particles.
 template <int D, int PUSHER>
-__device__ __forceinline__ int push_classify(const PushArgs& a, const CellCoef<D>& K, const int co[3], bool edge,
-                                             float f[3], float v[3], unsigned lost_cnt[2 * D]) {
+__device__ __forceinline__ int push_classify(const PushArgs& a, const CellField<D>& F, const int co[3], float f[3],
+                                             float v[3], int cn[3], unsigned lost_cnt[2 * D]) {
     float G[3];
-    grad_scaled<D>(K, f, G);
-    kick<D, PUSHER>(a, G, v);
+    interp_grad<D>(F, f, G);
     int dc[3] = {0, 0, 0};
-    const bool ok = move<D>(a, v, f, dc);
+    const bool ok = kick_move_core<D, PUSHER>(a, G, f, v, dc);
+    // common path: the new cell lies inside the lattice on every axis (one
+    // unsigned test per axis); wrapping, losses and non-finite states take
+    // the rare path, which follows kick_move and apply_step exactly
+    const GridView& g = a.g;
+    bool out = false;
+    cn[2] = co[2];
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        cn[d] = co[d] + dc[d];
+        out |= (unsigned)cn[d] >= (unsigned)(g.periodic[d] ? g.M[d] : g.cells[d]);
+    }
+    if (!ok || out) {
+        if (!ok) {
+            atomicOr(a.err, kErrNonFinite);
+            return -3;
+        }
+        cn[0] = co[0];
+        cn[1] = co[1];
+        cn[2] = co[2];
+        const int lost = apply_step<D>(g, cn, dc);
+        if (lost >= 0) {
+#pragma unroll
+            for (int q = 0; q < 2 * D; ++q) lost_cnt[q] += (lost == q);
+            return -3;
+        }
+    }
     int cls = 0;
     bool far = false;
 #pragma unroll
@@ -669,31 +669,7 @@ __device__ __forceinline__ int push_classify(const PushArgs& a, const CellCoef<D
         far |= (unsigned)(dc[d] + 1) > 2u;
         cls = cls * 3 + dc[d] + 1;
     }
-    if (!ok || far || edge) {
-        if (!ok) {
-            atomicOr(a.err, kErrNonFinite);
-            return -3;
-        }
-        int cn[3] = {co[0], co[1], co[2]};
-        const int lost = apply_step<D>(a.g, cn, dc);
-        if (lost >= 0) {
-#pragma unroll
-            for (int q = 0; q < 2 * D; ++q) lost_cnt[q] += (lost == q);
-            return -3;
-        }
-        if (far) return -1;
-    }
-    return cls;
-}
-
-// True when cell co has a neighbour outside the lattice or across a
-// periodic seam on some axis (one-cell moves from it need the boundary test).
-template <int D>
-__device__ __forceinline__ bool edge_cell(const GridView& g, const int co[3]) {
-    bool e = false;
-#pragma unroll
-    for (int d = 0; d < D; ++d) e |= co[d] == 0 || co[d] >= (g.periodic[d] ? g.M[d] : g.cells[d]) - 1;
-    return e;
+    return far ? -1 : cls;
 }
 
 // Exact warp sum of per-lane values below 2^32 (two reductions of 26-bit
@@ -732,22 +708,17 @@ struct CellTileCap {
 
 
 template <int D, int PUSHER, int kClsRounds>
-__global__ void __launch_bounds__(kPicThreads, PSUM_V_P1B) k_cls_pass1(ClsArgs a) {
+__global__ void __launch_bounds__(kPicThreads) k_cls_pass1(ClsArgs a) {
     constexpr int NC = MoveClasses<D>::N;
     constexpr int STAY = MoveClasses<D>::STAY;
     constexpr int NM = 1 << D;
     constexpr int CT = CellTileCap<D>::N;
     constexpr int NT = CellTileCap<D>::NODES;
-    constexpr int NV = (D == 2 && PUSHER == PSUM_PIC_LEAPFROG) ? 2 : 3;   // velocity components the push reads
     // per (warp, moment, class): count (moment 0, low word only) and moment
-    // sums of the movers of the warp's current cell; per cell of the block's
-    // box the count and moment sums (units of 2^-26) of the particles that
-    // end there; the box's node tile
+    // sums of the warp's current cell; per cell of the block's box the count
+    // and moment sums (units of 2^-26) of the particles that end there; the
+    // box's node tile
     __shared__ unsigned mom_lo[kClsWarps][NM][NC], mom_hi[kClsWarps][NM][NC];
-    for (int q = threadIdx.x; q < kClsWarps * NM * NC; q += blockDim.x) {
-        (&mom_lo[0][0][0])[q] = 0u;
-        (&mom_hi[0][0][0])[q] = 0u;
-    }
     __shared__ NodeTile cbox, nbox;
     extern __shared__ __align__(16) unsigned dsm[];
     unsigned* const ct_n = dsm;                             // [CT]
@@ -755,12 +726,16 @@ __global__ void __launch_bounds__(kPicThreads, PSUM_V_P1B) k_cls_pass1(ClsArgs a
     unsigned(*const ct_hi)[CT] = reinterpret_cast<unsigned(*)[CT]>(dsm + CT + (NM - 1) * CT);
     unsigned* const tile_lo = dsm + CT + 2 * (NM - 1) * CT;  // [NT]
     unsigned* const tile_hi = tile_lo + NT;
-    const unsigned ca = a.block_first[blockIdx.x], cb = a.block_first[blockIdx.x + 1];
+    const long long ca = a.block_first[blockIdx.x], cb = a.block_first[blockIdx.x + 1];
     if (ca >= cb) return;
     const GridView& g = a.p.g;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned full = 0xffffffffu;
     if (threadIdx.x == 0) deposit_boxes<D>(g, ca, cb, CT, NT, cbox, nbox);
+    for (int q = threadIdx.x; q < kClsWarps * NM * NC; q += blockDim.x) {
+        (&mom_lo[0][0][0])[q] = 0u;
+        (&mom_hi[0][0][0])[q] = 0u;
+    }
     __syncthreads();
     for (int q = threadIdx.x; q < cbox.vol; q += blockDim.x) {
         ct_n[q] = 0u;
@@ -773,116 +748,102 @@ __global__ void __launch_bounds__(kPicThreads, PSUM_V_P1B) k_cls_pass1(ClsArgs a
 #pragma unroll
     for (int q = 0; q < 2 * D; ++q) lost_cnt[q] = 0u;
     bool far_seen = false;
-    // lane k < NC: count (W[0]) and moment sums of the particles of the
-    // current cell that take move class k
-    unsigned long long W[NM];
-    for (unsigned c = ca + warp; c < cb; c += kClsWarps) {
-        const unsigned p0 = a.starts[c], p1 = a.starts[c + 1];
+    for (long long c = ca + warp; c < cb; c += kClsWarps) {
+        const long long p0 = a.starts[c], p1 = a.starts[c + 1];
         int co[3];
         key_to_cell(g, (int)c, co[0], co[1], co[2]);
-#pragma unroll
-        for (int m = 0; m < NM; ++m) W[m] = 0ull;
         if (p1 > p0) {
-            CellCoef<D> K;
-            cell_coef<D>(a.p, co[0], co[1], co[2], K);
-            const bool edge = edge_cell<D>(g, co);
-            const float* pf[3];
-            const float* pv[3];
-#pragma unroll
-            for (int d = 0; d < D; ++d) pf[d] = a.p.off[d] + p0;
-#pragma unroll
-            for (int q = 0; q < NV; ++q) pv[q] = a.p.vel[q] + p0;
-            const unsigned n = p1 - p0;
-            // stayers: per-lane moment sums (below 2^32 for 32 rounds), reduced every 32 rounds
+            CellField<D> F;
+            load_cell_field<D>(a.p, co[0], co[1], co[2], F);
+            // particles that keep their cell: per-lane count and moment sums
+            // (at most 2^31 over 32 rounds), reduced over the warp every 32 rounds
             unsigned sacc[NM];
 #pragma unroll
             for (int m = 0; m < NM; ++m) sacc[m] = 0u;
-            unsigned stay_n = 0;
             int pending = 0;
-            for (unsigned base = 0; base < n; base += 32 * kClsRounds) {
+            for (long long base = p0; base < p1; base += 32 * kClsRounds) {
                 // all rounds' loads in flight before the first push
                 float f[kClsRounds][3], v[kClsRounds][3];
                 bool live[kClsRounds];
 #pragma unroll
                 for (int r = 0; r < kClsRounds; ++r) {
-                    const unsigned i = base + 32 * r + lane;
-                    live[r] = i < n;
+                    const long long i = base + 32 * r + lane;
+                    live[r] = i < p1;
                     f[r][0] = f[r][1] = f[r][2] = 0.f;
                     v[r][0] = v[r][1] = v[r][2] = 0.f;
                     if (live[r]) {
 #pragma unroll
-                        for (int d = 0; d < D; ++d) f[r][d] = pf[d][i];
+                        for (int d = 0; d < D; ++d) f[r][d] = a.p.off[d][i];
 #pragma unroll
-                        for (int q = 0; q < NV; ++q) v[r][q] = pv[q][i];
+                        for (int q = 0; q < 3; ++q) v[r][q] = a.p.vel[q][i];
                     }
                 }
 #pragma unroll
                 for (int r = 0; r < kClsRounds; ++r) {
-                    const int cls = live[r] ? push_classify<D, PUSHER>(a.p, K, co, edge, f[r], v[r], lost_cnt) : -2;
-                    far_seen |= cls == -1;
-                    const bool stay = cls == STAY, mover = cls >= 0 && !stay;
+                    int cn[3];
+                    const int cls = live[r] ? push_classify<D, PUSHER>(a.p, F, co, f[r], v[r], cn, lost_cnt) : -2;
                     unsigned q[8];
                     cic_moments<D>(f[r], q);
-                    if (stay) {
+                    if (cls == STAY) {
+                        sacc[0] += 1u;
 #pragma unroll
                         for (int m = 1; m < NM; ++m) sacc[m] += q[m];
-                    }
-                    stay_n += (unsigned)__popc(__ballot_sync(full, stay));
-                    if (mover) {   // a few per round, distinct classes mostly
+                    } else if (cls >= 0) {
+                        // mover: a few per round, distinct classes mostly
                         atomicAdd(&mom_lo[warp][0][cls], 1u);
 #pragma unroll
                         for (int m = 1; m < NM; ++m) smem_add64(&mom_lo[warp][m][cls], &mom_hi[warp][m][cls], q[m]);
+                    } else if (cls == -1) {
+                        // far mover: the species is flagged at the end (one atomic per
+                        // warp); the caller redoes its move and its whole deposit
+                        far_seen = true;
                     }
                 }
-                if (++pending == 32 / kClsRounds) {
+                if (++pending == 32 / kClsRounds || base + 32 * kClsRounds >= p1) {
                     pending = 0;
 #pragma unroll
-                    for (int m = 1; m < NM; ++m) {
+                    for (int m = 0; m < NM; ++m) {
                         const unsigned long long t = warp_sum_u32(sacc[m]);
                         sacc[m] = 0u;
-                        if (lane == STAY) W[m] += t;
+                        if (lane == 0) {
+                            const unsigned long long v64 = pair64(mom_lo[warp][m][STAY], mom_hi[warp][m][STAY]) + t;
+                            mom_lo[warp][m][STAY] = (unsigned)v64;
+                            mom_hi[warp][m][STAY] = (unsigned)(v64 >> 32);
+                        }
                     }
                 }
             }
-#pragma unroll
-            for (int m = 1; m < NM; ++m) {
-                const unsigned long long t = warp_sum_u32(sacc[m]);
-                if (lane == STAY) W[m] += t;
-            }
-            if (lane == STAY) W[0] += stay_n;
-            __syncwarp();
-            if (lane < NC && lane != STAY) {
-                W[0] += mom_lo[warp][0][lane];
-                mom_lo[warp][0][lane] = 0u;
-#pragma unroll
-                for (int m = 1; m < NM; ++m) {
-                    W[m] += pair64(mom_lo[warp][m][lane], mom_hi[warp][m][lane]);
-                    mom_lo[warp][m][lane] = mom_hi[warp][m][lane] = 0u;
-                }
-            }
-            __syncwarp();
         }
+        __syncwarp();
         // class lanes: count out, the class's moment sums into its target cell
         if (lane < NC) {
-            const unsigned n = (unsigned)W[0];
-            a.cls[(size_t)lane * a.n_cells + c] = n;
+            const unsigned n = mom_lo[warp][0][lane];
+            a.cls[lane * a.n_cells + c] = n;
             if (n) {
+                mom_lo[warp][0][lane] = 0u;
                 int cn[3];
                 class_target<D>(g, co, lane, cn);   // inside: the class holds no absorbed particle
                 const int sl = box_slot(cbox, cn);
                 if (sl >= 0) {
                     atomicAdd(&ct_n[sl], n);
 #pragma unroll
-                    for (int m = 1; m < NM; ++m) smem_add64(&ct_lo[m - 1][sl], &ct_hi[m - 1][sl], W[m]);
+                    for (int m = 1; m < NM; ++m) {
+                        smem_add64(&ct_lo[m - 1][sl], &ct_hi[m - 1][sl], pair64(mom_lo[warp][m][lane], mom_hi[warp][m][lane]));
+                        mom_lo[warp][m][lane] = mom_hi[warp][m][lane] = 0u;
+                    }
                 } else {
-                    long long Ws[8];
-                    Ws[0] = (long long)n << kCicBits;
+                    long long W[8];
+                    W[0] = (long long)n << kCicBits;
 #pragma unroll
-                    for (int m = 1; m < NM; ++m) Ws[m] = (long long)W[m];
-                    deposit_direct<D>(a.p, cn, Ws);
+                    for (int m = 1; m < NM; ++m) {
+                        W[m] = (long long)pair64(mom_lo[warp][m][lane], mom_hi[warp][m][lane]);
+                        mom_lo[warp][m][lane] = mom_hi[warp][m][lane] = 0u;
+                    }
+                    deposit_direct<D>(a.p, cn, W);
                 }
             }
         }
+        __syncwarp();
     }
 #pragma unroll
     for (int q = 0; q < 2 * D; ++q) {
@@ -899,16 +860,16 @@ __global__ void __launch_bounds__(kPicThreads, PSUM_V_P1B) k_cls_pass1(ClsArgs a
         for (int q = threadIdx.x; q < cbox.vol; q += blockDim.x) {
             const unsigned n = ct_n[q];
             if (n == 0u) continue;
-            long long Ws[8];
-            Ws[0] = (long long)n << kCicBits;
+            long long W[8];
+            W[0] = (long long)n << kCicBits;
 #pragma unroll
-            for (int m = 1; m < NM; ++m) Ws[m] = (long long)pair64(ct_lo[m - 1][q], ct_hi[m - 1][q]);
+            for (int m = 1; m < NM; ++m) W[m] = (long long)pair64(ct_lo[m - 1][q], ct_hi[m - 1][q]);
             const int ti = q / e12, r = q - ti * e12;
             const int tj = r / e2;
             const int cc[3] = {ti + cbox.lo[0], tj + cbox.lo[1], r - tj * e2 + cbox.lo[2]};
 #pragma unroll
             for (int B = 0; B < NM; ++B) {
-                const long long w = cic_corner<D>(Ws, B);
+                const long long w = cic_corner<D>(W, B);
                 if (w == 0) continue;
                 int nd[3];
                 corner_node<D>(g, B, cc, nd);
@@ -1007,7 +968,7 @@ constexpr int kMoverCap = 192;
 // class's run is written in the old particle order.
 // (2D: 48 registers, 5 blocks per SM, for more loads in flight.)
 template <int D, int PUSHER, int kClsRounds>
-__global__ void __launch_bounds__(kPicThreads, D == 2 ? PSUM_V_P2B : 1) k_cls_pass2(ClsArgs a) {
+__global__ void __launch_bounds__(kPicThreads, D == 2 ? 5 : 1) k_cls_pass2(ClsArgs a) {
     constexpr int kMoverFlushAt = kMoverCap - 32 * kClsRounds;
     constexpr int NC = MoveClasses<D>::N;
     constexpr int STAY = MoveClasses<D>::STAY;
@@ -1020,7 +981,7 @@ __global__ void __launch_bounds__(kPicThreads, D == 2 ? PSUM_V_P2B : 1) k_cls_pa
         return;
     }
     double kin = 0.0;   // kinetic energy of the particles this block writes (option "diagnostics 1")
-    const unsigned ca = a.block_first[blockIdx.x], cb = a.block_first[blockIdx.x + 1];
+    const long long ca = a.block_first[blockIdx.x], cb = a.block_first[blockIdx.x + 1];
     const GridView& g = a.p.g;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned full = 0xffffffffu;
@@ -1032,9 +993,9 @@ __global__ void __launch_bounds__(kPicThreads, D == 2 ? PSUM_V_P2B : 1) k_cls_pa
     auto flush = [&](int nm) {
         __syncwarp();
         for (int s0 = 0; s0 < nm; s0 += 32) {
-            const int sl = s0 + lane;
-            const bool has = sl < nm;
-            const int k = has ? mcls[warp][sl] : -1;
+            const int s = s0 + lane;
+            const bool has = s < nm;
+            const int k = has ? mcls[warp][s] : -1;
             const unsigned peers = __match_any_sync(full, k);
             const unsigned p = __shfl_sync(full, mpos, k & 31);
             ccount[warp][lane] = 0u;
@@ -1042,7 +1003,7 @@ __global__ void __launch_bounds__(kPicThreads, D == 2 ? PSUM_V_P2B : 1) k_cls_pa
             if (has) {
                 const unsigned dest = p + (unsigned)__popc(peers & lt);
 #pragma unroll
-                for (int fld = 0; fld < NF; ++fld) out_field(fld)[dest] = mstage[warp][fld][sl];
+                for (int fld = 0; fld < NF; ++fld) out_field(fld)[dest] = mstage[warp][fld][s];
                 if (lane == __ffs(peers) - 1) ccount[warp][k] = (unsigned)__popc(peers);
             }
             __syncwarp();
@@ -1050,8 +1011,8 @@ __global__ void __launch_bounds__(kPicThreads, D == 2 ? PSUM_V_P2B : 1) k_cls_pa
             __syncwarp();
         }
     };
-    for (unsigned c = ca + warp; c < cb; c += kClsWarps) {
-        const unsigned p0 = a.starts[c], p1 = a.starts[c + 1];
+    for (long long c = ca + warp; c < cb; c += kClsWarps) {
+        const long long p0 = a.starts[c], p1 = a.starts[c + 1];
         if (p1 == p0) continue;
         int co[3];
         key_to_cell(g, (int)c, co[0], co[1], co[2]);
@@ -1059,21 +1020,13 @@ __global__ void __launch_bounds__(kPicThreads, D == 2 ? PSUM_V_P2B : 1) k_cls_pa
         if (lane < NC) {
             int cn[3];
             if (class_target<D>(g, co, lane, cn))
-                mpos = __ldg(a.new_starts + cell_to_key(g, cn[0], cn[1], cn[2])) + __ldg(a.cls + (size_t)lane * a.n_cells + c);
+                mpos = __ldg(a.new_starts + cell_to_key(g, cn[0], cn[1], cn[2])) + __ldg(a.cls + lane * a.n_cells + c);
         }
-        CellCoef<D> K;
-        cell_coef<D>(a.p, co[0], co[1], co[2], K);
-        const bool edge = edge_cell<D>(g, co);
-        const float* pf[3];
-        const float* pv[3];
-#pragma unroll
-        for (int d = 0; d < D; ++d) pf[d] = a.p.off[d] + p0;
-#pragma unroll
-        for (int q = 0; q < 3; ++q) pv[q] = a.p.vel[q] + p0;
-        const unsigned n = p1 - p0;
+        CellField<D> F;
+        load_cell_field<D>(a.p, co[0], co[1], co[2], F);
         unsigned stay_next = __shfl_sync(full, mpos, STAY);   // next slot of the class that keeps its cell
         int nm = 0;
-        for (unsigned base = 0; base < n; base += 32 * kClsRounds) {
+        for (long long base = p0; base < p1; base += 32 * kClsRounds) {
             if (nm > kMoverFlushAt) {
                 flush(nm);
                 nm = 0;
@@ -1082,20 +1035,21 @@ __global__ void __launch_bounds__(kPicThreads, D == 2 ? PSUM_V_P2B : 1) k_cls_pa
             bool live[kClsRounds];
 #pragma unroll
             for (int r = 0; r < kClsRounds; ++r) {
-                const unsigned i = base + 32 * r + lane;
-                live[r] = i < n;
+                const long long i = base + 32 * r + lane;
+                live[r] = i < p1;
                 f[r][0] = f[r][1] = f[r][2] = 0.f;
                 v[r][0] = v[r][1] = v[r][2] = 0.f;
                 if (live[r]) {
 #pragma unroll
-                    for (int d = 0; d < D; ++d) f[r][d] = pf[d][i];
+                    for (int d = 0; d < D; ++d) f[r][d] = a.p.off[d][i];
 #pragma unroll
-                    for (int q = 0; q < 3; ++q) v[r][q] = pv[q][i];
+                    for (int q = 0; q < 3; ++q) v[r][q] = a.p.vel[q][i];
                 }
             }
 #pragma unroll
             for (int r = 0; r < kClsRounds; ++r) {
-                const int cls = live[r] ? push_classify<D, PUSHER>(a.p, K, co, edge, f[r], v[r], lost_dummy) : -2;
+                int cn[3];
+                const int cls = live[r] ? push_classify<D, PUSHER>(a.p, F, co, f[r], v[r], cn, lost_dummy) : -2;
                 if (a.p.kin_part && cls >= 0) kin += a.p.kin_hmw * kinetic_v2(v[r]);
                 const unsigned stay = __ballot_sync(full, cls == STAY);
                 if (cls == STAY) {
@@ -1109,15 +1063,16 @@ __global__ void __launch_bounds__(kPicThreads, D == 2 ? PSUM_V_P2B : 1) k_cls_pa
                 const bool mover = cls >= 0 && cls != STAY;
                 const unsigned mb = __ballot_sync(full, mover);
                 if (mb) {
+                    const int cnt = __popc(mb);
                     if (mover) {
-                        const int sl = nm + __popc(mb & lt);
+                        const int slot = nm + __popc(mb & lt);
 #pragma unroll
-                        for (int d = 0; d < D; ++d) mstage[warp][d][sl] = f[r][d];
+                        for (int d = 0; d < D; ++d) mstage[warp][d][slot] = f[r][d];
 #pragma unroll
-                        for (int q = 0; q < 3; ++q) mstage[warp][D + q][sl] = v[r][q];
-                        mcls[warp][sl] = cls;
+                        for (int q = 0; q < 3; ++q) mstage[warp][D + q][slot] = v[r][q];
+                        mcls[warp][slot] = cls;
                     }
-                    nm += __popc(mb);
+                    nm += cnt;
                 }
             }
         }
@@ -1190,9 +1145,9 @@ __global__ void k_state_positions(GridView g, int mixed, const int* __restrict__
 }
 
 // Mixed push with the field's gradient gathered by the caller (grad[d*n_upper + i],
-// per unit length): the scaled gradient of the kick is gs_a * grad_a * dx_a, then
-// the same kick, move and boundary as every mixed push; no deposit (the next
-// step's charge density is the B-spline deposit of the new positions).
+// per unit length): grad_a * dx_a takes the place of the CIC edge difference,
+// then the same kick, move and boundary as every mixed push; no deposit (the
+// next step's charge density is the B-spline deposit of the new positions).
 template <int D, int PUSHER>
 __global__ void __launch_bounds__(kPicThreads) k_push_grad_mixed(PushArgs a, const double* __restrict__ grad,
                                                                  long long n_upper) {
@@ -1208,13 +1163,13 @@ __global__ void __launch_bounds__(kPicThreads) k_push_grad_mixed(PushArgs a, con
             float f[3] = {0.f, 0.f, 0.f}, v[3];
             for (int d = 0; d < D; ++d) f[d] = a.off[d][i];
             for (int q = 0; q < 3; ++q) v[q] = a.vel[q][i];
+            // the gathered gradient times dx is the edge difference the CIC push blends
             float G[3] = {0.f, 0.f, 0.f};
-            for (int d = 0; d < D; ++d) G[d] = (float)((double)a.gs[d] * grad[(long long)d * n_upper + i] * a.g.dx[d]);
-            kick<D, PUSHER>(a, G, v);
+            for (int d = 0; d < D; ++d) G[d] = (float)(grad[(long long)d * n_upper + i] * a.g.dx[d]);
             int dc[3] = {0, 0, 0};
             int nk = -1;
-            if (!move<D>(a, v, f, dc)) {
-                atomicOr(a.err, kErrNonFinite);
+            if (!kick_move<D, PUSHER>(a, G, f, v, dc)) {
+                // non-finite: flagged in the error word by kick_move
             } else {
                 lost = apply_step<D>(a.g, c, dc);
                 if (lost < 0) nk = cell_to_key(a.g, c[0], c[1], c[2]);
@@ -1932,10 +1887,13 @@ static PushArgs make_push_args(psum_pic_ctx* c, Species& sp, int sidx, double dt
     a.edges = c->edges.p;
     const double qm = sp.q / sp.m;
     for (int d = 0; d < 3; ++d) {
-        a.gs[d] = pusher == PSUM_PIC_BORIS ? (float)(-c->g.dr[d] * qm * dt * 0.5) : (float)(-qm * dt * c->g.dr[d]);
+        a.kE[d] = (float)(qm * dt * c->g.dr[d]);
         a.dtdr[d] = (float)(dt * c->g.dr[d]);
+        a.dr[d] = (float)c->g.dr[d];
         a.Bt[d] = (float)((B ? B[d] : 0.0) * qm * dt * 0.5);
     }
+    a.qmdt_half = (float)(qm * dt * 0.5);
+    (void)pusher;
     a.acc = sp.acc.p;
     a.dep_lsh = sp.dep_shift - kCicBits;
     a.losses = c->losses.p + (size_t)sidx * 6;

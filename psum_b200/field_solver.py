@@ -759,6 +759,12 @@ class solver_backend:
         check(lib().psum_mg_hierarchy_info(self._h(), C.byref(lv), C.byref(cr), C.byref(ex)))
         return {"levels": lv.value, "coarse_rows": cr.value, "exception_rows_level0": ex.value}
 
+    def tma_sweeps(self):
+        """Level vectors the TMA-staged sweep kernel has read so far (one tensor map each)."""
+        lv = C.c_int()
+        check(lib().psum_mg_tma_sweeps(self._h(), C.byref(lv)))
+        return lv.value
+
     def free(self):
         if self.handle is not None:
             check(lib().psum_mg_destroy(self.handle))
