@@ -63,6 +63,8 @@ def parse():
                          "c4: the differentiable run (forward and adjoint); bspline: B-spline gather + deposit")
     ap.add_argument("--order", type=int, default=2, help="B-spline order of the bspline workload (1-4)")
     ap.add_argument("--bs-cells", type=int, default=1023, help="cells per axis of the bspline workload")
+    ap.add_argument("--wl-cells", type=int, default=0, help="cells per axis of c1/c3/c5 (default: the workload's)")
+    ap.add_argument("--wl-ppc", type=int, default=0, help="particles per cell of c1/c3 (default: the workload's)")
     ap.add_argument("--mg-extra", default="", help="extra multigrid options (e.g. 'graph 0' to launch the solve's "
                     "kernels one by one, which profilers need)")
     return ap.parse_args()
@@ -612,6 +614,12 @@ def run_workload(args):
     if args.workload == "bspline":
         return run_bspline(args, torch, P)
     w = dict(WORKLOADS[args.workload], name=args.workload)
+    if args.wl_cells:   # a smaller (or larger) box of the same plasma, e.g. for profiler captures
+        w["cells"] = args.wl_cells
+    if args.wl_ppc and "ppc" in w:
+        w["ppc"] = args.wl_ppc
+    if args.wl_cells or args.wl_ppc:
+        w["desc"] += f" [resized: {w['cells'] + 1}^{w['dim']} nodes, {w.get('ppc', '-')} per cell]"
     if args.workload == "c4":
         return run_c4(args, torch, P, w)
     torch.cuda.set_device(0)

@@ -68,6 +68,7 @@ struct DevStencil {
         view.n2 = op.dims[2];
         view.n = op.n;
         view.ns = op.ns;
+        view.any_exc = exceptions > 0;
         view.div12 = make_fastdiv((unsigned)(op.dims[1] * op.dims[2]));
         view.div2 = make_fastdiv((unsigned)op.dims[2]);
         for (int t = 0; t < op.ns && t < kMaxTaps; ++t) {
@@ -113,8 +114,27 @@ struct DevAxis {
 // Launches of the stencil kernels with the operator's tap count as a
 // compile-time constant where it is one of the common ones.
 // 3-D levels of at least this many rows whose rows are a multiple of 16
-// bytes long take the TMA-staged sweep (when the solver's option `tma` is on).
-constexpr long long kTmaMinRows = 1LL << 16;
+// bytes long take the TMA-staged sweep (when the solver's option `tma` is on;
+// option `tma_min_rows` overrides it).  Smaller levels stay in L2, where the
+// per-row kernel's cached reads need no staging.
+constexpr long long kTmaMinRows = 1LL << 22;
+
+// Blocks of a TMA-staged sweep that fit on the GPU at once (SMs x resident
+// blocks of the kernel), cached per kernel.
+template <class T, int Mode, int NS>
+int tma_resident_blocks() {
+    static int blocks = 0;
+    if (!blocks) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+        cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+        cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_level_op_tma<T, Mode, NS>, kTmaThreads,
+                                                                 TmaShape<T>::smem()),
+                   "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+        blocks = std::max(1, sms * std::max(1, per_sm));
+    }
+    return blocks;
+}
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
 // against the driver library).
@@ -166,9 +186,11 @@ struct TmapCache {
     }
 };
 
+// Launch over V's tiles; the planes are cut into as many chunks as keep one
+// wave of resident blocks busy (each chunk re-reads two halo planes).
 template <class T, int Mode, int NS>
-void launch_tma_ns(const CUtensorMap& map, const StencilDev<T>& A, const TmaTile& V, unsigned blocks, const T* x,
-                   const T* b, T* out, T omega, const MGState* st, int* stall, cudaStream_t s) {
+void launch_tma_ns(const CUtensorMap& map, const StencilDev<T>& A, TmaTile V, const T* x, const T* b, T* out,
+                   T omega, const MGState* st, int* stall, cudaStream_t s) {
     static bool attr = false;
     if (!attr) {
         cuda_check(cudaFuncSetAttribute(k_level_op_tma<T, Mode, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -176,42 +198,47 @@ void launch_tma_ns(const CUtensorMap& map, const StencilDev<T>& A, const TmaTile
                    "cudaFuncSetAttribute");
         attr = true;
     }
+    const long long tiles = (long long)V.tiles_c * V.tiles_r;
+    const long long want = std::max(1LL, (long long)tma_resident_blocks<T, Mode, NS>() / tiles);
+    V.chunk = (int)std::max(1LL, (V.P + want - 1) / want);
+    V.chunks = (V.P + V.chunk - 1) / V.chunk;
+    const unsigned blocks = (unsigned)(tiles * V.chunks);
     k_level_op_tma<T, Mode, NS><<<blocks, kTmaThreads, TmaShape<T>::smem(), s>>>(map, A, V, x, b, out, omega, st, stall);
 }
 
 // TMA-staged sweep of a level (k_level_op_tma); false when the level does
 // not qualify (small, not 3-D, or rows not a multiple of 16 bytes).
 template <class T, int Mode>
-bool launch_level_op_tma(TmapCache& cache, const StencilDev<T>& A, const T* x, const T* b, T* out, T omega,
-                         const MGState* st, int* stall, cudaStream_t s) {
+bool launch_level_op_tma(TmapCache& cache, long long min_rows, const StencilDev<T>& A, const T* x, const T* b, T* out,
+                         T omega, const MGState* st, int* stall, cudaStream_t s) {
     using S = TmaShape<T>;
-    if (Mode == kSmoothFromZero || A.n < kTmaMinRows) return false;
+    if (Mode == kSmoothFromZero || A.n < min_rows) return false;
     if (!(A.n0 > 2 && A.n1 > 1 && A.n2 > 1)) return false;          // 3-D boxes only (2-D levels stay in L2)
     if ((A.n2 * (int)sizeof(T)) % 16 != 0) return false;             // tensor-map row pitch: 16-byte multiple
     if ((reinterpret_cast<uintptr_t>(x) & 15) != 0) return false;
+    if (A.ns != 7 && A.ns != 27) return false;                         // the kernel's two stencil shapes
+    for (int t = 0; t < A.ns; ++t)
+        if (A.di[t] != tma_tap_d(A.ns, t, 0) || A.dj[t] != tma_tap_d(A.ns, t, 1) || A.dk[t] != tma_tap_d(A.ns, t, 2))
+            return false;
     TmaTile V{};
     V.P = A.n0;
     V.R = A.n1;
     V.C = A.n2;
-    V.chunk = 32;
     V.tiles_c = (V.C + S::TC - 1) / S::TC;
     V.tiles_r = (V.R + S::TR - 1) / S::TR;
-    V.chunks = (V.P + V.chunk - 1) / V.chunk;
+
     const CUtensorMap& map = cache.get<T>(x, V.P, V.R, V.C);
-    const unsigned blocks = (unsigned)((long long)V.tiles_c * V.tiles_r * V.chunks);
-    if (A.ns == 5) launch_tma_ns<T, Mode, 5>(map, A, V, blocks, x, b, out, omega, st, stall, s);
-    else if (A.ns == 7) launch_tma_ns<T, Mode, 7>(map, A, V, blocks, x, b, out, omega, st, stall, s);
-    else if (A.ns == 9) launch_tma_ns<T, Mode, 9>(map, A, V, blocks, x, b, out, omega, st, stall, s);
-    else if (A.ns == 27) launch_tma_ns<T, Mode, 27>(map, A, V, blocks, x, b, out, omega, st, stall, s);
-    else launch_tma_ns<T, Mode, 0>(map, A, V, blocks, x, b, out, omega, st, stall, s);
+    if (A.ns == 7) launch_tma_ns<T, Mode, 7>(map, A, V, x, b, out, omega, st, stall, s);
+    else launch_tma_ns<T, Mode, 27>(map, A, V, x, b, out, omega, st, stall, s);
     count_launch();
     return true;
 }
 
 template <class T, int Mode>
 void launch_level_op(const StencilDev<T>& A, const T* x, const T* b, T* out, T omega, const MGState* st,
-                     cudaStream_t s, int* stall = nullptr, TmapCache* cache = nullptr) {
-    if (stall && cache && launch_level_op_tma<T, Mode>(*cache, A, x, b, out, omega, st, stall, s)) return;
+                     cudaStream_t s, int* stall = nullptr, TmapCache* cache = nullptr,
+                     long long tma_min_rows = kTmaMinRows) {
+    if (stall && cache && launch_level_op_tma<T, Mode>(*cache, tma_min_rows, A, x, b, out, omega, st, stall, s)) return;
     const unsigned g = grid_for(A.n);
     if (Mode == kSmoothFromZero) k_level_op<T, Mode, 0><<<g, kThreads, 0, s>>>(A, x, b, out, omega, st);
     else if (A.ns == 5) k_level_op<T, Mode, 5><<<g, kThreads, 0, s>>>(A, x, b, out, omega, st);
@@ -261,6 +288,7 @@ struct SolverBase {
     bool ns_built = false;                  // the hierarchy was built for a singular operator
     int use_graph = 1;                      // option `graph 0|1`: replay the solve as one CUDA graph
     int use_tma = 1;                        // option `tma 0|1`: TMA-staged sweeps on large levels
+    long long tma_min_rows = kTmaMinRows;   // option `tma_min_rows`: smallest level (rows) swept that way
     unsigned long long n_row = 0;
     bool ready = false;
     cudaStream_t own_stream = nullptr;
@@ -376,7 +404,7 @@ struct Solver : SolverBase {
                 launch_level_op<T, kSmoothFromZero>(V.op.view, xcur[l], bl[l], xoth[l], omega, st, s);
                 zero[l] = false;
             } else {
-                launch_level_op<T, kSmooth>(V.op.view, xcur[l], bl[l], xoth[l], omega, st, s, tma_stall(), &tmaps);
+                launch_level_op<T, kSmooth>(V.op.view, xcur[l], bl[l], xoth[l], omega, st, s, tma_stall(), &tmaps, tma_min_rows);
             }
             std::swap(xcur[l], xoth[l]);
         };
@@ -389,7 +417,7 @@ struct Solver : SolverBase {
                     { k_restrict<T><<<grid_for(lv[l + 1]->n), kThreads, 0, s>>>(V.xfer, bl[l], bl[l + 1], xcur[l + 1],
                                                                              lv[l + 1]->dinv.p, st); count_launch(); }
                 } else {
-                    launch_level_op<T, kResidual>(V.op.view, xcur[l], bl[l], xoth[l], omega, st, s, tma_stall(), &tmaps);
+                    launch_level_op<T, kResidual>(V.op.view, xcur[l], bl[l], xoth[l], omega, st, s, tma_stall(), &tmaps, tma_min_rows);
                     { k_restrict<T><<<grid_for(lv[l + 1]->n), kThreads, 0, s>>>(V.xfer, xoth[l], bl[l + 1],
                                                                              xcur[l + 1], lv[l + 1]->dinv.p, st); count_launch(); }
                 }
@@ -590,6 +618,11 @@ void solver_set_options(SolverBase* s, const char* options) {
         else if (key == "periodic_K") s->periodic[2] = parse_int(iss, key) != 0;
         else if (key == "graph") s->use_graph = parse_int(iss, key) != 0;
         else if (key == "tma") s->use_tma = parse_int(iss, key) != 0;
+        else if (key == "tma_min_rows") {
+            long long v = 0;
+            if (!(iss >> v) || v < 1) throw std::invalid_argument("tma_min_rows must be positive");
+            s->tma_min_rows = v;
+        }
         else if (key == "null_space") s->null_space = parse_int(iss, key) != 0;
         else if (key == "correction_interval") {
             int v = 0;

@@ -43,6 +43,7 @@ struct StencilDev {
     int n0, n1, n2;
     long long n;            // rows (below 2^31)
     int ns;
+    int any_exc;            // some row is an exception row (mask has a bit set)
     signed char di[kMaxTaps], dj[kMaxTaps], dk[kMaxTaps];
     int off[kMaxTaps];      // linear offset of each tap on interior rows
     T c[kMaxTaps];
@@ -162,10 +163,13 @@ __global__ void __launch_bounds__(kThreads) k_level_op(StencilDev<T> A, const T*
 // (zero-filled by the copy) are patched from global memory with the
 // stencil's own wrap (PSuM's cyclic neighbour rule), corners included.
 // Planes p-1, p, p+1 are resident while p is computed and p+2, p+3 are in
-// flight; one block barrier per plane orders the refill of the slot of p-2.
+// flight; thread 0 waits on the mbarriers and one block barrier per plane
+// (two on edge tiles, around the halo patch) passes the planes on and orders
+// the refill of the slot of p-2.
 // Taps are summed in the same order as stencil_row, and exception rows take
 // the same CSR path, so the results are bit-identical to k_level_op.  b is
-// read and out written directly (each once, coalesced).  Every mbarrier wait
+// read one plane ahead into registers and out written directly (each once,
+// coalesced).  Every mbarrier wait
 // is bounded: after 2^16 suspended polls the block records a stall in
 // *stall, and once a stall is recorded later waits return at once, so a
 // wrong byte count cannot hang the GPU.  The tensor map covers only the
@@ -175,6 +179,17 @@ struct TmaTile {
     int tiles_c, tiles_r;
     int chunk, chunks;    // planes per block, blocks along the planes
 };
+
+// The two 3-D stencil shapes the TMA-staged sweep takes, with their taps in
+// the order the host's stencil extraction sorts them (by (di, dj, dk)) and
+// stencil_row sums them: the 7-point fine operator and the 27-point
+// Galerkin coarse operator.  The launcher checks the level's taps against
+// these; any other shape keeps the per-row kernel.
+__host__ __device__ constexpr int tma_tap_d(int ns, int t, int axis) {
+    return ns == 27 ? (axis == 0 ? t / 9 : (axis == 1 ? (t / 3) % 3 : t % 3)) - 1
+                    : (axis == 0 ? (t == 0 ? -1 : (t == 6 ? 1 : 0))
+                                 : (axis == 1 ? (t == 1 ? -1 : (t == 5 ? 1 : 0)) : (t == 2 ? -1 : (t == 4 ? 1 : 0))));
+}
 
 constexpr int kTmaThreads = 256;
 constexpr int kTmaSlots = 5;
@@ -238,7 +253,7 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const void* tmap, int x, 
 }
 
 template <class T, int Mode, int NS>
-__global__ void __launch_bounds__(kTmaThreads) k_level_op_tma(const __grid_constant__ CUtensorMap xmap, StencilDev<T> A,
+__global__ void __launch_bounds__(kTmaThreads, 4) k_level_op_tma(const __grid_constant__ CUtensorMap xmap, StencilDev<T> A,
                                                               TmaTile V, const T* __restrict__ x,
                                                               const T* __restrict__ b, T* __restrict__ out, T omega,
                                                               const MGState* __restrict__ st, int* stall) {
@@ -275,60 +290,103 @@ __global__ void __launch_bounds__(kTmaThreads) k_level_op_tma(const __grid_const
         tma_load_3d(ring + (size_t)slot * SLOT, &xmap, c0 - KA, r0 - 1, plane_of(L), &bar[slot]);
     };
     auto wrapi = [](int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); };
-    // halo cells the box could not read: row -1 / row R and column -1 / column C, wrapped
+    // halo cells the box could not read, wrapped: row -1 (first row tile),
+    // row R (last row tile), column -1 (first column tile), column C (last
+    // column tile); corners belong to both a row and a column and are written
+    // twice with the same value
+    const bool top = r0 == 0, bottom = r0 + TR >= V.R, left = c0 == 0, right = c0 + TC >= V.C;
+    const int lr_bottom = V.R - r0 + 1, k_right = V.C - c0 + 1;   // box row of row R, box column of column C (+1)
     auto patch = [&](int L) {
         if (!edge) return;
         T* slot = ring + (size_t)(L % NSL) * SLOT;
         const long long pbase = (long long)plane_of(L) * V.R;
-        for (int e = threadIdx.x; e < H * (TC + 2); e += blockDim.x) {
-            const int lr = e / (TC + 2), k = e % (TC + 2);
+        auto put = [&](int lr, int k) {   // box row lr (row r0 - 1 + lr), column c0 - 1 + k
             const int r = r0 - 1 + lr, c = c0 - 1 + k;
-            if (r > V.R || c > V.C) continue;                               // beyond the halo: never read
-            if (r >= 0 && r < V.R && c >= 0 && c < V.C) continue;           // inside the box: the copy read it
-            slot[lr * W + (c - (c0 - KA))] = x[(pbase + wrapi(r, V.R)) * V.C + wrapi(c, V.C)];
-        }
+            slot[lr * W + k - 1 + KA] = x[(pbase + wrapi(r, V.R)) * V.C + wrapi(c, V.C)];
+        };
+        const int t = threadIdx.x;
+        const int kmax = min(TC + 2, k_right + 1);   // columns up to column C
+        const int lmax = min(H, lr_bottom + 1);      // rows up to row R
+        if (top)
+            for (int k = t; k < kmax; k += kTmaThreads) put(0, k);
+        if (bottom)
+            for (int k = t; k < kmax; k += kTmaThreads) put(lr_bottom, k);
+        if (left)
+            for (int lr = t; lr < lmax; lr += kTmaThreads) put(lr, 0);
+        if (right)
+            for (int lr = t; lr < lmax; lr += kTmaThreads) put(lr, k_right);
     };
     if (threadIdx.x == 0)
         for (int L = 0; L < min(NSL - 1, nlocal); ++L) issue(L);
+    // each thread owns PER points of the tile (rows lr0 + 2u, column cc): their
+    // b values and exception-mask words are loaded one plane ahead, so the
+    // loads are in flight while the previous plane is computed
+    constexpr int PER = TR * TC / kTmaThreads;
+    static_assert(PER * kTmaThreads == TR * TC && kTmaThreads % TC == 0, "tile / block shape");
+    constexpr int RSTEP = kTmaThreads / TC;
+    const int lr0 = threadIdx.x / TC + 1, cc = threadIdx.x % TC;
+    const int c = c0 + cc;
+    const bool any_exc = A.any_exc != 0;
+    // points u < nu of this thread lie inside the level (rows r0 + lr0 - 1 + u * RSTEP, column c)
+    const int rfirst = r0 + lr0 - 1;
+    const int nu = c < V.C && rfirst < V.R ? min(PER, (V.R - rfirst + RSTEP - 1) / RSTEP) : 0;
+    const long long ustride = (long long)RSTEP * V.C;
+    const int at0 = lr0 * W + cc + KA;   // this thread's first point in a slot; point u is RSTEP * W further
+    T bnext[PER];
+    auto prefetch = [&](int p) {
+        const T* bp = b + ((long long)p * V.R + rfirst) * V.C + c;
+#pragma unroll
+        for (int u = 0; u < PER; ++u) bnext[u] = u < nu ? __ldg(bp + u * ustride) : T(0);
+    };
+    static_assert(NS == 7 || NS == 27, "TMA-staged sweeps take the 7- and 27-point shapes");
     const int planes = pb - pa;
+    prefetch(pa);
     for (int j = 0; j < planes; ++j) {
-        // local planes j, j + 1, j + 2 (planes p - 1, p, p + 1) must have landed
-        for (int L = j == 0 ? 0 : j + 2; L <= j + 2; ++L) {
-            mbar_wait_bounded(&bar[L % NSL], (unsigned)((L / NSL) & 1), stall);
-            patch(L);
-        }
-        __syncthreads();   // every thread is done with plane j - 1's slot and sees the patches
-        if (threadIdx.x == 0 && j + NSL - 1 < nlocal) issue(j + NSL - 1);   // refills the slot of local j - 1
         const int p = pa + j;
-        const T* const sm = ring + (size_t)(j % NSL) * SLOT;
-        const T* const s0 = ring + (size_t)((j + 1) % NSL) * SLOT;
-        const T* const sp = ring + (size_t)((j + 2) % NSL) * SLOT;
-        for (int e = threadIdx.x; e < TR * TC; e += blockDim.x) {
-            const int lr = e / TC + 1, cc = e % TC;
-            const int rr = r0 + lr - 1, c = c0 + cc;
-            if (rr >= V.R || c >= V.C) continue;
-            const long long row = ((long long)p * V.R + rr) * V.C + c;   // global row index of the level
-            const int at = lr * W + cc + KA;                                 // (lr, c) in a slot
-            constexpr int NT = NS > 0 ? NS : kMaxTaps;
+        T bcur[PER];
+#pragma unroll
+        for (int u = 0; u < PER; ++u) bcur[u] = bnext[u];
+        if (j + 1 < planes) prefetch(p + 1);
+        // local planes j, j + 1, j + 2 (planes p - 1, p, p + 1) must have
+        // landed: thread 0 waits (one poller instead of a block of them), the
+        // block barrier passes the completed copies on to every thread
+        const int Lfirst = j == 0 ? 0 : j + 2;
+        if (threadIdx.x == 0)
+            for (int L = Lfirst; L <= j + 2; ++L) mbar_wait_bounded(&bar[L % NSL], (unsigned)((L / NSL) & 1), stall);
+        __syncthreads();   // planes landed; every thread is done with plane j - 1's slot
+        if (edge) {
+            for (int L = Lfirst; L <= j + 2; ++L) patch(L);
+            __syncthreads();
+        }
+        if (threadIdx.x == 0 && j + NSL - 1 < nlocal) issue(j + NSL - 1);   // refills the slot of local j - 1
+        // ring index of this thread's first point in the slots of planes p - 1, p, p + 1
+        const int bm = (j % NSL) * SLOT + at0, b0 = ((j + 1) % NSL) * SLOT + at0, bp = ((j + 2) % NSL) * SLOT + at0;
+        const long long row0 = ((long long)p * V.R + rfirst) * V.C + c;   // global row index of point 0
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+            if (u >= nu) break;
+            const int du = u * (RSTEP * W);
+            const long long row = row0 + u * ustride;
             T s = T(0);
 #pragma unroll
-            for (int t = 0; t < NT; ++t) {
-                if (NS > 0 || t < A.ns) {
-                    const T* pl = A.di[t] < 0 ? sm : (A.di[t] > 0 ? sp : s0);
-                    s += A.c[t] * pl[at + A.dj[t] * W + A.dk[t]];
+            for (int t = 0; t < NS; ++t) {
+                const int di = tma_tap_d(NS, t, 0);
+                const int base = di < 0 ? bm : (di > 0 ? bp : b0);
+                s += A.c[t] * ring[base + tma_tap_d(NS, t, 1) * W + tma_tap_d(NS, t, 2) + du];
+            }
+            if (any_exc) {
+                const int r32 = (int)row;
+                const uint32_t word = __ldg(A.mask + (r32 >> 5));
+                const uint32_t bit = 1u << (r32 & 31);
+                if (word & bit) {
+                    const int q = (int)__ldg(A.mask_prefix + (r32 >> 5)) + __popc(word & (bit - 1u));
+                    const int b0 = __ldg(A.exc_ptr + q), e0 = __ldg(A.exc_ptr + q + 1);
+                    s = T(0);
+                    for (int t = b0; t < e0; ++t) s += __ldg(A.exc_val + t) * __ldg(x + __ldg(A.exc_col + t));
                 }
             }
-            const int r32 = (int)row;
-            const uint32_t word = __ldg(A.mask + (r32 >> 5));
-            const uint32_t bit = 1u << (r32 & 31);
-            if (word & bit) {
-                const int q = (int)__ldg(A.mask_prefix + (r32 >> 5)) + __popc(word & (bit - 1u));
-                const int b0 = __ldg(A.exc_ptr + q), e0 = __ldg(A.exc_ptr + q + 1);
-                s = T(0);
-                for (int t = b0; t < e0; ++t) s += __ldg(A.exc_val + t) * __ldg(x + __ldg(A.exc_col + t));
-            }
-            if (Mode == kSmooth) out[row] = s0[at] + omega * (__ldg(b + row) - s);
-            else out[row] = __ldg(b + row) - s;
+            if (Mode == kSmooth) out[row] = ring[b0 + du] + omega * (bcur[u] - s);
+            else out[row] = bcur[u] - s;
         }
     }
     // every issued plane was waited on: nothing is in flight at exit

@@ -9,7 +9,10 @@ Over one checkpoint segment (10 steps) central differences with eps = 1e-3
 stay on one smooth piece for most probes, and the FP64 adjoint must agree
 with them to 1e-4 (probes whose perturbed runs change a cell sequence are
 counted, not compared); the mixed adjoint too, against the FP64 forward's
-differences.  Over the full 100 steps the perturbed runs of eps = 1e-3 change
+differences.  The differences' O(eps^2) truncation reaches about 1e-4 on the
+largest components (measured 1.1e-4): a probe above the bound is compared
+through the Richardson value of eps and eps / 2, after checking that halving
+eps moves the difference towards the adjoint.  Over the full 100 steps the perturbed runs of eps = 1e-3 change
 thousands of crossings (measured: differences far from any derivative), so
 the full run is checked for the consistency of its two adjoints (loss to
 1e-5, gradients to 5e-3 relative L2, measured 2e-3), and its velocity probes
@@ -118,10 +121,22 @@ def _probe_fd(run64, vel, phi_ext, gv64, gp64, gv32, gp32, n, eps, nv, npot, see
             crossing += 1
             continue
         smooth += 1
-        worst64 = max(worst64, abs(d - g64) / scale)
-        worst32 = max(worst32, abs(d - g32) / scale)
-        assert abs(d - g64) <= tol64 * scale, (which, idx, d, g64)
-        assert abs(d - g32) <= tol32 * scale, (which, idx, d, g32)
+        e64, e32 = abs(d - g64), abs(d - g32)
+        if max(e64 - tol64 * scale, e32 - tol32 * scale) > 0:
+            # above the bound: the central difference's own O(eps^2) truncation must be what is left, i.e. the
+            # difference at eps / 2 moves towards the adjoint (by 4x without noise; at least 2x asked) and the
+            # Richardson value (4 D(eps/2) - D(eps)) / 3 is within the bound
+            dh, same_h = fd(run64, vel, phi_ext, which, idx, eps / 2)
+            assert same_h
+            rich = (4 * dh - d) / 3
+            print(f"probe {which} {idx}: D(eps) {d:.9e}, D(eps/2) {dh:.9e}, Richardson {rich:.9e}, "
+                  f"FP64 adjoint {g64:.9e}, mixed {g32:.9e}")
+            assert abs(dh - g64) <= 0.5 * e64 or abs(dh - g64) <= tol64 * scale, (which, idx, d, dh, g64)
+            e64, e32 = abs(rich - g64), abs(rich - g32)
+        worst64 = max(worst64, e64 / scale)
+        worst32 = max(worst32, e32 / scale)
+        assert e64 <= tol64 * scale, (which, idx, d, g64)
+        assert e32 <= tol32 * scale, (which, idx, d, g32)
     return smooth, crossing, worst64, worst32
 
 

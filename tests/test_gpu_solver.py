@@ -416,8 +416,8 @@ def test_1d_operators_multigrid_match_direct(kind):
 @pytest.mark.parametrize("kind", ["cuda_multigrid64_gpu", "cuda_multigrid32f_gpu"])
 @pytest.mark.parametrize("case", ["3d_dirichlet_128", "3d_periodic_128", "3d_odd_65x70x92", "3d_dirichlet_129"])
 def test_tma_staged_sweeps_equal_per_row_sweeps(kind, case):
-    """3-D levels of 2^16 rows and more whose rows are a multiple of 16 bytes long are swept by the TMA-staged
-    kernel (one cp.async.bulk.tensor.3d box per tile and plane into a shared-memory plane ring); option `tma 0`
+    """3-D levels of 2^16 rows and more (option tma_min_rows; 2^22 by default) whose rows are a multiple of 16 bytes
+    long are swept by the TMA-staged kernel (one cp.async.bulk.tensor.3d box per tile and plane into a shared-memory plane ring); option `tma 0`
     keeps the per-row kernel.  Same taps in the same order: the iterates are identical.  129-node rows are not
     16-byte multiples: that box keeps the per-row kernel on every level."""
     if case in ("3d_dirichlet_128", "3d_dirichlet_129"):
@@ -446,7 +446,7 @@ def test_tma_staged_sweeps_equal_per_row_sweeps(kind, case):
     outs, maps = [], []
     for tma in (1, 0):
         s = P.solver_backend(kind)
-        s.set_options(f"{opts} tma {tma}")
+        s.set_options(f"{opts} tma {tma} tma_min_rows 65536")
         s.set_matrix(n, n, r.size, r, c, v)
         bd, xd = dev(b), dev(x0)
         assert s.solve(bd, xd) in (0, 4)   # fixed cycle count, no tol: never a stall
@@ -461,7 +461,8 @@ def test_tma_staged_fp64_vcycles_match_oracle():
     """The FP64 V-cycles on a 48^3-node periodic box (TMA-staged sweeps on the finest level) equal the oracle's."""
     g, r, c, v, n, b = periodic_case(3, 48, seed=11)
     s = P.solver_backend("cuda_multigrid64_gpu")
-    s.set_options("I 48 J 48 K 48 depth 3 pre_relax 2 post_relax 1 max_cycles 3 periodic_I 1 periodic_J 1 periodic_K 1")
+    s.set_options("I 48 J 48 K 48 depth 3 pre_relax 2 post_relax 1 max_cycles 3 periodic_I 1 periodic_J 1 periodic_K 1 "
+                  "tma_min_rows 65536")
     s.set_matrix(n, n, r.size, r, c, v)
     x0 = np.random.default_rng(12).normal(size=n) * 0.1
     bd, xd = dev(b), dev(x0)
