@@ -117,7 +117,7 @@ struct DevAxis {
 // bytes long take the TMA-staged sweep (when the solver's option `tma` is on;
 // option `tma_min_rows` overrides it).  Smaller levels stay in L2, where the
 // per-row kernel's cached reads need no staging.
-constexpr long long kTmaMinRows = 1LL << 22;
+constexpr long long kTmaMinRows = 1LL << 20;
 
 // Blocks of a TMA-staged sweep that fit on the GPU at once (SMs x resident
 // blocks of the kernel), cached per kernel.

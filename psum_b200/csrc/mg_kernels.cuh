@@ -197,7 +197,7 @@ constexpr int kTmaSlots = 5;
 template <class T>
 struct TmaShape {
     static constexpr int TC = sizeof(T) == 4 ? 128 : 64;   // columns per tile (512 bytes)
-    static constexpr int TR = 16;                           // rows per tile
+    static constexpr int TR = 8;                            // rows per tile
     static constexpr int KA = 16 / (int)sizeof(T);          // elements per 16 bytes: the column halo of the box
     static constexpr int W = TC + 2 * KA;                   // box columns (multiple of 16 bytes)
     static constexpr int H = TR + 2;                        // box rows

@@ -2247,6 +2247,14 @@ static void finish_cls_step(psum_pic_ctx* c) {
     cuda_check(cudaEventSynchronize(c->ev_pass1), "far flag wait");
     const int ns = (int)c->sp.size();
     bool redo_diag = false;   // a fallback rewrote a species' energy sums: the side stream's reduction is stale
+    bool any_far = false;
+    for (int si = 0; si < ns && si < 8; ++si) any_far |= c->sp[si]->n > 0 && c->far_host[si] != 0;
+    if (any_far) {
+        c->fused_skip = c->fused_backoff;
+        c->fused_backoff = std::min(64, 2 * c->fused_backoff);
+    } else {
+        c->fused_backoff = 1;
+    }
     for (int si = 0; si < ns; ++si) {
         Species& sp = *c->sp[si];
         if (sp.n <= 0) continue;
@@ -3048,6 +3056,10 @@ EXPORT int psum_pic_step(psum_pic_ctx* ctx, psum_field_solver_handle solver, dou
         bool fused = ctx->precision == PSUM_PIC_MIXED && ctx->sort_interval == 1 && cls_step_applies(ctx) &&
                      ctx->interp_order == 1;
         for (auto& sp : ctx->sp) fused = fused && (sp->sorted || sp->n == 0);
+        if (fused && ctx->fused_skip > 0) {   // far movers in a recent fused step: the general path for now
+            ctx->fused_skip--;
+            fused = false;
+        }
         if (pusher != PSUM_PIC_LEAPFROG && pusher != PSUM_PIC_BORIS) throw std::invalid_argument("step: unknown pusher");
         if (fused) {
             // push, deposit and re-sort in the two passes of the fused step (timed by cls_step)

@@ -84,6 +84,13 @@ struct psum_pic_ctx {
     int pend_pusher = 0;
     bool pend_has_B = false;
     double pend_B[3] = {0, 0, 0};
+    // After a fused step in which a particle moved more than one cell (its
+    // species then took the in-place push and full re-sort), the next
+    // fused_skip steps go straight to the general path instead of paying a
+    // first pass that would be thrown away again; the skip doubles while the
+    // far movers persist (up to 64 steps) and resets after a clean step.
+    int fused_skip = 0;
+    int fused_backoff = 1;
     int sort_interval = 1;
     bool fp64_fma = false;                    // FP64 mode: the contracted kernel build (not bit-exact)
     // option "interp_order k" (2-4): the step deposits and gathers with PSuM's B-spline weights of order k

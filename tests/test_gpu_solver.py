@@ -416,7 +416,7 @@ def test_1d_operators_multigrid_match_direct(kind):
 @pytest.mark.parametrize("kind", ["cuda_multigrid64_gpu", "cuda_multigrid32f_gpu"])
 @pytest.mark.parametrize("case", ["3d_dirichlet_128", "3d_periodic_128", "3d_odd_65x70x92", "3d_dirichlet_129"])
 def test_tma_staged_sweeps_equal_per_row_sweeps(kind, case):
-    """3-D levels of 2^16 rows and more (option tma_min_rows; 2^22 by default) whose rows are a multiple of 16 bytes
+    """3-D levels of 2^16 rows and more (option tma_min_rows; 2^20 by default) whose rows are a multiple of 16 bytes
     long are swept by the TMA-staged kernel (one cp.async.bulk.tensor.3d box per tile and plane into a shared-memory plane ring); option `tma 0`
     keeps the per-row kernel.  Same taps in the same order: the iterates are identical.  129-node rows are not
     16-byte multiples: that box keeps the per-row kernel on every level."""
