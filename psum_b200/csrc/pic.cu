@@ -1717,6 +1717,24 @@ __device__ double block_fixed_sum(const double* __restrict__ v, long long n) {
     return red[0];
 }
 
+// First level of the diagnostics reduction: block (x, y) sums slice x of
+// array y (y < ns: species y's kinetic partials; ns: the field-energy
+// partials; ns + 1: the density partials) in fixed order into
+// stage[y * kDiagStageBlocks + x], so the one-block finisher reads only
+// kDiagStageBlocks values per array.
+constexpr int kDiagStageBlocks = 128;
+
+__global__ void __launch_bounds__(kDiagFinishThreads) k_diag_stage(DiagFinishArgs a, double* __restrict__ stage) {
+    const int y = blockIdx.y;
+    const double* v = y < a.ns ? a.kin_part[y] : (y == a.ns ? a.fe_part : a.rho_part);
+    const long long n = y < a.ns ? a.kin_n[y] : (y == a.ns ? a.fe_n : a.rho_n);
+    if (!v) return;
+    const long long len = (n + kDiagStageBlocks - 1) / kDiagStageBlocks;
+    const long long lo = min((long long)blockIdx.x * len, n), hi = min(lo + len, n);
+    const double t = block_fixed_sum(v + lo, hi - lo);
+    if (threadIdx.x == 0) stage[(long long)y * kDiagStageBlocks + blockIdx.x] = t;
+}
+
 __global__ void __launch_bounds__(kDiagFinishThreads) k_diag_finish(DiagFinishArgs a) {
     for (int s = 0; s < a.ns; ++s) {
         const double k = a.kin_part[s] ? block_fixed_sum(a.kin_part[s], a.kin_n[s]) : 0.0;
@@ -2332,6 +2350,7 @@ static void ensure_diag_buffers(psum_pic_ctx* c) {
     }
     grow(d.kin, (size_t)std::max<long long>(off, 1));
     grow(d.qsum, 8);
+    grow(d.stage, (size_t)kDiagStageBlocks * 10);
     grow(c->diag_out, 16);
     d.fe_n = 0;
     d.rho_n = 0;
@@ -2359,7 +2378,19 @@ static void finish_diagnostics(psum_pic_ctx* c, int par) {
     a.rho_n = d.rho_n;
     a.rho_coef = vol;
     a.out = c->diag_out.p;
-    { k_diag_finish<<<1, kDiagFinishThreads, 0, c->stream>>>(a); count_launch(); }
+    // two levels: slices of every partial array, then the slices' sums
+    double* stage = c->dbuf[par].stage.p;
+    { k_diag_stage<<<dim3(kDiagStageBlocks, a.ns + 2), kDiagFinishThreads, 0, c->stream>>>(a, stage); count_launch(); }
+    DiagFinishArgs b = a;
+    for (int s = 0; s < a.ns; ++s) {
+        b.kin_part[s] = a.kin_part[s] ? stage + (long long)s * kDiagStageBlocks : nullptr;
+        b.kin_n[s] = a.kin_part[s] ? kDiagStageBlocks : 0;
+    }
+    b.fe_part = a.fe_part ? stage + (long long)a.ns * kDiagStageBlocks : nullptr;
+    b.fe_n = a.fe_part ? kDiagStageBlocks : 0;
+    b.rho_part = a.rho_part ? stage + (long long)(a.ns + 1) * kDiagStageBlocks : nullptr;
+    b.rho_n = a.rho_part ? kDiagStageBlocks : 0;
+    { k_diag_finish<<<1, kDiagFinishThreads, 0, c->stream>>>(b); count_launch(); }
     cuda_check(cudaGetLastError(), "diagnostics launch");
 }
 

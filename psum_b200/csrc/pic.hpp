@@ -108,6 +108,7 @@ struct psum_pic_ctx {
         psum_b200::DevBuf<double> fe, kin;
         psum_b200::DevBuf<unsigned long long> qsum;
         psum_b200::DevBuf<double> rho_part;   // B-spline steps: per-block sums of rho - background
+        psum_b200::DevBuf<double> stage;      // first-level sums of the partial arrays (k_diag_stage)
         long long rho_n = 0;
         long long fe_n = 0;
         long long kin_n[8] = {0, 0, 0, 0, 0, 0, 0, 0};
