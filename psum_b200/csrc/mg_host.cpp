@@ -191,7 +191,20 @@ Axis1D identity_axis(int n) {
     return ax;
 }
 
+inline int wrap_delta(int d, int n) {
+    // minimal periodic image of an index difference on an axis of n nodes
+    if (n <= 1) return d;
+    if (d > 1 && d == n - 1) return -1;
+    if (d < -1 && d == -(n - 1)) return 1;
+    return d;
+}
+
 // ---- Galerkin product R * Ahat * P with the tensor-product transfers ----
+// Each fine row's entries are taken in the order of their (wrapped) offsets,
+// not of their column indices, so that rows equal up to a translation --
+// the rows beside a periodic seam included -- sum in the same order and
+// give bit-identical coarse rows (the stencil decomposition then finds no
+// exception rows on uniform periodic lattices).
 HostCSR galerkin(const HostCSR& ahat, const std::array<int, 3>& fd, const std::array<Axis1D, 3>& ax) {
     const std::array<int, 3> cd{ax[0].nc, ax[1].nc, ax[2].nc};
     const long long nc = (long long)cd[0] * cd[1] * cd[2];
@@ -204,6 +217,7 @@ HostCSR galerkin(const HostCSR& ahat, const std::array<int, 3>& fd, const std::a
         std::unordered_map<long long, double> acc;
         acc.reserve(256);
         std::vector<std::pair<long long, double>> tmp;
+        std::vector<std::pair<long long, long long>> ent;   // (offset order, CSR position) of a fine row's entries
 #pragma omp for schedule(dynamic, 1024)
         for (long long c = 0; c < nc; ++c) {
             acc.clear();
@@ -221,7 +235,19 @@ HostCSR galerkin(const HostCSR& ahat, const std::array<int, 3>& fd, const std::a
                         if (fk < 0) continue;
                         const double wr = ax[0].r_w[3 * ci + qa] * ax[1].r_w[3 * cj + qb] * ax[2].r_w[3 * ck + qc];
                         const long long f = ((long long)fi * fd[1] + fj) * fd[2] + fk;
+                        ent.clear();
                         for (long long k = ahat.ptr[f]; k < ahat.ptr[f + 1]; ++k) {
+                            const long long g = ahat.col[k];
+                            const int di = wrap_delta(int(g / ((long long)fd[1] * fd[2])) - fi, fd[0]);
+                            const int dj = wrap_delta(int((g / fd[2]) % fd[1]) - fj, fd[1]);
+                            const int dk = wrap_delta(int(g % fd[2]) - fk, fd[2]);
+                            const bool near = di >= -1 && di <= 1 && dj >= -1 && dj <= 1 && dk >= -1 && dk <= 1;
+                            // offsets within one node first (by offset code), any others after, by column
+                            ent.push_back({near ? (di + 1) * 9 + (dj + 1) * 3 + (dk + 1) : 27 + (k - ahat.ptr[f]), k});
+                        }
+                        std::sort(ent.begin(), ent.end());
+                        for (const auto& [order, k] : ent) {
+                            (void)order;
                             const long long g = ahat.col[k];
                             const double a = wr * ahat.val[k];
                             const int gi = int(g / ((long long)fd[1] * fd[2]));
@@ -330,13 +356,6 @@ std::vector<double> dense_inverse(const HostCSR& a, double shift = 0.0) {
     return inv;
 }
 
-inline int wrap_delta(int d, int n) {
-    // minimal periodic image of an index difference on an axis of n nodes
-    if (n <= 1) return d;
-    if (d > 1 && d == n - 1) return -1;
-    if (d < -1 && d == -(n - 1)) return 1;
-    return d;
-}
 
 struct RowPattern {
     std::vector<std::pair<int, double>> e;  // (delta code, value) sorted by code

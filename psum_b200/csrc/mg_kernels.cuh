@@ -88,7 +88,7 @@ __device__ __forceinline__ T ldv(const T* p) {
 
 template <class T, class Acc, int NS, bool RO = true>
 __device__ __forceinline__ Acc stencil_row(const StencilDev<T>& A, const T* __restrict__ x, int r) {
-    const uint32_t word = __ldg(A.mask + (r >> 5));
+    const uint32_t word = A.any_exc ? __ldg(A.mask + (r >> 5)) : 0u;
     const int i = (int)fastdiv((unsigned)r, A.div12);
     const int rem = r - i * (int)A.div12.d;
     const int j = (int)fastdiv((unsigned)rem, A.div2);
@@ -332,21 +332,26 @@ __global__ void __launch_bounds__(kTmaThreads, 4) k_level_op_tma(const __grid_co
     const int nu = c < V.C && rfirst < V.R ? min(PER, (V.R - rfirst + RSTEP - 1) / RSTEP) : 0;
     const long long ustride = (long long)RSTEP * V.C;
     const int at0 = lr0 * W + cc + KA;   // this thread's first point in a slot; point u is RSTEP * W further
+    static_assert(NS == 7 || NS == 27, "TMA-staged sweeps take the 7- and 27-point shapes");
+    // 7 taps: b one plane ahead in registers; 27 taps (coarse levels, in L2):
+    // b read at the point, so the 27 taps' loads have the registers
+    constexpr bool BPRE = NS == 7;
     T bnext[PER];
     auto prefetch = [&](int p) {
         const T* bp = b + ((long long)p * V.R + rfirst) * V.C + c;
 #pragma unroll
         for (int u = 0; u < PER; ++u) bnext[u] = u < nu ? __ldg(bp + u * ustride) : T(0);
     };
-    static_assert(NS == 7 || NS == 27, "TMA-staged sweeps take the 7- and 27-point shapes");
     const int planes = pb - pa;
-    prefetch(pa);
+    if (BPRE) prefetch(pa);
     for (int j = 0; j < planes; ++j) {
         const int p = pa + j;
         T bcur[PER];
+        if (BPRE) {
 #pragma unroll
-        for (int u = 0; u < PER; ++u) bcur[u] = bnext[u];
-        if (j + 1 < planes) prefetch(p + 1);
+            for (int u = 0; u < PER; ++u) bcur[u] = bnext[u];
+            if (j + 1 < planes) prefetch(p + 1);
+        }
         // local planes j, j + 1, j + 2 (planes p - 1, p, p + 1) must have
         // landed: thread 0 waits (one poller instead of a block of them), the
         // block barrier passes the completed copies on to every thread
@@ -362,9 +367,7 @@ __global__ void __launch_bounds__(kTmaThreads, 4) k_level_op_tma(const __grid_co
         // ring index of this thread's first point in the slots of planes p - 1, p, p + 1
         const int bm = (j % NSL) * SLOT + at0, b0 = ((j + 1) % NSL) * SLOT + at0, bp = ((j + 2) % NSL) * SLOT + at0;
         const long long row0 = ((long long)p * V.R + rfirst) * V.C + c;   // global row index of point 0
-#pragma unroll
-        for (int u = 0; u < PER; ++u) {
-            if (u >= nu) break;
+        auto point = [&](int u, T bval) {
             const int du = u * (RSTEP * W);
             const long long row = row0 + u * ustride;
             T s = T(0);
@@ -380,13 +383,21 @@ __global__ void __launch_bounds__(kTmaThreads, 4) k_level_op_tma(const __grid_co
                 const uint32_t bit = 1u << (r32 & 31);
                 if (word & bit) {
                     const int q = (int)__ldg(A.mask_prefix + (r32 >> 5)) + __popc(word & (bit - 1u));
-                    const int b0 = __ldg(A.exc_ptr + q), e0 = __ldg(A.exc_ptr + q + 1);
+                    const int e_lo = __ldg(A.exc_ptr + q), e_hi = __ldg(A.exc_ptr + q + 1);
                     s = T(0);
-                    for (int t = b0; t < e0; ++t) s += __ldg(A.exc_val + t) * __ldg(x + __ldg(A.exc_col + t));
+                    for (int t = e_lo; t < e_hi; ++t) s += __ldg(A.exc_val + t) * __ldg(x + __ldg(A.exc_col + t));
                 }
             }
-            if (Mode == kSmooth) out[row] = ring[b0 + du] + omega * (bcur[u] - s);
-            else out[row] = bcur[u] - s;
+            if (Mode == kSmooth) out[row] = ring[b0 + du] + omega * (bval - s);
+            else out[row] = bval - s;
+        };
+        if constexpr (BPRE) {
+#pragma unroll
+            for (int u = 0; u < PER; ++u)
+                if (u < nu) point(u, bcur[u]);
+        } else {
+#pragma unroll 1
+            for (int u = 0; u < nu; ++u) point(u, __ldg(b + row0 + u * ustride));
         }
     }
     // every issued plane was waited on: nothing is in flight at exit
@@ -436,9 +447,9 @@ __global__ void __launch_bounds__(kThreads) k_restrict(XferDev<T> X, const T* __
     restrict_row<T, true>(X, rf, bc, xc, dinv_c, c);
 }
 
-// x_f += P x_c at fine row f
+// (P x_c) at fine row f
 template <class T, bool RO>
-__device__ __forceinline__ void prolong_row(const XferDev<T>& X, const T* __restrict__ xc, T* __restrict__ xf, int f) {
+__device__ __forceinline__ T prolong_value(const XferDev<T>& X, const T* __restrict__ xc, int f) {
     const int nf1 = X.ax[1].nf, nf2 = X.ax[2].nf;
     const int nc1 = X.ax[1].nc, nc2 = X.ax[2].nc;
     const int fi = (int)fastdiv((unsigned)f, X.divf12);
@@ -465,16 +476,38 @@ __device__ __forceinline__ void prolong_row(const XferDev<T>& X, const T* __rest
             }
         }
     }
+    return s;
+}
+
+// x_f += P x_c at fine row f
+template <class T, bool RO>
+__device__ __forceinline__ void prolong_row(const XferDev<T>& X, const T* __restrict__ xc, T* __restrict__ xf, int f) {
+    const T s = prolong_value<T, RO>(X, xc, f);
     xf[f] = s + xf[f];
 }
+
+// kProlongPer fine points per thread (a block's points are kProlongPer
+// consecutive runs of kThreads), their loads issued together.
+constexpr int kProlongPer = 4;
 
 template <class T>
 __global__ void __launch_bounds__(kThreads) k_prolong_add(XferDev<T> X, const T* __restrict__ xc, T* __restrict__ xf,
                                                           const MGState* __restrict__ st) {
     if (st && st->done) return;   // st == nullptr: ungated (inside the device-side loop)
-    const int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= X.ax[0].nf * X.ax[1].nf * X.ax[2].nf) return;
-    prolong_row<T, true>(X, xc, xf, f);
+    const int nf = X.ax[0].nf * X.ax[1].nf * X.ax[2].nf;
+    const int f0 = blockIdx.x * (blockDim.x * kProlongPer) + threadIdx.x;
+    T e[kProlongPer], old[kProlongPer];
+#pragma unroll
+    for (int u = 0; u < kProlongPer; ++u) {
+        const int f = f0 + u * (int)blockDim.x;
+        e[u] = f < nf ? prolong_value<T, true>(X, xc, f) : T(0);
+        old[u] = f < nf ? xf[f] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kProlongPer; ++u) {
+        const int f = f0 + u * (int)blockDim.x;
+        if (f < nf) xf[f] = e[u] + old[u];
+    }
 }
 
 // x = Ainv b (dense, row-major), one warp per row, fixed shuffle tree.  The
@@ -522,13 +555,32 @@ __device__ __forceinline__ double block_sum(double v) {
 // bhat = TOut(dinv * r) (the FP32 defect of the refinement); per-block
 // partial sums of r^2 (grid-stride, fixed grid -> deterministic).
 template <class TOut, int NS>
-__global__ void __launch_bounds__(kThreads) k_residual64(StencilDev<double> A, const double* __restrict__ x,
+__global__ void __launch_bounds__(kThreads, NS == 27 || NS == 0 ? 2 : 3) k_residual64(StencilDev<double> A, const double* __restrict__ x,
                                                          const double* __restrict__ b, const double* __restrict__ dinv,
                                                          TOut* __restrict__ bhat, double* __restrict__ partials,
                                                          const MGState* __restrict__ st, int gated) {
     if (gated && st && st->done) return;
     double acc = 0.0;
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < A.n; r += gridDim.x * blockDim.x) {
+    const int S = gridDim.x * blockDim.x;
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    // four grid strides per iteration, all loads first (the sums keep the order of the plain loop)
+    constexpr int U = 4;
+    for (; r + (U - 1) * S < A.n; r += U * S) {
+        double ax[U], bb[U], dd[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            ax[u] = stencil_row<double, double, NS>(A, x, r + u * S);
+            bb[u] = b[r + u * S];
+            dd[u] = bhat ? dinv[r + u * S] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const double res = bb[u] - ax[u];
+            acc += res * res;
+            if (bhat) bhat[r + u * S] = TOut(dd[u] * res);
+        }
+    }
+    for (; r < A.n; r += S) {
         const double ax = stencil_row<double, double, NS>(A, x, r);
         const double res = b[r] - ax;
         acc += res * res;
