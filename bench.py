@@ -633,7 +633,8 @@ def run_workload(args):
     precision = P.FP64 if w["precision"] == "fp64" else P.MIXED
     ctx = P.ParticleContext((w["cells"],) * w["dim"], (0.5,) * w["dim"], (w["cells"] + 0.5,) * w["dim"],
                             (1,) * w["dim"], precision)
-    ctx.set_options(f"sort_interval {1 if precision == P.MIXED else 20}")
+    sort_interval = args.sort_interval if precision == P.MIXED else 20
+    ctx.set_options(f"sort_interval {sort_interval}")
     e = ctx.add_species(-1.0, 1.0, L ** w["dim"] / n, n)
     ctx.load(e, pos, vel)
     del pos, vel
@@ -679,7 +680,7 @@ def run_workload(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "dtype": "f64" if precision == P.FP64 else "f32 push / f32-in-f64 MG", "data": "synthetic",
             "config": {"workload": w["desc"], "particles": n, "nodes": nn, "dt": w["dt"], "mg": opts,
-                       "sort_interval": 1 if precision == P.MIXED else 20},
+                       "sort_interval": sort_interval},
             "particle_roofline": {"algorithmic_bytes_per_step": b_step,
                                   "achieved": round(b_step / (ms * 1e-3) / 1e9, 1), "peak": peak,
                                   "frac": round(b_step / (ms * 1e-3) / 1e9 / peak, 4)},

@@ -1495,6 +1495,49 @@ __global__ void k_gather(const T* __restrict__ in, T* __restrict__ out, const in
     if (i < n) out[i] = in[perm[i]];
 }
 
+// Every array of a species' state permuted at once: out[a][i] = in[a][perm[i]]
+// for up to 8 arrays of 4-byte and 6 of 8-byte elements.  perm is read once
+// and each thread has kGatherPer elements of every array in flight.
+struct GatherSet {
+    const uint32_t* in4[8];
+    uint32_t* out4[8];
+    int n4;
+    const unsigned long long* in8[6];
+    unsigned long long* out8[6];
+    int n8;
+};
+constexpr int kGatherPer = 4;
+
+__global__ void __launch_bounds__(256) k_gather_all(GatherSet g, const int* __restrict__ perm, long long n) {
+    const long long i0 = (long long)blockIdx.x * (blockDim.x * kGatherPer) + threadIdx.x;
+    int p[kGatherPer];
+#pragma unroll
+    for (int u = 0; u < kGatherPer; ++u) {
+        const long long i = i0 + (long long)u * blockDim.x;
+        p[u] = i < n ? __ldg(perm + i) : -1;
+    }
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        if (a >= g.n4) break;
+        uint32_t v[kGatherPer];
+#pragma unroll
+        for (int u = 0; u < kGatherPer; ++u) v[u] = p[u] >= 0 ? __ldg(g.in4[a] + p[u]) : 0u;
+#pragma unroll
+        for (int u = 0; u < kGatherPer; ++u)
+            if (p[u] >= 0) g.out4[a][i0 + (long long)u * blockDim.x] = v[u];
+    }
+#pragma unroll
+    for (int a = 0; a < 6; ++a) {
+        if (a >= g.n8) break;
+        unsigned long long v[kGatherPer];
+#pragma unroll
+        for (int u = 0; u < kGatherPer; ++u) v[u] = p[u] >= 0 ? __ldg(g.in8[a] + p[u]) : 0ull;
+#pragma unroll
+        for (int u = 0; u < kGatherPer; ++u)
+            if (p[u] >= 0) g.out8[a][i0 + (long long)u * blockDim.x] = v[u];
+    }
+}
+
 __global__ void k_count_valid(const unsigned* __restrict__ sorted_keys, long long n, unsigned sentinel,
                               long long* __restrict__ count) {
     // first index holding the sentinel (keys are sorted ascending)
@@ -1843,14 +1886,25 @@ static void sort_species(psum_pic_ctx* c, Species& sp, int sidx) {
     int* perm;
     radix_sort(c, n, sentinel, &skeys, &perm);
     const unsigned gb = blocks_for(n, 256);
-    { k_gather<int><<<gb, 256, 0, s>>>(sp.key[cur].p, sp.key[nxt].p, perm, n); count_launch(); }
-    if (c->precision == PSUM_PIC_MIXED) {
-        for (int a = 0; a < c->g.dim; ++a) { k_gather<float><<<gb, 256, 0, s>>>(sp.off[a][cur].p, sp.off[a][nxt].p, perm, n); count_launch(); }
-        for (int q = 0; q < 3; ++q) { k_gather<float><<<gb, 256, 0, s>>>(sp.vel[q][cur].p, sp.vel[q][nxt].p, perm, n); count_launch(); }
-    } else {
-        for (int a = 0; a < c->g.dim; ++a)
-            { k_gather<double><<<gb, 256, 0, s>>>(sp.pos64[a][cur].p, sp.pos64[a][nxt].p, perm, n); count_launch(); }
-        for (int q = 0; q < 3; ++q) { k_gather<double><<<gb, 256, 0, s>>>(sp.vel64[q][cur].p, sp.vel64[q][nxt].p, perm, n); count_launch(); }
+    {
+        GatherSet gs{};
+        auto add4 = [&](const void* in, void* out) {
+            gs.in4[gs.n4] = static_cast<const uint32_t*>(in);
+            gs.out4[gs.n4++] = static_cast<uint32_t*>(out);
+        };
+        auto add8 = [&](const void* in, void* out) {
+            gs.in8[gs.n8] = static_cast<const unsigned long long*>(in);
+            gs.out8[gs.n8++] = static_cast<unsigned long long*>(out);
+        };
+        add4(sp.key[cur].p, sp.key[nxt].p);
+        if (c->precision == PSUM_PIC_MIXED) {
+            for (int a = 0; a < c->g.dim; ++a) add4(sp.off[a][cur].p, sp.off[a][nxt].p);
+            for (int q = 0; q < 3; ++q) add4(sp.vel[q][cur].p, sp.vel[q][nxt].p);
+        } else {
+            for (int a = 0; a < c->g.dim; ++a) add8(sp.pos64[a][cur].p, sp.pos64[a][nxt].p);
+            for (int q = 0; q < 3; ++q) add8(sp.vel64[q][cur].p, sp.vel64[q][nxt].p);
+        }
+        { k_gather_all<<<blocks_for((n + kGatherPer - 1) / kGatherPer, 256), 256, 0, s>>>(gs, perm, n); count_launch(); }
     }
     { k_count_valid<<<gb, 256, 0, s>>>(skeys, n, sentinel, c->count.p + sidx); count_launch(); }
     sp.cur = nxt;
