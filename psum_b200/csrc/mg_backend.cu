@@ -129,7 +129,7 @@ int tma_resident_blocks() {
         cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
         cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
         cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_level_op_tma<T, Mode, NS>, kTmaThreads,
-                                                                 TmaShape<T>::smem()),
+                                                                 TmaShape<T, NS>::smem()),
                    "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
         blocks = std::max(1, sms * std::max(1, per_sm));
     }
@@ -153,9 +153,9 @@ inline PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
 
 // The tensor map of a level vector viewed as (planes, rows, columns) with the
 // sweep's box; the vector is one of the solver's own buffers on this GPU.
-template <class T>
+template <class T, int NS>
 CUtensorMap make_level_map(const T* x, int P, int R, int C) {
-    using S = TmaShape<T>;
+    using S = TmaShape<T, NS>;
     CUtensorMap m;
     const cuuint64_t dims[3] = {(cuuint64_t)C, (cuuint64_t)R, (cuuint64_t)P};
     const cuuint64_t strides[2] = {(cuuint64_t)C * sizeof(T), (cuuint64_t)R * C * sizeof(T)};
@@ -169,19 +169,20 @@ CUtensorMap make_level_map(const T* x, int P, int R, int C) {
     return m;
 }
 
-// Tensor maps of the level vectors the sweeps read, by pointer and view.
+// Tensor maps of the level vectors the sweeps read, by pointer, view and
+// stencil shape (the shape sets the box).
 struct TmapCache {
     struct Entry {
         const void* p;
-        int P, R, C;
+        int P, R, C, ns;
         CUtensorMap m;
     };
     std::vector<Entry> e;
-    template <class T>
+    template <class T, int NS>
     const CUtensorMap& get(const T* x, int P, int R, int C) {
         for (auto& q : e)
-            if (q.p == x && q.P == P && q.R == R && q.C == C) return q.m;
-        e.push_back({x, P, R, C, make_level_map<T>(x, P, R, C)});
+            if (q.p == x && q.P == P && q.R == R && q.C == C && q.ns == NS) return q.m;
+        e.push_back({x, P, R, C, NS, make_level_map<T, NS>(x, P, R, C)});
         return e.back().m;
     }
 };
@@ -189,21 +190,29 @@ struct TmapCache {
 // Launch over V's tiles; the planes are cut into as many chunks as keep one
 // wave of resident blocks busy (each chunk re-reads two halo planes).
 template <class T, int Mode, int NS>
-void launch_tma_ns(const CUtensorMap& map, const StencilDev<T>& A, TmaTile V, const T* x, const T* b, T* out,
-                   T omega, const MGState* st, int* stall, cudaStream_t s) {
+void launch_tma_ns(TmapCache& cache, const StencilDev<T>& A, const T* x, const T* b, T* out, T omega,
+                   const MGState* st, int* stall, cudaStream_t s) {
+    using S = TmaShape<T, NS>;
     static bool attr = false;
     if (!attr) {
         cuda_check(cudaFuncSetAttribute(k_level_op_tma<T, Mode, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)TmaShape<T>::smem()),
+                                        (int)S::smem()),
                    "cudaFuncSetAttribute");
         attr = true;
     }
+    TmaTile V{};
+    V.P = A.n0;
+    V.R = A.n1;
+    V.C = A.n2;
+    V.tiles_c = (V.C + S::TC - 1) / S::TC;
+    V.tiles_r = (V.R + S::TR - 1) / S::TR;
+    const CUtensorMap& map = cache.get<T, NS>(x, V.P, V.R, V.C);
     const long long tiles = (long long)V.tiles_c * V.tiles_r;
     const long long want = std::max(1LL, (long long)tma_resident_blocks<T, Mode, NS>() / tiles);
     V.chunk = (int)std::max(1LL, (V.P + want - 1) / want);
     V.chunks = (V.P + V.chunk - 1) / V.chunk;
     const unsigned blocks = (unsigned)(tiles * V.chunks);
-    k_level_op_tma<T, Mode, NS><<<blocks, kTmaThreads, TmaShape<T>::smem(), s>>>(map, A, V, x, b, out, omega, st, stall);
+    k_level_op_tma<T, Mode, NS><<<blocks, kTmaThreads, S::smem(), s>>>(map, A, V, x, b, out, omega, st, stall);
 }
 
 // TMA-staged sweep of a level (k_level_op_tma); false when the level does
@@ -211,7 +220,6 @@ void launch_tma_ns(const CUtensorMap& map, const StencilDev<T>& A, TmaTile V, co
 template <class T, int Mode>
 bool launch_level_op_tma(TmapCache& cache, long long min_rows, const StencilDev<T>& A, const T* x, const T* b, T* out,
                          T omega, const MGState* st, int* stall, cudaStream_t s) {
-    using S = TmaShape<T>;
     if (Mode == kSmoothFromZero || A.n < min_rows) return false;
     if (!(A.n0 > 2 && A.n1 > 1 && A.n2 > 1)) return false;          // 3-D boxes only (2-D levels stay in L2)
     if ((A.n2 * (int)sizeof(T)) % 16 != 0) return false;             // tensor-map row pitch: 16-byte multiple
@@ -220,16 +228,8 @@ bool launch_level_op_tma(TmapCache& cache, long long min_rows, const StencilDev<
     for (int t = 0; t < A.ns; ++t)
         if (A.di[t] != tma_tap_d(A.ns, t, 0) || A.dj[t] != tma_tap_d(A.ns, t, 1) || A.dk[t] != tma_tap_d(A.ns, t, 2))
             return false;
-    TmaTile V{};
-    V.P = A.n0;
-    V.R = A.n1;
-    V.C = A.n2;
-    V.tiles_c = (V.C + S::TC - 1) / S::TC;
-    V.tiles_r = (V.R + S::TR - 1) / S::TR;
-
-    const CUtensorMap& map = cache.get<T>(x, V.P, V.R, V.C);
-    if (A.ns == 7) launch_tma_ns<T, Mode, 7>(map, A, V, x, b, out, omega, st, stall, s);
-    else launch_tma_ns<T, Mode, 27>(map, A, V, x, b, out, omega, st, stall, s);
+    if (A.ns == 7) launch_tma_ns<T, Mode, 7>(cache, A, x, b, out, omega, st, stall, s);
+    else launch_tma_ns<T, Mode, 27>(cache, A, x, b, out, omega, st, stall, s);
     count_launch();
     return true;
 }

@@ -194,10 +194,10 @@ __host__ __device__ constexpr int tma_tap_d(int ns, int t, int axis) {
 constexpr int kTmaThreads = 256;
 constexpr int kTmaSlots = 5;
 
-template <class T>
+template <class T, int NS>
 struct TmaShape {
     static constexpr int TC = sizeof(T) == 4 ? 128 : 64;   // columns per tile (512 bytes)
-    static constexpr int TR = 8;                            // rows per tile
+    static constexpr int TR = NS == 7 ? 16 : 8;             // rows per tile (27 taps: more tiles, fewer registers)
     static constexpr int KA = 16 / (int)sizeof(T);          // elements per 16 bytes: the column halo of the box
     static constexpr int W = TC + 2 * KA;                   // box columns (multiple of 16 bytes)
     static constexpr int H = TR + 2;                        // box rows
@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(kTmaThreads, 4) k_level_op_tma(const __grid_co
                                                               TmaTile V, const T* __restrict__ x,
                                                               const T* __restrict__ b, T* __restrict__ out, T omega,
                                                               const MGState* __restrict__ st, int* stall) {
-    using S = TmaShape<T>;
+    using S = TmaShape<T, NS>;
     constexpr int TC = S::TC, TR = S::TR, KA = S::KA, W = S::W, H = S::H;
     constexpr int NSL = kTmaSlots;
     constexpr int SLOT = (int)(S::slot_bytes() / sizeof(T));   // slot stride in elements
