@@ -31,9 +31,12 @@ struct Support64 {
     double coef[8];
 };
 
+// D = g.dim as a template argument: the loops unroll and the support stays
+// in registers; the operations and their order are those of the generic
+// restatement, so the bits are too.
+template <int D>
 __device__ __forceinline__ void cic64(const GridView& g, const double* p, long long* idx, double* coef,
                                       double (*dcoef)[8]) {
-    const int D = g.dim;
     int base[3];
     double xn[3];
     for (int a = 0; a < D; ++a) {
@@ -41,7 +44,8 @@ __device__ __forceinline__ void cic64(const GridView& g, const double* p, long l
         const double base_pos = g.lo[a] + (double)base[a] * g.dx[a];
         xn[a] = (p[a] - base_pos) * g.dr[a];
     }
-    const int cnt = 1 << D;
+    constexpr int cnt = 1 << D;
+#pragma unroll
     for (int i = 0; i < cnt; ++i) {
         int node[3] = {base[0], base[1], base[2]};
         int t = i;
@@ -83,6 +87,18 @@ __device__ __forceinline__ void cic64(const GridView& g, const double* p, long l
     }
 }
 
+template <int D>
+__device__ __forceinline__ int key64_d(const GridView& g, const double* p) {
+    int c[3] = {0, 0, 0};
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        int v = (int)floor((p[a] - g.lo[a]) * g.dr[a]);
+        v = v < 0 ? 0 : (v >= g.M[a] ? g.M[a] - 1 : v);
+        c[a] = v;
+    }
+    return (c[0] * g.M[1] + c[1]) * g.M[2] + c[2];
+}
+
 __device__ __forceinline__ int key64(const GridView& g, const double* p) {
     int c[3] = {0, 0, 0};
     for (int a = 0; a < g.dim; ++a) {
@@ -93,12 +109,14 @@ __device__ __forceinline__ int key64(const GridView& g, const double* p) {
     return (c[0] * g.M[1] + c[1]) * g.M[2] + c[2];
 }
 
+template <int D>
 __device__ __forceinline__ void deposit64(const GridView& g, const double* p, bool alive,
                                           unsigned long long* acc, double scale) {
     long long idx[8];
     double coef[8];
-    const int cnt = 1 << g.dim;
-    if (alive) cic64(g, p, idx, coef, nullptr);
+    constexpr int cnt = 1 << D;
+    if (alive) cic64<D>(g, p, idx, coef, nullptr);
+#pragma unroll
     for (int k = 0; k < cnt; ++k) {
         long long node = -1, val = 0;
         if (alive && fabs(coef[k]) > 1e-10) {   // field_interp.hpp:73
@@ -109,10 +127,10 @@ __device__ __forceinline__ void deposit64(const GridView& g, const double* p, bo
     }
 }
 
+template <int D>
 __global__ void __launch_bounds__(kPicThreads) k_push64(Push64Args a) {
     const GridView& g = a.g;
     const long long count = *a.count;
-    const int D = g.dim;
     const int lane = threadIdx.x & 31;
     double kin = 0.0;
     for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < count;
@@ -133,10 +151,12 @@ __global__ void __launch_bounds__(kPicThreads) k_push64(Push64Args a) {
             } else {
                 long long idx[8];
                 double dcoef[3][8];
-                cic64(g, p, idx, nullptr, dcoef);
-                const int cnt = 1 << D;
+                cic64<D>(g, p, idx, nullptr, dcoef);
+                constexpr int cnt = 1 << D;
+#pragma unroll
                 for (int d = 0; d < D; ++d) {
                     double res = 0;
+#pragma unroll
                     for (int k = 0; k < cnt; ++k)
                         if (fabs(dcoef[d][k]) > 1e-10) res += a.phi[idx[k]] * dcoef[d][k];
                     E[d] = -res;
@@ -192,17 +212,18 @@ __global__ void __launch_bounds__(kPicThreads) k_push64(Push64Args a) {
             }
             for (int d = 0; d < D; ++d) a.pos[d][i] = p[d];
             if (!alive) a.pos[0][i] = __longlong_as_double(0x7ff8000000000000LL);   // NaN x: invalid
-            a.key[i] = alive ? key64(g, p) : -1;
+            a.key[i] = alive ? key64_d<D>(g, p) : -1;
             if (a.kin_part && alive) kin += a.kin_hmw * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
         } else if (i < count) {
             a.key[i] = -1;
         }
         warp_count_losses(a.losses, D, lost);
-        if (a.acc) deposit64(g, p, alive, a.acc, a.scale);
+        if (a.acc) deposit64<D>(g, p, alive, a.acc, a.scale);
     }
     if (a.kin_part) block_sum_to(kin, a.kin_part);
 }
 
+template <int D>
 __global__ void __launch_bounds__(kPicThreads) k_deposit64(Deposit64Args a) {
     const GridView& g = a.g;
     const long long count = *a.count;
@@ -215,9 +236,9 @@ __global__ void __launch_bounds__(kPicThreads) k_deposit64(Deposit64Args a) {
         if (alive) {
             p[0] = a.pos[0][i];
             alive = isfinite(p[0]);
-            for (int d = 1; d < g.dim && alive; ++d) p[d] = a.pos[d][i];
+            for (int d = 1; d < D && alive; ++d) p[d] = a.pos[d][i];
         }
-        deposit64(g, p, alive, a.acc, a.scale);
+        deposit64<D>(g, p, alive, a.acc, a.scale);
     }
 }
 
@@ -238,14 +259,21 @@ long long push64_blocks(long long n_upper) {
 
 void launch_push64(const Push64Args& a, long long n_upper, cudaStream_t s) {
     if (n_upper <= 0) return;
-    { k_push64<<<(unsigned)push64_blocks(n_upper), kPicThreads, 0, s>>>(a); count_launch(); }
+    const unsigned blocks = (unsigned)push64_blocks(n_upper);
+    if (a.g.dim == 1) k_push64<1><<<blocks, kPicThreads, 0, s>>>(a);
+    else if (a.g.dim == 2) k_push64<2><<<blocks, kPicThreads, 0, s>>>(a);
+    else k_push64<3><<<blocks, kPicThreads, 0, s>>>(a);
+    count_launch();
 }
 
 void launch_deposit64(const Deposit64Args& a, long long n_upper, cudaStream_t s) {
     if (n_upper <= 0) return;
     const long long warps = (n_upper + 31) / 32;
     const unsigned blocks = (unsigned)std::min<long long>((warps + 7) / 8, 148LL * 16);
-    { k_deposit64<<<blocks, kPicThreads, 0, s>>>(a); count_launch(); }
+    if (a.g.dim == 1) k_deposit64<1><<<blocks, kPicThreads, 0, s>>>(a);
+    else if (a.g.dim == 2) k_deposit64<2><<<blocks, kPicThreads, 0, s>>>(a);
+    else k_deposit64<3><<<blocks, kPicThreads, 0, s>>>(a);
+    count_launch();
 }
 
 void launch_keys64(const GridView& g, double* const pos[3], int* key, const long long* count, long long n_upper,
