@@ -43,7 +43,7 @@ inline unsigned grid_for(long long n, int threads = kThreads) {
     return (unsigned)std::max<long long>(1, (n + threads - 1) / threads);
 }
 
-constexpr int kNormBlocks = 296;   // 2 x 148 SMs: fixed grid -> fixed reduction order
+constexpr int kNormBlocks = 444;   // 3 x 148 SMs: fixed grid -> fixed reduction order
 
 template <class T>
 struct DevStencil {
