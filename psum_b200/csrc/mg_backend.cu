@@ -435,8 +435,14 @@ struct Solver : SolverBase {
                     cuda_check(cudaMemsetAsync(xcur[l], 0, sizeof(T) * lv[l]->n, s), "memset");
                     zero[l] = false;
                 }
-                { k_prolong_add<T><<<grid_for((lv[l]->n + kProlongPer - 1) / kProlongPer), kThreads, 0, s>>>(
-                      lv[l]->xfer, xcur[l + 1], xcur[l], st); count_launch(); }
+                if (lv[l]->xfer.ax[2].nf % 4 == 0) {
+                    k_prolong_add_row4<T><<<grid_for(lv[l]->n / 4), kThreads, 0, s>>>(lv[l]->xfer, xcur[l + 1],
+                                                                                       xcur[l], st);
+                } else {
+                    k_prolong_add<T><<<grid_for((lv[l]->n + kProlongPer - 1) / kProlongPer), kThreads, 0, s>>>(
+                        lv[l]->xfer, xcur[l + 1], xcur[l], st);
+                }
+                count_launch();
                 for (int k = 0; k < post_relax; ++k) smooth(l);
             }
         }

@@ -486,6 +486,70 @@ __device__ __forceinline__ void prolong_row(const XferDev<T>& X, const T* __rest
     xf[f] = s + xf[f];
 }
 
+// Four consecutive fine nodes along the last axis per thread (levels whose
+// rows are a multiple of 4 nodes long): the first two axes' transfer
+// factors and their products are loaded and formed once for the four, and
+// x_f moves as one 4-wide access.  Each node's terms are summed in
+// prolong_value's order, so the bits are prolong_row's.
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_prolong_add_row4(XferDev<T> X, const T* __restrict__ xc,
+                                                               T* __restrict__ xf, const MGState* __restrict__ st) {
+    if (st && st->done) return;
+    const int nf1 = X.ax[1].nf, nf2 = X.ax[2].nf;
+    const int nc1 = X.ax[1].nc, nc2 = X.ax[2].nc;
+    const long long quads = (long long)X.ax[0].nf * nf1 * nf2 / 4;
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= quads) return;
+    const int f = (int)(q * 4);
+    const int fi = (int)fastdiv((unsigned)f, X.divf12);
+    const int rem = f - fi * nf1 * nf2;
+    const int fj = (int)fastdiv((unsigned)rem, X.divf2);
+    const int fk0 = rem - fj * nf2;
+    const int ci[2] = {__ldg(X.ax[0].p_c0 + fi), __ldg(X.ax[0].p_c1 + fi)};
+    const int cj[2] = {__ldg(X.ax[1].p_c0 + fj), __ldg(X.ax[1].p_c1 + fj)};
+    const T wi[2] = {__ldg(X.ax[0].p_w0 + fi), __ldg(X.ax[0].p_w1 + fi)};
+    const T wj[2] = {__ldg(X.ax[1].p_w0 + fj), __ldg(X.ax[1].p_w1 + fj)};
+    int ck[4][2];
+    T wk[4][2];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        ck[u][0] = __ldg(X.ax[2].p_c0 + fk0 + u);
+        ck[u][1] = __ldg(X.ax[2].p_c1 + fk0 + u);
+        wk[u][0] = __ldg(X.ax[2].p_w0 + fk0 + u);
+        wk[u][1] = __ldg(X.ax[2].p_w1 + fk0 + u);
+    }
+    T s[4] = {T(0), T(0), T(0), T(0)};
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+        if (ci[a] < 0) continue;
+#pragma unroll
+        for (int b2 = 0; b2 < 2; ++b2) {
+            if (cj[b2] < 0) continue;
+            const T wij = wi[a] * wj[b2];
+            const T* row = xc + (ci[a] * nc1 + cj[b2]) * nc2;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int c2 = 0; c2 < 2; ++c2) {
+                    if (ck[u][c2] < 0) continue;
+                    s[u] += (wij * wk[u][c2]) * __ldg(row + ck[u][c2]);
+                }
+        }
+    }
+    if constexpr (sizeof(T) == 4) {
+        float4* p = reinterpret_cast<float4*>(xf + f);
+        float4 o = *p;
+        o.x = s[0] + o.x;
+        o.y = s[1] + o.y;
+        o.z = s[2] + o.z;
+        o.w = s[3] + o.w;
+        *p = o;
+    } else {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) xf[f + u] = s[u] + xf[f + u];
+    }
+}
+
 // kProlongPer fine points per thread (a block's points are kProlongPer
 // consecutive runs of kThreads), their loads issued together.
 constexpr int kProlongPer = 4;
