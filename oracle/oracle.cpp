@@ -4,14 +4,16 @@
 // __graft_entry__.smoke() and bench.py's CPU-baseline leg call it to produce
 // the expected results.  No product code path links, loads or calls it.
 //
-// Parity status: the reference path cannot be compiled here (it needs
-// AdaptiveCpp `acpp` for every SYCL kernel and Eigen 3.4 for every solver
-// frontend and multigrid setup; neither is present), so this restatement is
-// pinned by (1) the known-answer properties the reference's own tests assert
-// for this path (CIC partition of unity / one-hot / linear reproduction at
-// 1e-12, derivative vs central differences, multigrid residual reduction,
+// Parity status: parity unpinned at the source.  The reference path cannot
+// be compiled here (it needs AdaptiveCpp `acpp` for every SYCL kernel and
+// Eigen 3.4 for every solver frontend and multigrid setup; neither is
+// present) and the reference ships no golden vectors for it, so no output of
+// PSuM itself checks this restatement.  What constrains it: (1) the
+// known-answer properties the reference's own tests assert for this path
+// (CIC partition of unity / one-hot / linear reproduction at 1e-12,
+// derivative vs central differences, multigrid residual reduction,
 // multigrid vs direct solve within 1e-4 in <= 5 cycles, five-point residual
-// < 1e-8) and (2) golden fixtures committed under tests/golden.
+// < 1e-8) and (2) closed-form fixtures committed under tests/golden.
 //
 // Every function names the reference file:line it restates.
 #include <algorithm>
