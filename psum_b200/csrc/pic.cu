@@ -977,7 +977,7 @@ __global__ void __launch_bounds__(kPicThreads, D == 2 ? 5 : 1) k_cls_pass2(ClsAr
     __shared__ int mcls[kClsWarps][kMoverCap];
     __shared__ unsigned ccount[kClsWarps][32];
     if (*a.far) {   // some particle moved too far: the caller takes the general path (and sums its energy)
-        if (a.p.kin_part && threadIdx.x == 0) a.p.kin_part[blockIdx.x] = 0.0;
+        if (a.p.kin_part && threadIdx.x < kClsWarps) a.p.kin_part[(long long)blockIdx.x * kClsWarps + threadIdx.x] = 0.0;
         return;
     }
     double kin = 0.0;   // kinetic energy of the particles this block writes (option "diagnostics 1")
@@ -1078,7 +1078,12 @@ __global__ void __launch_bounds__(kPicThreads, D == 2 ? 5 : 1) k_cls_pass2(ClsAr
         }
         if (nm) flush(nm);
     }
-    if (a.p.kin_part) block_sum_to(kin, a.p.kin_part);
+    // one partial per warp (fixed butterfly order), so no block barrier at the end
+    if (a.p.kin_part) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) kin += __shfl_xor_sync(full, kin, o);
+        if (lane == 0) a.p.kin_part[(long long)blockIdx.x * kClsWarps + warp] = kin;
+    }
 }
 
 // Cell offsets of a sorted key array in O(particles + cells): the first and
@@ -2278,7 +2283,7 @@ static void cls_step(psum_pic_ctx* c, const double* phi, double dt, int pusher, 
         if (c->sp[si]->n <= 0) continue;
         args[si].block_first = c->sp[si]->cls_first2.p;
         // the second pass sums the kinetic energy of the particles it writes
-        args[si].p.kin_part = kin_slot(c, si, cls_blocks2(c->sp[si]->n, nc, c->g.dim));
+        args[si].p.kin_part = kin_slot(c, si, cls_blocks2(c->sp[si]->n, nc, c->g.dim) * kClsWarps);
         launch_pass(args[si], c->g.dim, pusher, 2, c->sp[si]->n, c->side);
     }
     if (c->timing) {
@@ -2399,7 +2404,7 @@ static void ensure_diag_buffers(psum_pic_ctx* c) {
         const long long n = std::max<long long>(c->sp[s]->n, 1);
         d.kin_off[s] = off;
         d.kin_n[s] = 0;
-        off += std::max({cls_blocks2(n, c->g.n_cells, c->g.dim), (long long)capped_blocks(4LL * kPicThreads, n),
+        off += std::max({cls_blocks2(n, c->g.n_cells, c->g.dim) * kClsWarps, (long long)capped_blocks(4LL * kPicThreads, n),
                          fp64_exact::push64_blocks(n), (long long)blocks_for(n, kPicThreads)});
     }
     grow(d.kin, (size_t)std::max<long long>(off, 1));
