@@ -482,13 +482,15 @@ constexpr int kClsRoundsMax = 4;
 constexpr int cls_rounds(double particles_per_cell) { return particles_per_cell < 64.0 ? 1 : kClsRoundsMax; }
 
 // Particles per block: 2D blocks cover a few tens of cells of one row; 3D
-// blocks stay short enough that their node box usually fits the tile.
-__host__ __device__ constexpr int cls_block_lg(int dim) { return dim == 2 ? 13 : 11; }
+// blocks stay short enough that their node box usually fits the tile, and
+// their tiles small enough for six blocks per SM.
+__host__ __device__ constexpr int cls_block_lg(int dim) { return dim == 2 ? 13 : 10; }
 // Second-pass blocks are short (no node tile to amortise), so that a pending
 // second pass frees SM slots often for the higher-priority work beside it.
 __host__ __device__ constexpr int cls_block_lg2(int) { return 11; }
-// weight of a cell in the block table, in particles (at most 2048 cells per block)
-__host__ __device__ constexpr long long cls_cell_weight(int lgT) { return 1LL << (lgT - 11); }
+// weight of a cell in the block table, in particles (at most 2048 cells per
+// block; blocks of fewer than 2048 particles weigh every cell 1)
+__host__ __device__ constexpr long long cls_cell_weight(int lgT) { return lgT >= 11 ? 1LL << (lgT - 11) : 1LL; }
 
 template <int D>
 struct MoveClasses {
@@ -696,12 +698,12 @@ __device__ __forceinline__ unsigned long long pair64(unsigned lo, unsigned hi) {
 
 // Cells of the pass-1 moment tile and nodes of its node tile: the boxes of a
 // 2D block (one row segment +-1) and of a 3D block (a z-run +-1 in x and y;
-// 2048 particles at 32 per cell span 64 cells: 3 x 3 x 66 cells).  The tiles
-// live in dynamic shared memory (above the 48 KB static limit in 3D).
+// 1024 particles at 32 per cell span 32 cells: 3 x 3 x 34 cells, 4 x 4 x 35
+// nodes).  The tiles live in dynamic shared memory.
 template <int D>
 struct CellTileCap {
-    static constexpr int N = D == 2 ? 384 : 600;
-    static constexpr int NODES = D == 2 ? kClsTileMax : 1100;
+    static constexpr int N = D == 2 ? 384 : 320;
+    static constexpr int NODES = D == 2 ? kClsTileMax : 576;
     // dynamic shared memory of pass 1: cell counts, moment low/high words, node tile
     static constexpr size_t BYTES = sizeof(unsigned) * ((size_t)N * (1 + 2 * ((1 << D) - 1)) + 2 * (size_t)NODES);
 };
