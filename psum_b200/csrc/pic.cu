@@ -970,7 +970,7 @@ constexpr int kMoverCap = 192;
 // class's run is written in the old particle order.
 // (2D: 48 registers, 5 blocks per SM, for more loads in flight.)
 template <int D, int PUSHER, int kClsRounds>
-__global__ void __launch_bounds__(kPicThreads, D == 2 ? 5 : 1) k_cls_pass2(ClsArgs a) {
+__global__ void __launch_bounds__(kPicThreads, D == 2 ? 5 : 4) k_cls_pass2(ClsArgs a) {
     constexpr int kMoverFlushAt = kMoverCap - 32 * kClsRounds;
     constexpr int NC = MoveClasses<D>::N;
     constexpr int STAY = MoveClasses<D>::STAY;
