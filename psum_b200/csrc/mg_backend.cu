@@ -179,7 +179,7 @@ struct TmapCache {
     };
     std::vector<Entry> e;
     template <class T, int NS>
-    const CUtensorMap& get(const T* x, int P, int R, int C) {
+    CUtensorMap get(const T* x, int P, int R, int C) {   // by value: a later insertion may move the entries
         for (auto& q : e)
             if (q.p == x && q.P == P && q.R == R && q.C == C && q.ns == NS) return q.m;
         e.push_back({x, P, R, C, NS, make_level_map<T, NS>(x, P, R, C)});
@@ -206,7 +206,7 @@ void launch_tma_ns(TmapCache& cache, const StencilDev<T>& A, const T* x, const T
     V.C = A.n2;
     V.tiles_c = (V.C + S::TC - 1) / S::TC;
     V.tiles_r = (V.R + S::TR - 1) / S::TR;
-    const CUtensorMap& map = cache.get<T, NS>(x, V.P, V.R, V.C);
+    const CUtensorMap map = cache.get<T, NS>(x, V.P, V.R, V.C);
     const long long tiles = (long long)V.tiles_c * V.tiles_r;
     const long long want = std::max(1LL, (long long)tma_resident_blocks<T, Mode, NS>() / tiles);
     V.chunk = (int)std::max(1LL, (V.P + want - 1) / want);
