@@ -271,6 +271,60 @@ __global__ void __launch_bounds__(kBsThreads, 2) k_bs_gather(BsGrid g, long long
 // the same set as w > 1e-10.
 constexpr int kAggGroups = 4;
 
+// One stencil for the whole warp (the usual case for particles stored cell
+// by cell): the support weights are transposed through shared memory, 16
+// nodes at a time, and lane j (with lane j + 16 over the other half of the
+// warp) sums node j over the 32 lanes -- no warp reductions.  The sums are
+// the same integers as the reductions' (32 parts below 2^27 and 2^13), so
+// the bits are too.  off holds the lane's per-axis node offsets; the
+// leader's are the group's.
+constexpr int kTrChunk = 16;
+struct TrScratch {
+    unsigned lo[kTrChunk][33];
+    unsigned hi[kTrChunk][33];
+    int off[3][8];
+};
+
+template <int N0, int N1, int N2, int NA, class Q>
+__device__ __forceinline__ void deposit_one_group(const Q& q_at, bool ok, int leader, const int (&off)[3][NA],
+                                                  unsigned long long* __restrict__ acc, TrScratch& t, int lane) {
+    constexpr int NN = N0 * N1 * N2;
+    if (lane == leader) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int j = 0; j < NA; ++j) t.off[a][j] = off[a][j];
+    }
+#pragma unroll
+    for (int base = 0; base < NN; base += kTrChunk) {
+#pragma unroll
+        for (int j = 0; j < kTrChunk; ++j) {
+            const int node = base + j;
+            if (node < NN) {
+                const unsigned long long q = ok ? q_at(node / (N1 * N2), (node / N2) % N1, node % N2) : 0ULL;
+                t.lo[j][lane] = (unsigned)(q & 0x7ffffffULL);
+                t.hi[j][lane] = (unsigned)(q >> 27);
+            }
+        }
+        __syncwarp();
+        const int j = lane & (kTrChunk - 1), h = lane >> 4, node = base + j;
+        unsigned slo = 0, shi = 0;
+        if (node < NN) {
+#pragma unroll
+            for (int l = 0; l < 16; ++l) {
+                slo += t.lo[j][h * 16 + l];
+                shi += t.hi[j][h * 16 + l];
+            }
+        }
+        slo += __shfl_xor_sync(0xffffffffu, slo, 16);
+        shi += __shfl_xor_sync(0xffffffffu, shi, 16);
+        const unsigned long long sum = ((unsigned long long)shi << 27) + slo;
+        if (h == 0 && node < NN && sum)
+            atomicAdd(acc + (t.off[0][node / (N1 * N2)] + t.off[1][(node / N2) % N1] + t.off[2][node % N2]), sum);
+        __syncwarp();
+    }
+}
+
 template <int D, int ORDER>
 __global__ void __launch_bounds__(kBsThreads) k_bs_deposit(BsGrid g, long long n, const double* __restrict__ pos,
                                                            double scale, unsigned long long* __restrict__ acc,
@@ -312,7 +366,10 @@ __global__ void __launch_bounds__(kBsThreads) k_bs_deposit(BsGrid g, long long n
     const int key = ok ? off[0][0] + off[1][0] + off[2][0] : -1;
     const unsigned grp = __match_any_sync(kFull, key);
     const unsigned leaders = __ballot_sync(kFull, ok && __ffs(grp) - 1 == lane);
-    if (__popc(leaders) <= kAggGroups) {
+    __shared__ TrScratch tr[kBsThreads / 32];
+    if (__popc(leaders) == 1) {
+        deposit_one_group<S, S1, S2, S>(q_at, ok, __ffs(leaders) - 1, off, acc, tr[threadIdx.x >> 5], lane);
+    } else if (__popc(leaders) <= kAggGroups) {
 #pragma unroll
         for (int k0 = 0; k0 < S; ++k0)
 #pragma unroll
@@ -417,7 +474,10 @@ __global__ void __launch_bounds__(kBsThreads) k_bs_deposit_near(BsGrid g, long l
     const long long gkey = ok ? key : -1LL;
     const unsigned grp = __match_any_sync(kFull, gkey);
     const unsigned leaders = __ballot_sync(kFull, ok && __ffs(grp) - 1 == lane);
-    if (__popc(leaders) <= kAggGroups) {
+    __shared__ TrScratch tr[kBsThreads / 32];
+    if (__popc(leaders) == 1) {
+        deposit_one_group<E, E1, E2, E>(q_at, ok, __ffs(leaders) - 1, off, acc, tr[threadIdx.x >> 5], lane);
+    } else if (__popc(leaders) <= kAggGroups) {
 #pragma unroll
         for (int k0 = 0; k0 < E; ++k0)
 #pragma unroll
