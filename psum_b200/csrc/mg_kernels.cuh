@@ -203,7 +203,8 @@ struct TmaShape {
     static constexpr int H = TR + 2;                        // box rows
     static constexpr size_t box_bytes() { return sizeof(T) * (size_t)W * H; }
     static constexpr size_t slot_bytes() { return (box_bytes() + 127) / 128 * 128; }   // 128-byte aligned slots
-    static constexpr size_t smem() { return slot_bytes() * kTmaSlots + 8 * kTmaSlots; }   // slots, then mbarriers
+    static constexpr int SLOTS = kTmaSlots;
+    static constexpr size_t smem() { return slot_bytes() * SLOTS + 8 * SLOTS; }   // slots, then mbarriers
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -259,7 +260,7 @@ __global__ void __launch_bounds__(kTmaThreads, 4) k_level_op_tma(const __grid_co
                                                               const MGState* __restrict__ st, int* stall) {
     using S = TmaShape<T, NS>;
     constexpr int TC = S::TC, TR = S::TR, KA = S::KA, W = S::W, H = S::H;
-    constexpr int NSL = kTmaSlots;
+    constexpr int NSL = S::SLOTS;
     constexpr int SLOT = (int)(S::slot_bytes() / sizeof(T));   // slot stride in elements
     if (st && st->done) return;   // st == nullptr: ungated (inside the device-side loop)
     extern __shared__ __align__(128) unsigned char tma_smem[];
