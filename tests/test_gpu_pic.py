@@ -501,6 +501,51 @@ def test_fused_step_far_movers_fall_back():
         assert (df.view(np.int64) == dg.view(np.int64)).all()
 
 
+@pytest.mark.parametrize("kind", ["2d_periodic", "3d_periodic"])
+def test_far_mover_back_off_over_several_steps(kind):
+    """After a fused step with far movers the context takes the general path for a doubling back-off, then tries
+    the fused step again.  Every step equals the general path followed by the stable sort: state element by
+    element, keys and densities bit for bit."""
+    steps = 7
+    results = []
+    for interval in (1, 0):
+        ctx, g, pos, vel, phi = make_case(kind, P.MIXED, seed=35, n=40000)
+        pos = wrap_into(pos, g)
+        ctx.set_options(f"sort_interval {interval}")
+        sp = ctx.add_species(-1.0, 1.0, 0.5, pos.shape[1])
+        ctx.load(sp, pos, vel * 8.0)
+        ctx.sort()
+        nn = ctx.n_nodes
+        solver = P.solver_backend("cuda_multigrid64_gpu")
+        dims = [c + 1 for c in g.cells[:g.dim]] + [1] * (3 - g.dim)
+        solver.set_options(f"I {dims[0]} J {dims[1]} K {dims[2]} depth 1 max_cycles 0")
+        idx = np.arange(nn, dtype=np.uint64)
+        solver.set_matrix(nn, nn, nn, idx, idx, np.ones(nn))
+        rho, phi_t = dev(np.zeros(nn)), dev(phi)
+        ctx.deposit()
+        per_step = []
+        for k in range(steps):
+            # far movers in steps 0 and 2 (the second fused attempt doubles the back-off to 2 steps),
+            # slow particles otherwise, so steps 5 and 6 take the fused step again
+            dt = 0.5 if k in (0, 2) else 0.01
+            ctx.step(solver, 0.0, rho, phi_t, dt, P.LEAPFROG)
+            if interval == 0:
+                ctx.sort()
+            torch.cuda.synchronize()
+            p_, v_ = ctx.get_state(sp)
+            kk = torch.zeros(p_.shape[1], dtype=torch.int32, device="cuda")
+            ctx.get_keys(sp, kk)
+            d = dev(np.zeros(nn))
+            ctx.density(sp, d)
+            per_step.append((p_, v_, kk.cpu().numpy(), d.cpu().numpy()))
+        results.append(per_step)
+    for k, ((pf, vf, kf, df), (pg, vg, kg, dg)) in enumerate(zip(*results)):
+        assert (kf == kg).all(), k
+        assert (pf.view(np.int64) == pg.view(np.int64)).all(), k
+        assert (vf.view(np.int64) == vg.view(np.int64)).all(), k
+        assert (df.view(np.int64) == dg.view(np.int64)).all(), k
+
+
 @pytest.mark.parametrize("kind", ["2d_absorb", "2d_periodic", "2d_mixed_bc", "3d_periodic"])
 @pytest.mark.parametrize("pusher", [P.LEAPFROG, P.BORIS])
 def test_fused_step_equals_general_step_then_stable_sort(kind, pusher):
