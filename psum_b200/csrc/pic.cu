@@ -697,12 +697,12 @@ __device__ __forceinline__ unsigned long long pair64(unsigned lo, unsigned hi) {
 }
 
 // Cells of the pass-1 moment tile and nodes of its node tile: the boxes of a
-// 2D block (one row segment +-1) and of a 3D block (a z-run +-1 in x and y;
+// 2D block (one row segment +-1: up to 3 x 170 cells) and of a 3D block (a z-run +-1 in x and y;
 // 1024 particles at 32 per cell span 32 cells: 3 x 3 x 34 cells, 4 x 4 x 35
 // nodes).  The tiles live in dynamic shared memory.
 template <int D>
 struct CellTileCap {
-    static constexpr int N = D == 2 ? 384 : 320;
+    static constexpr int N = D == 2 ? 512 : 320;
     static constexpr int NODES = D == 2 ? kClsTileMax : 576;
     // dynamic shared memory of pass 1: cell counts, moment low/high words, node tile
     static constexpr size_t BYTES = sizeof(unsigned) * ((size_t)N * (1 + 2 * ((1 << D) - 1)) + 2 * (size_t)NODES);
@@ -2139,8 +2139,21 @@ struct PhaseTimer {
 // than one cell along an axis take the general path (in-place push, radix
 // sort) for this step; their deposit from pass 1 stands.
 // blocks of the two tables for up to n particles over nc cells
+// Pass-1 block size (log2 of the particles per block): cls_block_lg, and
+// for dense 2-D species (mean p particles per cell) the largest power of
+// two up to 128 p, at most 2^15, so that a block's three-row cell box
+// (3 x (2^lg / p + 2) cells) stays inside the tile: fewer blocks, less
+// per-block work.
+static int cls_lg1(long long n, long long nc, int dim) {
+    if (dim != 2) return cls_block_lg(dim);
+    const double ppc = nc > 0 ? (double)n / (double)nc : 0.0;
+    int lg = cls_block_lg(dim);
+    while (lg < 15 && (double)(1LL << (lg + 1)) <= 128.0 * ppc) ++lg;
+    return lg;
+}
 static long long cls_blocks(long long n, long long nc, int dim) {
-    return ((n + nc * cls_cell_weight(cls_block_lg(dim))) >> cls_block_lg(dim)) + 1;
+    const int lg = cls_lg1(n, nc, dim);
+    return ((n + nc * cls_cell_weight(lg)) >> lg) + 1;
 }
 static long long cls_blocks2(long long n, long long nc, int dim) {
     return ((n + nc * cls_cell_weight(cls_block_lg2(dim))) >> cls_block_lg2(dim)) + 1;
@@ -2257,7 +2270,8 @@ static void cls_step(psum_pic_ctx* c, const double* phi, double dt, int pusher, 
         }
         a.n_cells = nc;
         const long long nb = cls_blocks(sp.n, nc, c->g.dim);
-        { k_cls_blocks<<<blocks_for(std::max(nc, nb) + 1, 256), 256, 0, s>>>(a.starts, nc, nb, cls_block_lg(c->g.dim),
+        { k_cls_blocks<<<blocks_for(std::max(nc, nb) + 1, 256), 256, 0, s>>>(a.starts, nc, nb,
+                                                                             cls_lg1(sp.n, nc, c->g.dim),
                                                                              sp.cls_first.p); count_launch(); }
         launch_pass(a, c->g.dim, pusher, 1, sp.n, s);
         const long long nb2 = cls_blocks2(sp.n, nc, c->g.dim);

@@ -563,6 +563,21 @@ def test_fused_step_equals_general_step_then_stable_sort(kind, pusher):
         assert (df.view(np.int64) == dg.view(np.int64)).all()
 
 
+@pytest.mark.parametrize("kind", ["2d_periodic", "2d_absorb"])
+def test_fused_step_dense_species_large_blocks(kind):
+    # about 280 particles per cell: the first pass takes blocks of 2^15 particles (up to 130 cells of a row)
+    n = 1_100_000 if kind == "2d_periodic" else 215_000
+    (fused, loss_f, cnt_f), (gen, loss_g, cnt_g) = _fused_vs_general(kind, P.LEAPFROG, 0.12, seed=36,
+                                                                      sort_general=True, n=n)
+    assert (loss_f == loss_g).all()
+    assert cnt_f == cnt_g
+    for (pf, vf, kf, df), (pg, vg, kg, dg) in zip(fused, gen):
+        assert (kf == kg).all()
+        assert (pf.view(np.int64) == pg.view(np.int64)).all()
+        assert (vf.view(np.int64) == vg.view(np.int64)).all()
+        assert (df.view(np.int64) == dg.view(np.int64)).all()
+
+
 @pytest.mark.parametrize("kind", ["2d_periodic", "3d_periodic"])
 def test_fused_step_clustered_cells(kind):
     # a dense blob: cells far above one block's particle budget, many empty
