@@ -241,6 +241,25 @@ def test_mg_mixed_refinement_reaches_fp64():
     assert all(h2 < h1 for h1, h2 in zip(hist, hist[1:]))
 
 
+def test_mg_mixed_refinement_stops_at_tol():
+    """The tol-stopped mixed solve of the CPU arm stops after the first batch of cycles whose relative
+    residual reaches tol (the GPU backends' rule), with the same iterate as the fixed-count solve run for as
+    many batches."""
+    N = 64
+    r, c, v, fixed = dirichlet_box_2d(N)
+    n = (N + 1) ** 2
+    rng = np.random.default_rng(5)
+    b = rng.normal(size=n)
+    b[fixed] = 0.0
+    mg = O.Multigrid(r, c, v, n, N + 1, N + 1, 1, 4)
+    x, hist = mg.solve_mixed_tol(b, np.zeros(n), 24, 2, 2, 2, 1e-8)
+    assert hist[-1] <= 1e-8 < hist[-2]
+    assert all(h > 1e-8 for h in hist[:-1])
+    assert mg.rel_residual(b, x) <= 1.01e-8
+    x_fixed, _ = mg.solve_mixed(b, np.zeros(n), 2 * len(hist), 2, 2, 2)
+    assert np.array_equal(x, x_fixed)
+
+
 def test_fd_order_manufactured():
     # test_manufactured_solution_2d.cpp:87-91: L2 < 1e-3 and order in (1.5, 2.5)
     errs = []
